@@ -1,0 +1,266 @@
+// substep.cuh — per-particle and per-node device code of one MLS-MPM substep.
+//
+// The device functions here are shared by the single-instance kernels
+// (substep.cu) and the batched kernels. Formulas follow
+// phys_sim/diff_simulator/warp_mpm/mpm_utils.py (line numbers cited per function).
+#pragma once
+#include "../../include/empm_b200.h"
+#include "mat3.cuh"
+#include "constitutive.cuh"
+
+namespace empm {
+
+// Quadratic B-spline stencil of one particle (mpm_utils.py:368-383):
+// base = int(x * inv_dx - 0.5) (truncation), fx = x * inv_dx - base,
+// w[axis][offset], dw[axis][offset] = dw/dfx.
+struct Stencil {
+    int   b[3];
+    float fx[3];
+    float w[3][3];
+    float dw[3][3];
+};
+
+EMPM_HD Stencil make_stencil(V3 x, float inv_dx) {
+    Stencil st;
+    const float gp[3] = {x.x * inv_dx, x.y * inv_dx, x.z * inv_dx};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        st.b[a] = (int)(gp[a] - 0.5f);
+        const float f = gp[a] - (float)st.b[a];
+        st.fx[a] = f;
+        const float wa = 1.5f - f, wb = f - 1.f, wc = f - 0.5f;
+        st.w[a][0] = (wa * wa) * 0.5f;
+        st.w[a][1] = (0.f - wb * wb) + 0.75f;
+        st.w[a][2] = (wc * wc) * 0.5f;
+        st.dw[a][0] = f - 1.5f;
+        st.dw[a][1] = -2.f * (f - 1.f);
+        st.dw[a][2] = f - 0.5f;
+    }
+    return st;
+}
+
+EMPM_HD bool stencil_in_grid(const Stencil& st, int G) {
+    return st.b[0] >= 0 && st.b[1] >= 0 && st.b[2] >= 0 &&
+           st.b[0] + 2 < G && st.b[1] + 2 < G && st.b[2] + 2 < G;
+}
+
+// Pre-P2G particle velocity modifiers (mpm_solver_diff.py:977-991, 1022-1036,
+// 1098-1142, 1198-1212, 1332-1348, 1391-1410). Returns true when v changed.
+__device__ __forceinline__ bool apply_modifiers(const EmpmStep& st, int mask_index, V3 x, float mass, V3& v) {
+    bool changed = false;
+    const float dt = st.dt;
+    for (int m = 0; m < st.n_modifiers; ++m) {
+        const EmpmModifier& md = st.modifiers[m];
+        if (md.gate != EMPM_GATE_APPLY) continue;
+        const int mk = md.mask ? __ldg(md.mask + mask_index) : 0;
+        const V3 vec = v3(md.vec[0], md.vec[1], md.vec[2]);
+        switch (md.kind) {
+            case EMPM_MOD_IMPULSE:
+                if (mk == 1) {
+                    const V3 imp = v3(vec.x / mass, vec.y / mass, vec.z / mass);
+                    v = v + imp * dt;
+                    changed = true;
+                }
+                break;
+            case EMPM_MOD_IMPULSE_MASK:
+                if (mk >= 1) { v = v + vec * dt; changed = true; }
+                break;
+            case EMPM_MOD_SET_VELOCITY:
+                if (mk == 1) { v = vec; changed = true; }
+                break;
+            case EMPM_MOD_ROTATION:
+                if (mk == 1) {
+                    const V3 n = v3(md.normal[0], md.normal[1], md.normal[2]);
+                    const V3 a1 = v3(md.axis1[0], md.axis1[1], md.axis1[2]);
+                    const V3 a2 = v3(md.axis2[0], md.axis2[1], md.axis2[2]);
+                    const V3 off = x - v3(md.point[0], md.point[1], md.point[2]);
+                    const float hd = length(off - dot(off, n) * n);
+                    const float cosine = dot(off, a1) / hd;
+                    float theta = acosf(cosine);
+                    if (!(dot(off, a2) > 0.f)) theta = -theta;
+                    const float s1 = -hd * sinf(theta) * md.scale[0];
+                    const float s2 = hd * cosf(theta) * md.scale[0];
+                    v = s1 * a1 + s2 * a2 + md.scale[1] * n;
+                    changed = true;
+                }
+                break;
+            case EMPM_MOD_MOVER:
+                if (mk == 1) {
+                    V3 nv = v + vec;
+                    const V3 off = x - v3(md.point[0], md.point[1], md.point[2]);
+                    nv = nv + md.scale[0] * cross(v3(md.normal[0], md.normal[1], md.normal[2]), off);
+                    v = nv;
+                    changed = true;
+                }
+                break;
+            default: break;
+        }
+    }
+    return changed;
+}
+
+// Grid boundary conditions for node (i, j, k), applied in registration order
+// (the collide closures of mpm_solver_diff.py:473-528, 612-672, 756-793,
+// 835-858, 878-935, 1275-1286). v is the node velocity after normalisation.
+__device__ __forceinline__ void apply_colliders(const EmpmStep& st, int i, int j, int k, int G, float dx,
+                                                long long node, V3& v) {
+    for (int c = 0; c < st.n_colliders; ++c) {
+        const EmpmCollider& cl = st.colliders[c];
+        if (cl.gate == EMPM_GATE_OFF) continue;
+        if (cl.gate == EMPM_GATE_ZERO_ALL) { v = v3(0.f, 0.f, 0.f); continue; }
+        const V3 p = v3(cl.point[0], cl.point[1], cl.point[2]);
+        const V3 off = v3((float)i * dx - p.x, (float)j * dx - p.y, (float)k * dx - p.z);
+        switch (cl.kind) {
+            case EMPM_COLL_SURFACE:
+            case EMPM_COLL_GEOMETRY: {
+                bool inside = false;
+                int shape = (cl.kind == EMPM_COLL_SURFACE) ? EMPM_SHAPE_HALFSPACE : cl.shape;
+                if (shape == EMPM_SHAPE_CUBE) {
+                    inside = fabsf(off.x) < cl.size[0] && fabsf(off.y) < cl.size[1] && fabsf(off.z) < cl.size[2];
+                    if (inside) v = v3(0.f, 0.f, 0.f);
+                } else if (shape == EMPM_SHAPE_SPHERE) {
+                    if (length(off) < cl.radius) v = v3(0.f, 0.f, 0.f);
+                } else if (shape == EMPM_SHAPE_CYLINDER) {
+                    const V3 ax = v3(cl.normal[0], cl.normal[1], cl.normal[2]);
+                    const float proj = dot(off, ax);
+                    const V3 radial = off - proj * ax;
+                    if (fabsf(proj) < cl.half_height && length(radial) < cl.radius) v = v3(0.f, 0.f, 0.f);
+                } else if (shape == EMPM_SHAPE_HALFSPACE) {
+                    const V3 n = v3(cl.normal[0], cl.normal[1], cl.normal[2]);
+                    if (dot(off, n) < 0.f) {
+                        if (cl.surface_type == 11) {
+                            const float z = (float)k * dx;
+                            if (z < 0.4f || z > 0.53f) v = v3(0.f, 0.f, 0.f);
+                            else v = v3(v.x, 0.f, v.z) * 0.3f;
+                        } else {
+                            // sticky, and (as in the reference) slip / separate as well:
+                            // the projected velocity is computed there but zero is written.
+                            v = v3(0.f, 0.f, 0.f);
+                        }
+                    }
+                }
+                break;
+            }
+            case EMPM_COLL_GRID_VELOCITY: {
+                const V3 vset = v3(cl.velocity[0], cl.velocity[1], cl.velocity[2]) +
+                                cl.angular_velocity * cross(v3(cl.rot_axis[0], cl.rot_axis[1], cl.rot_axis[2]), off);
+                bool inside = false;
+                if (cl.shape == EMPM_SHAPE_CUBE) {
+                    inside = fabsf(off.x) < cl.size[0] && fabsf(off.y) < cl.size[1] && fabsf(off.z) < cl.size[2];
+                } else if (cl.shape == EMPM_SHAPE_SPHERE) {
+                    inside = length(off) < cl.radius;
+                } else if (cl.shape == EMPM_SHAPE_CYLINDER) {
+                    const V3 ax = v3(cl.normal[0], cl.normal[1], cl.normal[2]);
+                    const float proj = dot(off, ax);
+                    inside = fabsf(proj) < cl.half_height && length(off - proj * ax) < cl.radius;
+                } else if (cl.shape == EMPM_SHAPE_HALFSPACE) {
+                    inside = dot(off, v3(cl.normal[0], cl.normal[1], cl.normal[2])) < 0.f;
+                }
+                if (inside) v = vset;
+                break;
+            }
+            case EMPM_COLL_CUBOID_VELOCITY:
+                if (fabsf(off.x) < cl.size[0] && fabsf(off.y) < cl.size[1] && fabsf(off.z) < cl.size[2])
+                    v = v3(cl.velocity[0], cl.velocity[1], cl.velocity[2]);
+                break;
+            case EMPM_COLL_BOUNDING_BOX: {
+                const int pad = 3;
+                if (i < pad && v.x < 0.f) v.x = 0.f;
+                if (i >= G - pad && v.x > 0.f) v.x = 0.f;
+                if (j < pad && v.y < 0.f) v.y = 0.f;
+                if (j >= G - pad && v.y > 0.f) v.y = 0.f;
+                if (k < pad && v.z < 0.f) v.z = 0.f;
+                if (k >= G - pad && v.z > 0.f) v.z = 0.f;
+                break;
+            }
+            case EMPM_COLL_GRID_MASK:
+                if (cl.mask && __ldg(cl.mask + node) >= 1) v = v3(0.f, 0.f, 0.f);
+                break;
+            default: break;
+        }
+    }
+}
+
+// Grid normalisation, gravity and damping (mpm_utils.py:426-438, 722-734).
+__device__ __forceinline__ V3 grid_velocity(float4 a, float dt, V3 g, float damping_scale) {
+    V3 v = v3(0.f, 0.f, 0.f);
+    if (a.w > 1e-15f) {
+        const float inv = 1.f / a.w;
+        v = v3(a.x, a.y, a.z) * inv;
+        v = v + dt * g;
+    }
+    if (damping_scale < 1.f) v = v - (1.f - damping_scale) * v;
+    return v;
+}
+
+// Everything P2G needs about one particle after the return map.
+struct P2GParticle {
+    Stencil st;
+    float   wm_scale;   // particle mass
+    V3      v;          // velocity (after modifiers)
+    M3      Cd;         // damped affine matrix
+    M3      Sv;         // -vol * stress
+};
+
+// Contribution of one particle to stencil node (i, j, k) of its stencil:
+// (weight * mass) * (v + C dpos) + dt * (-vol * stress * dweight), and weight * mass
+// (mpm_utils.py:385-423).
+EMPM_HD float4 p2g_node(const P2GParticle& q, int i, int j, int k, float dx, float inv_dx, float dt) {
+    const Stencil& st = q.st;
+    const V3 dpos = v3(((float)i - st.fx[0]) * dx, ((float)j - st.fx[1]) * dx, ((float)k - st.fx[2]) * dx);
+    const float weight = st.w[0][i] * st.w[1][j] * st.w[2][k];
+    const V3 dweight = v3(st.dw[0][i] * st.w[1][j] * st.w[2][k],
+                          st.w[0][i] * st.dw[1][j] * st.w[2][k],
+                          st.w[0][i] * st.w[1][j] * st.dw[2][k]) * inv_dx;
+    const float wm = weight * q.wm_scale;
+    const V3 force = q.Sv * dweight;
+    const V3 add = wm * (q.v + q.Cd * dpos) + dt * force;
+    return make_float4(add.x, add.y, add.z, wm);
+}
+
+__device__ __forceinline__ M3 damp_affine(const M3& C, float rpic) {
+    if (rpic < -0.001f) return m3_zero();
+    return (1.f - rpic) * C + (rpic / 2.f) * (C - transpose(C));
+}
+
+__device__ __forceinline__ void red_add_v4(float4* addr, float4 val) {
+    atomicAdd(addr, val);  // red.global.add.v4.f32 on sm_90+
+}
+
+// G2P gather for one particle from the node velocities (mpm_utils.py:528-576).
+struct G2POut {
+    V3 v;
+    M3 C;
+    M3 gradv;
+};
+
+template <typename Fetch>
+__device__ __forceinline__ G2POut g2p_gather(const Stencil& st, float inv_dx, Fetch fetch) {
+    G2POut o;
+    o.v = v3(0.f, 0.f, 0.f);
+    o.C = m3_zero();
+    o.gradv = m3_zero();
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const V3 dpos = v3((float)i - st.fx[0], (float)j - st.fx[1], (float)k - st.fx[2]);
+                const float weight = st.w[0][i] * st.w[1][j] * st.w[2][k];
+                const V3 gv = fetch(i, j, k);
+                o.v = o.v + gv * weight;
+                o.C = o.C + (weight * inv_dx * 4.f) * outer(gv, dpos);
+                const V3 dweight = v3(st.dw[0][i] * st.w[1][j] * st.w[2][k],
+                                      st.w[0][i] * st.dw[1][j] * st.w[2][k],
+                                      st.w[0][i] * st.w[1][j] * st.dw[2][k]) * inv_dx;
+                o.gradv = o.gradv + outer(gv, dweight);
+            }
+    return o;
+}
+
+__device__ __forceinline__ bool finite3(V3 a) {
+    return isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
+}
+
+}  // namespace empm

@@ -1,0 +1,219 @@
+/*
+ * empm_b200.h — C ABI of the B200 (sm_100a) MLS-MPM substep library.
+ *
+ * This library replaces the Warp kernels and the per-substep launch sequence of
+ * EMPM's differentiable MPM simulator (phys_sim/diff_simulator/warp_mpm/).
+ * Every function returns an int status (EMPM_OK = 0, negative = error) and
+ * takes plain pointers and sizes; device pointers are borrowed (the caller,
+ * normally PyTorch, owns them) and the CUDA stream is passed explicitly.
+ * A context owns only its own scratch (grid buffers, step tables, status word).
+ *
+ * Particle layout in HBM ("f4" and "f9" planes, structure of arrays):
+ *   x   : float[4*N]  per particle (x, y, z, mass)          -- one float4
+ *   v   : float[4*N]  per particle (vx, vy, vz, 0)          -- one float4
+ *   C,F : float[9*N]  3x3 row-major matrix split in three planes:
+ *         plane A float4[N] = (m00, m01, m02, m10)
+ *         plane B float4[N] = (m11, m12, m20, m21)
+ *         plane C float [N] = (m22)
+ *         plane A starts at the pointer, B at +16*N bytes, C at +32*N bytes.
+ * Grid layout: float4[G*G*G], node (i,j,k) at (i*G + j)*G + k.
+ *
+ * Reference interfaces replaced (paths relative to the EMPM repository):
+ *   empm_substep        <- MPMWARPDiff.p2g2p_differentiable
+ *                          phys_sim/diff_simulator/warp_mpm/mpm_solver_diff.py:165-291
+ *                          (kernels zero_grid, compute_stress_from_F_trial,
+ *                          p2g_apic_with_stress, grid_normalization_and_gravity,
+ *                          add_damping_via_grid, collider closures, g2p_differentiable
+ *                          in mpm_utils.py:286-665,722-734 and
+ *                          mpm_solver_diff.py:473-528,612-672,756-801,835-866,878-935,1275-1286)
+ *   empm_rollout        <- the substep loop of WarpMPMWrapper.advance_to
+ *                          warp_mpm_wrapper.py:278-306 and interface.py:137-145
+ *   empm_prepare        <- compute_mu_lam_from_E_nu (mpm_utils.py:277-283) and the
+ *                          mass = density * vol launch (mpm_data_structure.py:719-726)
+ *   empm_pack_particles / empm_unpack_particles
+ *                       <- MPMStateStruct.from_torch / continue_from_torch and
+ *                          wp.to_torch of particle arrays (mpm_data_structure.py:119-172,257-292)
+ */
+#ifndef EMPM_B200_H
+#define EMPM_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMPM_OK                 0
+#define EMPM_ERR_INVALID       -1  /* bad argument (null pointer, size out of range) */
+#define EMPM_ERR_CUDA          -2  /* a CUDA runtime call failed; see empm_last_error */
+#define EMPM_ERR_OOM           -3  /* device allocation failed */
+#define EMPM_ERR_UNSUPPORTED   -4  /* material or option not supported */
+#define EMPM_ERR_TIMEOUT       -5  /* a bounded device-side wait gave up */
+#define EMPM_ERR_NUMERIC       -6  /* device status word reported NaN/Inf or CFL breach */
+
+#define EMPM_MAX_COLLIDERS  16
+#define EMPM_MAX_MODIFIERS  8
+
+/* Device status word bits (empm_read_status). */
+#define EMPM_STATUS_NAN          1u   /* non-finite x, v or F written */
+#define EMPM_STATUS_CFL          2u   /* |v| * dt > dx for some particle */
+#define EMPM_STATUS_OUT_OF_BAND  4u   /* particle stencil outside the grid (clamped) */
+
+/* Material ids, identical to MPMWARPDiff.set_parameters_dict (mpm_solver_diff.py:39-55). */
+#define EMPM_MAT_JELLY        0
+#define EMPM_MAT_METAL        1
+#define EMPM_MAT_SAND         2
+#define EMPM_MAT_FOAM         3
+#define EMPM_MAT_SNOW         4
+#define EMPM_MAT_PLASTICINE   5
+#define EMPM_MAT_NEOHOOKEAN   6
+
+/* Scalar model parameters: the scalar fields of MPMModelStruct
+ * (mpm_data_structure.py:391-422; defaults in init_other_params :456-484). */
+typedef struct {
+    int   n_grid;                 /* cubic grid resolution G */
+    float grid_lim;               /* domain extent (dx = grid_lim / G) */
+    int   material;               /* EMPM_MAT_* */
+    float gravity[3];             /* gravitational_accelaration */
+    float rpic_damping;           /* 0 = APIC, < -0.001 = PIC */
+    float grid_v_damping_scale;   /* < 1 enables add_damping_via_grid */
+    float softening;
+    float hardening;
+    float xi;
+    float plastic_viscosity;
+    float alpha;                  /* Drucker-Prager alpha from friction_angle */
+} EmpmModelParams;
+
+/* Collider kinds: one per factory of MPMWARPDiff. */
+#define EMPM_COLL_SURFACE          1  /* add_surface_collider        mpm_solver_diff.py:437-531 */
+#define EMPM_COLL_GEOMETRY         2  /* add_geometry_collider       :533-683 */
+#define EMPM_COLL_GRID_VELOCITY    3  /* set_grid_velocity_on_geometry :685-804 */
+#define EMPM_COLL_CUBOID_VELOCITY  4  /* set_velocity_on_cuboid      :814-869 */
+#define EMPM_COLL_BOUNDING_BOX     5  /* add_bounding_box            :871-938 */
+#define EMPM_COLL_GRID_MASK        6  /* enforce_grid_velocity_by_mask :1264-1289 */
+
+/* Shapes of the geometry colliders (geo_type in the reference). */
+#define EMPM_SHAPE_CUBE       1
+#define EMPM_SHAPE_SPHERE     2
+#define EMPM_SHAPE_CYLINDER   3
+#define EMPM_SHAPE_HALFSPACE  4
+
+/* Per-substep gate decided on the host from the collider's time window
+ * (the `time >= start_time and time < end_time` tests of the closures). */
+#define EMPM_GATE_OFF        0    /* collider does nothing this substep */
+#define EMPM_GATE_APPLY      1    /* apply the collider's shape rule */
+#define EMPM_GATE_ZERO_ALL   2    /* reset branch: zero every grid node */
+
+typedef struct {
+    int   kind;            /* EMPM_COLL_* */
+    int   gate;            /* EMPM_GATE_* for this substep */
+    int   shape;           /* EMPM_SHAPE_* (geometry kinds) */
+    int   surface_type;    /* 0 sticky, 1 slip, 11 cut, 2 other */
+    float point[3];
+    float normal[3];       /* unit normal / cylinder axis */
+    float size[3];         /* half extents (cube, cuboid) */
+    float velocity[3];
+    float rot_axis[3];
+    float angular_velocity;
+    float radius;
+    float half_height;
+    float friction;
+    const int32_t* mask;   /* device [G^3] for EMPM_COLL_GRID_MASK, else NULL */
+} EmpmCollider;
+
+/* Particle velocity modifiers applied before P2G (pre_p2g_operations and
+ * particle_velocity_modifiers of MPMWARPDiff). */
+#define EMPM_MOD_IMPULSE          1  /* add_impulse_on_particles:           v += force/mass*dt (mask==1) :943-991 */
+#define EMPM_MOD_IMPULSE_MASK     2  /* add_impulse_on_particles_with_mask: v += force*dt     (mask>=1) :1353-1410 */
+#define EMPM_MOD_SET_VELOCITY     3  /* enforce_particle_velocity_translation/_by_mask: v = velocity (mask==1) :993-1036,1173-1212 */
+#define EMPM_MOD_ROTATION         4  /* enforce_particle_velocity_rotation  :1041-1142 */
+#define EMPM_MOD_MOVER            5  /* set_particle_mover: v += velocity + w * axis x (x - center) :1291-1348 */
+
+typedef struct {
+    int   kind;            /* EMPM_MOD_* */
+    int   gate;            /* EMPM_GATE_OFF or EMPM_GATE_APPLY for this substep */
+    float vec[3];          /* force or velocity */
+    float point[3];        /* rotation: cylinder point; mover: rotation center */
+    float normal[3];       /* rotation: cylinder axis; mover: rotation axis */
+    float axis1[3];        /* rotation: horizontal_axis_1 */
+    float axis2[3];        /* rotation: horizontal_axis_2 */
+    float scale[2];        /* rotation: rotation_scale, translation_scale; mover: angular velocity in [0] */
+    const int32_t* mask;   /* device [N] indexed by the caller's particle order */
+} EmpmModifier;
+
+/* One substep's host-side schedule: the solver time (float32 as the kernels
+ * see it), dt, and the colliders / modifiers with their gates resolved. */
+typedef struct {
+    float time;
+    float dt;
+    int   n_colliders;
+    int   n_modifiers;
+    EmpmCollider colliders[EMPM_MAX_COLLIDERS];
+    EmpmModifier modifiers[EMPM_MAX_MODIFIERS];
+} EmpmStep;
+
+/* Particle state buffers (device pointers, layout in the file header). */
+typedef struct {
+    float* x;       /* float4 plane (x, y, z, mass) */
+    float* v;       /* float4 plane (vx, vy, vz, 0) */
+    float* C;       /* f9 planes: APIC affine matrix */
+    float* F;       /* f9 planes: trial deformation gradient (particle_F_trial) */
+} EmpmParticles;
+
+/* Per-particle material arrays (device pointers, [N] each). */
+typedef struct {
+    const float*   vol;          /* particle_vol */
+    float*         mu;           /* mutated by plasticine (damage) */
+    float*         lam;          /* mutated by plasticine (damage) */
+    float*         yield_stress; /* mutated by the von Mises return maps */
+    const int32_t* selection;    /* particle_selection (0 = simulated) or NULL */
+    float*         F_elastic;    /* f9 planes [N]: receives particle_F (post-return-map F) */
+} EmpmMaterial;
+
+typedef struct EmpmCtx EmpmCtx;
+
+int  empm_version(void);
+
+/* Create a context for one simulation instance of n_particles on a G^3 grid.
+ * Allocates the two grid buffers (2 * 16 * G^3 bytes), a step table of
+ * max_steps entries and the status word on the current device. */
+int  empm_ctx_create(const EmpmModelParams* params, int n_particles, int max_steps, EmpmCtx** out);
+int  empm_ctx_destroy(EmpmCtx* ctx);
+int  empm_ctx_set_params(EmpmCtx* ctx, const EmpmModelParams* params);
+
+/* mu = E / (2 (1 + nu)), lam = E nu / ((1 + nu)(1 - 2 nu)); mass = density * vol,
+ * written into x[4p+3]. Any of E/nu (mu/lam) or density (x) may be NULL to skip. */
+int  empm_prepare(EmpmCtx* ctx, const float* E, const float* nu, float* mu, float* lam,
+                  const float* density, const float* vol, float* x, int n, void* stream);
+
+/* Reference layout <-> library layout. x3, v3: [N,3]; C9, F9: [N,3,3] row-major.
+ * pack: writes x (keeps mass already in x[4p+3] when keep_mass != 0, else sets
+ * it from mass3 (may be NULL -> 0)), v, C, F. NULL sources leave that plane alone. */
+int  empm_pack_particles(const float* x3, const float* v3, const float* C9, const float* F9,
+                         const float* mass, int keep_mass, EmpmParticles* dst, int n, void* stream);
+int  empm_unpack_particles(const EmpmParticles* src, float* x3, float* v3, float* C9, float* F9,
+                           int n, void* stream);
+
+/* One MLS-MPM substep: in -> out (distinct buffers). step is a host pointer;
+ * the schedule is copied to the device on the given stream. */
+int  empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out,
+                  const EmpmMaterial* mat, const EmpmStep* step, void* stream);
+
+/* n_steps substeps, ping-ponging between a and b (the result is in a when
+ * n_steps is even, else in b). steps is a host array of n_steps schedules
+ * (n_steps <= max_steps of the context). When use_graph != 0 the launch
+ * sequence is captured once into a CUDA graph per (a, b, n_steps) and replayed. */
+int  empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
+                  const EmpmStep* steps, int n_steps, int use_graph, void* stream);
+
+/* Device status word (EMPM_STATUS_* bits), read synchronously and cleared. */
+int  empm_read_status(EmpmCtx* ctx, uint32_t* status, void* stream);
+
+/* Last error message of the context (or of the library when ctx is NULL). */
+int  empm_last_error(EmpmCtx* ctx, char* buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMPM_B200_H */
