@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the MLS-MPM substep on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1] [--impl ours|reference]
+
+Workload (default c2, the large single forward configuration): 500,000
+particles in two seeded boxes, 128^3 grid, plasticine (von Mises + FCR),
+moving box collider, dt=1e-4 x 1000 substeps. One step = one full 1000-substep
+rollout from the initial state (reset by device copies inside the timed region).
+Metric: particle-substeps/s (whole job; replicas on N>1 GPUs, weak scaling).
+
+Timed region: W untimed steps, then K steps bracketed by a barrier and
+torch.cuda.synchronize(), CUDA events on the launch stream, max over ranks.
+The working set (two particle states of 60 MB, the 18 MB elastic-F buffer
+and two 34 MB grids) is larger than the 126 MB L2, so no flush is needed.
+
+--impl reference times the reference's algorithm on the host cores instead:
+the reference is Python + NVIDIA Warp, which cannot be installed offline,
+so its CPU path is represented by the FP32 OpenMP build of the CPU oracle
+(oracle/mpm_oracle.c) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-substeps/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return PEAKS_FALLBACK["hbm_gbs"], "fallback"
+
+
+def bytes_per_particle(material: str):
+    """Algorithmic bytes per particle-substep: x, v, C, F read + written
+    (192 B) and mass, vol, mu, lam read (16 B); plasticine adds the yield read
+    and the yield/mu/lam write-back (16 B). Split: the fused stress+P2G kernel
+    performs every read (112 / 116 B) and the material write-back (0 / 12 B);
+    G2P writes x, v, C, F (96 B)."""
+    if material == "plasticine":
+        return {"substep": 224, "stress_p2g": 128, "g2p": 96}
+    return {"substep": 208, "stress_p2g": 112, "g2p": 96}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples taken every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+    return world, rank, local
+
+
+def get_workload(name):
+    from empm_b200 import workloads as W
+
+    return {"c1": W.c1, "c2": W.c2}[name]()
+
+
+def cpu_baseline(w, budget_s=12.0, max_substeps=40):
+    """FP32 OpenMP oracle on the host cores over a bounded sample of w."""
+    from oracle import oracle as O
+    from oracle import specs as OS
+
+    sim = OS.sim_from_workload(w, precision="fp32_omp")
+    cb = OS.workload_callback(w)
+    t0 = time.perf_counter()
+    k = 0
+    while k < max_substeps and (time.perf_counter() - t0) < budget_s:
+        if cb:
+            cb(sim, k)
+        sim.substep(w.dt)
+        k += 1
+    el = time.perf_counter() - t0
+    return {"value": w.n * k / el, "unit": METRIC, "cores": int(O.lib("fp32_omp").lib.or_num_threads()),
+            "kind": "port",
+            "sample": f"{w.n} particles x {k} substeps of {w.name} from its initial state "
+                      f"(FP32 OpenMP build of the CPU oracle; Warp's CPU device is not installable offline)"}
+
+
+def run_reference(args):
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from oracle import specs as OS
+
+    w = get_workload(args.workload)
+    sim = OS.sim_from_workload(w, precision="fp32_omp")
+    cb = OS.workload_callback(w)
+    per_step = args.ref_substeps
+    step = 0
+
+    def one_step():
+        nonlocal step
+        for _ in range(per_step):
+            if cb:
+                cb(sim, step)
+            sim.substep(w.dt)
+            step += 1
+
+    for _ in range(args.warmup):
+        one_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_step()
+    el = time.perf_counter() - t0
+    value = w.n * per_step * args.steps / el
+    cores = int(O.lib("fp32_omp").lib.or_num_threads())
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.description, "sample_per_step": f"{w.n} particles x {per_step} substeps"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{w.n} particles x {per_step} substeps per step of {w.name} (FP32 OpenMP CPU "
+                                   "oracle; the reference's Warp CPU device cannot be installed offline)"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from empm_b200 import workloads as W
+
+    w = get_workload(args.workload)
+    solver, md, st, other = W.build_product(w, device=dev)
+    cb = W.cuboid_callback(w, solver)
+    schedule = solver.build_schedule(0.0, w.dt, w.T, cb)
+    init = dict(x=st._x4.clone(), v=st._v4.clone(), C=st._C.clone(), F=st._F_trial.clone(), mu=md.mu.clone(),
+                lam=md.lam.clone(), ys=md.yield_stress.clone())
+
+    def reset():
+        st._x4.copy_(init["x"])
+        st._v4.copy_(init["v"])
+        st._C.copy_(init["C"])
+        st._F_trial.copy_(init["F"])
+        md.mu.copy_(init["mu"])
+        md.lam.copy_(init["lam"])
+        md.yield_stress.copy_(init["ys"])
+
+    def step():
+        reset()
+        solver.rollout(md, st, other, w.dt, w.T, schedule=schedule)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    status = solver.read_status()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * w.particle_substeps * args.steps / (ms / 1e3)
+
+    # --- per-kernel durations: same workload on the stream path with events ---
+    solver.use_graph = False
+    solver.kernel_timing(True, max_launches=w.T + 8)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    step()
+    p1.record()
+    torch.cuda.synchronize()
+    kt = solver.kernel_times()
+    stream_ms = p0.elapsed_time(p1)
+    solver.kernel_timing(False)
+    solver.use_graph = True
+    peak, peak_kind = load_peaks()
+    bp = bytes_per_particle(w.material)
+    kms = {k: v[0] / max(v[1], 1) for k, v in kt.items()}
+    top = max(kms, key=kms.get)
+    dom = "stress_p2g"
+    achieved = w.n * bp[dom] / (kms[dom] / 1e3) / 1e9
+    substep_ms = ms / args.steps / w.T
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{w.name}.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(dom)
+
+    # --- end to end through the reference-facing API with host buffers ---
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    hx, hv, hE, hnu, hys = pin(w.x), pin(w.v), pin(w.E), pin(w.nu), pin(w.ys)
+    hout = torch.empty((w.n, 3), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        st.reset_state(hx, None, hv, device=dev)
+        md.E.copy_(hE, non_blocking=True)
+        md.nu.copy_(hnu, non_blocking=True)
+        md.yield_stress.copy_(hys, non_blocking=True)
+        solver.prepare_mu_lam(md, st)
+        res = solver.rollout(md, st, other, w.dt, w.T, schedule=schedule)
+        hout.copy_(res.particle_x, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    q1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1))
+    e2e_value = world * w.particle_substeps * args.steps / (e2e_ms / 1e3)
+    h2d = w.n * (12 + 12 + 4 + 4 + 4)
+    d2h = w.n * 12
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.description, "particles": w.n, "grid": w.G, "substeps_per_step": w.T,
+                   "dt": w.dt, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (working set ~200 MB > 126 MB), no flush",
+                   "launch": "CUDA graph per rollout (3 kernels per substep)",
+                   "substep_us": substep_ms * 1e3,
+                   "substep_hbm_frac": (w.n * bp["substep"] / (substep_ms / 1e3) / 1e9) / peak,
+                   "status_word": status},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_particle": bp[dom], "launch_ms": kms[dom],
+                     "kernel_ms": {k: round(v, 5) for k, v in kms.items()}, "top_kernel": top,
+                     "timing": "CUDA events around each kernel on its launch stream, stream path of one "
+                               f"rollout in this run ({stream_ms:.2f} ms vs {ms / args.steps:.2f} ms graph)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": 3 * w.T * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-substeps", type=int, default=2, help="substeps per step of the reference arm")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,6 +1,7 @@
 // ctx.hpp — the opaque EmpmCtx behind the C ABI.
 #pragma once
 #include <cuda_runtime.h>
+#include <vector>
 #include "../../include/empm_b200.h"
 
 struct GraphKey {
@@ -25,6 +26,11 @@ struct EmpmCtx {
     cudaGraphExec_t graph_exec = nullptr;
     GraphKey     graph_key{};
     bool         graph_valid = false;
+    // per-kernel event timing (stream path only)
+    bool         timing = false;
+    int          timing_capacity = 0;
+    int          timing_count[3] = {0, 0, 0};
+    std::vector<cudaEvent_t> timing_events;   // [3][capacity][2]
     char         err[512] = {0};
 };
 

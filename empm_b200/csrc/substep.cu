@@ -198,7 +198,23 @@ __global__ void k_prepare(const float* E, const float* nu, float* mu, float* lam
     if (density && vol && x) x[p].w = density[p] * vol[p];
 }
 
+__global__ void k_debug_stress(const float* Ft9, float* mu, float* lam, float* ys, float dt, MaterialScalars ms,
+                               float* F9, float* S9, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    M3 Ft;
+    for (int i = 0; i < 9; ++i) Ft.m[i] = Ft9[9 * p + i];
+    float m = mu[p], l = lam[p], y = ys[p];
+    const ConstitutiveOut co = constitutive(Ft, m, l, y, dt, ms);
+    mu[p] = m; lam[p] = l; ys[p] = y;
+    for (int i = 0; i < 9; ++i) { F9[9 * p + i] = co.F.m[i]; S9[9 * p + i] = co.tau.m[i]; }
+}
+
 inline int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+static_assert(sizeof(EmpmCollider) == 104, "EmpmCollider layout changed: update empm_b200/_native.py");
+static_assert(sizeof(EmpmModifier) == 88, "EmpmModifier layout changed: update empm_b200/_native.py");
+static_assert(sizeof(EmpmStep) == 2384, "EmpmStep layout changed: update empm_b200/_native.py");
 
 }  // namespace
 
@@ -278,6 +294,7 @@ extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, i
 extern "C" int empm_ctx_destroy(EmpmCtx* ctx) {
     if (!ctx) return EMPM_OK;
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    for (cudaEvent_t ev : ctx->timing_events) cudaEventDestroy(ev);
     if (ctx->grid_mom) cudaFree(ctx->grid_mom);
     if (ctx->grid_vel) cudaFree(ctx->grid_vel);
     if (ctx->d_steps) cudaFree(ctx->d_steps);
@@ -350,6 +367,14 @@ static int check_material(EmpmCtx* ctx, const EmpmMaterial* m) {
     return EMPM_OK;
 }
 
+static void timing_mark(EmpmCtx* ctx, int kernel, int which, cudaStream_t stream) {
+    if (!ctx->timing) return;
+    int idx = ctx->timing_count[kernel];
+    if (idx >= ctx->timing_capacity) return;
+    cudaEventRecord(ctx->timing_events[((size_t)kernel * ctx->timing_capacity + idx) * 2 + which], stream);
+    if (which == 1) ctx->timing_count[kernel] = idx + 1;
+}
+
 // Enqueue the three kernels of substep `s` (schedule at d_steps + s).
 static int launch_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out, const EmpmMaterial* mat,
                           const EmpmStep* d_step, cudaStream_t stream) {
@@ -386,7 +411,9 @@ static int launch_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* 
         a.rpic = P.rpic_damping;
         a.ms = ms;
         a.step = d_step;
+        timing_mark(ctx, 0, 0, stream);
         k_stress_p2g<<<blocks_for(n, 128), 128, 0, stream>>>(a);
+        timing_mark(ctx, 0, 1, stream);
         CK(cudaGetLastError(), "k_stress_p2g");
     }
     {
@@ -401,7 +428,9 @@ static int launch_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* 
         const long long total = (long long)G * G * G;
         int nb = blocks_for(total, 256);
         if (nb > 148 * 16) nb = 148 * 16;
+        timing_mark(ctx, 1, 0, stream);
         k_grid_update<<<nb, 256, 0, stream>>>(g);
+        timing_mark(ctx, 1, 1, stream);
         CK(cudaGetLastError(), "k_grid_update");
     }
     if (n > 0) {
@@ -420,7 +449,9 @@ static int launch_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* 
         a.inv_dx = inv_dx;
         a.grid_lim = P.grid_lim;
         a.step = d_step;
+        timing_mark(ctx, 2, 0, stream);
         k_g2p<<<blocks_for(n, 128), 128, 0, stream>>>(a);
+        timing_mark(ctx, 2, 1, stream);
         CK(cudaGetLastError(), "k_g2p");
     }
     return EMPM_OK;
@@ -486,7 +517,10 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
     if (!ctx->graph_valid || memcmp(&key, &ctx->graph_key, sizeof(key)) != 0) {
         if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
         ctx->graph_valid = false;
-        CK(cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        const bool timing_was = ctx->timing;
+        ctx->timing = false;
+        cudaError_t cap = cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal);
+        if (cap != cudaSuccess) { ctx->timing = timing_was; CK(cap, "begin capture"); }
         for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
             const EmpmParticles* in = (i & 1) ? b : a;
             EmpmParticles* out = (i & 1) ? a : b;
@@ -494,6 +528,7 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
         }
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
+        ctx->timing = timing_was;
         if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
         CK(e, "end capture");
         e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
@@ -524,5 +559,67 @@ extern "C" int empm_read_status(EmpmCtx* ctx, uint32_t* status, void* stream) {
 extern "C" int empm_last_error(EmpmCtx* ctx, char* buf, int len) {
     if (!buf || len <= 0) return EMPM_ERR_INVALID;
     snprintf(buf, (size_t)len, "%s", ctx ? ctx->err : g_err);
+    return EMPM_OK;
+}
+
+extern "C" int empm_debug_stress(const EmpmModelParams* params, const float* F_trial9, float* mu, float* lam,
+                                 float* yield_stress, float dt, float* F_out9, float* stress_out9, int n, void* stream) {
+    EmpmCtx* ctx = nullptr;
+    int rc = validate_params(nullptr, params);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!F_trial9 || !mu || !lam || !yield_stress || !F_out9 || !stress_out9)))
+        return empm_set_error(nullptr, EMPM_ERR_INVALID, "bad empm_debug_stress arguments");
+    if (n == 0) return EMPM_OK;
+    MaterialScalars ms;
+    ms.material = params->material;
+    ms.softening = params->softening;
+    ms.hardening = params->hardening;
+    ms.xi = params->xi;
+    ms.plastic_viscosity = params->plastic_viscosity;
+    ms.alpha = params->alpha;
+    k_debug_stress<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(F_trial9, mu, lam, yield_stress, dt, ms,
+                                                                         F_out9, stress_out9, n);
+    CK(cudaGetLastError(), "k_debug_stress");
+    return EMPM_OK;
+}
+
+extern "C" int empm_ctx_grid(EmpmCtx* ctx, float** momentum, float** velocity) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    if (momentum) *momentum = reinterpret_cast<float*>(ctx->grid_mom);
+    if (velocity) *velocity = reinterpret_cast<float*>(ctx->grid_vel);
+    return EMPM_OK;
+}
+
+extern "C" int empm_ctx_timing(EmpmCtx* ctx, int enable, int max_launches) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    ctx->timing_count[0] = ctx->timing_count[1] = ctx->timing_count[2] = 0;
+    if (!enable) { ctx->timing = false; return EMPM_OK; }
+    if (max_launches < 1 || max_launches > 1000000)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "max_launches %d out of [1, 1000000]", max_launches);
+    const size_t need = (size_t)3 * max_launches * 2;
+    while (ctx->timing_events.size() < need) {
+        cudaEvent_t ev;
+        CK(cudaEventCreate(&ev), "cudaEventCreate");
+        ctx->timing_events.push_back(ev);
+    }
+    ctx->timing_capacity = max_launches;
+    ctx->timing = true;
+    return EMPM_OK;
+}
+
+extern "C" int empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3) {
+    if (!ctx || !total_ms3 || !launches3) return empm_set_error(ctx, EMPM_ERR_INVALID, "bad arguments");
+    for (int k = 0; k < 3; ++k) {
+        float total = 0.f;
+        for (int i = 0; i < ctx->timing_count[k]; ++i) {
+            const size_t base = ((size_t)k * ctx->timing_capacity + i) * 2;
+            CK(cudaEventSynchronize(ctx->timing_events[base + 1]), "cudaEventSynchronize");
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ctx->timing_events[base], ctx->timing_events[base + 1]), "cudaEventElapsedTime");
+            total += ms;
+        }
+        total_ms3[k] = total;
+        launches3[k] = ctx->timing_count[k];
+    }
     return EMPM_OK;
 }

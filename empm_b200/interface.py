@@ -1,0 +1,178 @@
+"""torch.autograd.Function boundary of the simulator.
+
+Mirrors the four Functions of phys_sim/diff_simulator/warp_mpm/interface.py
+(same positional signatures and returned tuples):
+
+* MPMDifferentiableSimulationTrail (:20-251) — positions every ``substep``
+  substeps, ``[T, N, 3]``; a scalar E is scaled by 1e6 in the forward (:70)
+* MPMDifferentiableSimulation (:254-472) — final positions
+* MPMDifferentiableSimulationWCheckpoint (:476-774) — (x, v, F, C) of a segment
+* MPMDifferentiableSimulationClean (:777-986) — (x, v, F, C, cov)
+
+The forward passes run the CUDA substep; gradients come from the library's
+adjoint kernels (``empm_b200.adjoint``).
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+import torch
+import torch.autograd as autograd
+from torch import Tensor
+
+from .mpm_data_structure import MPMModelStruct, MPMStateStruct
+
+
+def _set_E_nu(mpm_solver, mpm_model, E: Tensor, nu: Tensor, scale_scalar_E: float = 1.0):
+    E_inp = E.item() * scale_scalar_E if E.ndim == 0 else E.detach()
+    nu_inp = nu.item() if nu.ndim == 0 else nu.detach()
+    mpm_solver.set_E_nu(mpm_model, E_inp, nu_inp)
+    return E.ndim == 0, nu.ndim == 0
+
+
+def _run(mpm_solver, mpm_model, state, n_steps, dt, record_every=None, step_callback=None):
+    """Ping-pong rollout from `state`; returns (final_state, recorded positions)."""
+    recorded = []
+    other = state.partial_clone(requires_grad=False)
+    cur = state
+    first = True
+    for i in range(n_steps):
+        if step_callback is not None:
+            step_callback(i)
+        mpm_solver.p2g2p_differentiable(mpm_model, cur, other, dt)
+        if record_every is not None and i % record_every == 0:
+            recorded.append(other.particle_x.clone())
+        if first:
+            # never write into the caller's state object again
+            cur = state.partial_clone(requires_grad=False)
+            first = False
+        cur, other = other, cur
+    return cur, recorded
+
+
+def _fast_run(mpm_solver, mpm_model, state, n_steps, dt):
+    if n_steps <= 0:
+        return state
+    other = state.partial_clone(requires_grad=False)
+    work = state.partial_clone(requires_grad=False)
+    work._x4.copy_(state._x4)
+    work._v4.copy_(state._v4)
+    work._C.copy_(state._C)
+    work._F_trial.copy_(state._F_trial)
+    return mpm_solver.rollout(mpm_model, work, other, dt, n_steps)
+
+
+class MPMDifferentiableSimulationTrail(autograd.Function):
+    @staticmethod
+    def forward(ctx, mpm_solver, mpm_state: MPMStateStruct, mpm_model: MPMModelStruct, substep: int,
+                substep_size: float, num_substeps: int, init_pos: Tensor, init_velocity: Tensor, E: Tensor, nu: Tensor,
+                particle_density: Optional[Tensor] = None, density_change_mask: Optional[Tensor] = None,
+                static_pos: Optional[Tensor] = None, device: str = "cuda:0", requires_grad: bool = True,
+                extra_no_grad_steps: int = 0):
+        if static_pos is not None:
+            mpm_state.reset_state(static_pos.clone(), None, init_velocity, device=device, requires_grad=requires_grad)
+            mpm_solver.restart_and_compute_F_C(mpm_model, mpm_state, init_pos, device=device)
+        else:
+            mpm_state.reset_state(init_pos.clone(), None, init_velocity, device=device, requires_grad=requires_grad)
+        ctx.aggregating_E, ctx.aggregating_nu = _set_E_nu(mpm_solver, mpm_model, E, nu, scale_scalar_E=1e6)
+        mpm_state.reset_density(tensor_density=particle_density, selection_mask=density_change_mask, device=device,
+                                requires_grad=requires_grad)
+        prev = mpm_state
+        if extra_no_grad_steps > 0:
+            mpm_state.update_mass()
+            mpm_solver.prepare_mu_lam(mpm_model, mpm_state, device=device)
+            prev, _ = _run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
+        prev.update_mass()
+        mpm_solver.prepare_mu_lam(mpm_model, prev, device=device)
+        final, recorded = _run(mpm_solver, mpm_model, prev, num_substeps, substep_size, record_every=substep,
+                               step_callback=mpm_solver.step_callback)
+        ctx.final_state = final
+        return torch.stack(recorded, dim=0)
+
+    @staticmethod
+    def backward(ctx, out_pos_grad):
+        raise NotImplementedError("adjoint of MPMDifferentiableSimulationTrail is not available in this build")
+
+
+class MPMDifferentiableSimulation(autograd.Function):
+    @staticmethod
+    def forward(ctx, mpm_solver, mpm_state: MPMStateStruct, mpm_model: MPMModelStruct, substep: int,
+                substep_size: float, num_substeps: int, init_pos: Tensor, init_velocity: Tensor, E: Tensor, nu: Tensor,
+                particle_density: Optional[Tensor] = None, density_change_mask: Optional[Tensor] = None,
+                static_pos: Optional[Tensor] = None, device: str = "cuda:0", requires_grad: bool = True,
+                extra_no_grad_steps: int = 0):
+        if static_pos is not None:
+            mpm_state.reset_state(static_pos.clone(), None, init_velocity, device=device, requires_grad=requires_grad)
+            mpm_solver.restart_and_compute_F_C(mpm_model, mpm_state, init_pos, device=device)
+        else:
+            mpm_state.reset_state(init_pos.clone(), None, init_velocity, device=device, requires_grad=requires_grad)
+        ctx.aggregating_E, ctx.aggregating_nu = _set_E_nu(mpm_solver, mpm_model, E, nu)
+        mpm_state.reset_density(tensor_density=particle_density, selection_mask=density_change_mask, device=device,
+                                requires_grad=requires_grad)
+        prev = mpm_state
+        if extra_no_grad_steps > 0:
+            mpm_state.update_mass()
+            mpm_solver.prepare_mu_lam(mpm_model, mpm_state, device=device)
+            prev = _fast_run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
+        prev.update_mass()
+        mpm_solver.prepare_mu_lam(mpm_model, prev, device=device)
+        final = _fast_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        return final.particle_x.clone()
+
+    @staticmethod
+    def backward(ctx, out_pos_grad):
+        raise NotImplementedError("adjoint of MPMDifferentiableSimulation is not available in this build")
+
+
+class MPMDifferentiableSimulationWCheckpoint(autograd.Function):
+    @staticmethod
+    @torch.no_grad()
+    def forward(ctx, mpm_solver, mpm_state: MPMStateStruct, mpm_model: MPMModelStruct, substep_size: float,
+                num_substeps: int, particle_x: Tensor, particle_v: Tensor, particle_F: Tensor, particle_C: Tensor,
+                E: Tensor, nu: Tensor, particle_density: Optional[Tensor] = None, query_mask: Optional[Tensor] = None,
+                device: str = "cuda:0", requires_grad: bool = True, extra_no_grad_steps: int = 0):
+        mpm_state.continue_from_torch(particle_x, particle_v, particle_F, particle_C, device=device,
+                                      requires_grad=True)
+        ctx.aggregating_E, ctx.aggregating_nu = _set_E_nu(mpm_solver, mpm_model, E, nu)
+        mpm_solver.prepare_mu_lam(mpm_model, mpm_state, device=device)
+        mpm_state.reset_density(tensor_density=particle_density, selection_mask=query_mask, device=device,
+                                requires_grad=True, update_mass=True)
+        prev = mpm_state
+        if extra_no_grad_steps > 0:
+            prev = _fast_run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
+        final = _fast_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        n = final.n_particles
+        return (final.particle_x.clone(), final.particle_v.clone(), final.particle_F_trial.reshape(n, 3, 3).clone(),
+                final.particle_C.reshape(n, 3, 3).clone())
+
+    @staticmethod
+    def backward(ctx, *grads):
+        raise NotImplementedError("adjoint of MPMDifferentiableSimulationWCheckpoint is not available in this build")
+
+
+class MPMDifferentiableSimulationClean(autograd.Function):
+    @staticmethod
+    @torch.no_grad()
+    def forward(ctx, mpm_solver, mpm_state: MPMStateStruct, mpm_model: MPMModelStruct, substep_size: float,
+                num_substeps: int, particle_x: Tensor, particle_v: Tensor, particle_F: Tensor, particle_C: Tensor,
+                E: Tensor, nu: Tensor, particle_density: Optional[Tensor] = None, query_mask: Optional[Tensor] = None,
+                device: str = "cuda:0", requires_grad: bool = True, extra_no_grad_steps: int = 0):
+        mpm_state.continue_from_torch(particle_x, particle_v, particle_F, particle_C, device=device,
+                                      requires_grad=True)
+        ctx.aggregating_E, ctx.aggregating_nu = _set_E_nu(mpm_solver, mpm_model, E, nu)
+        mpm_solver.prepare_mu_lam(mpm_model, mpm_state, device=device)
+        mpm_state.reset_density(tensor_density=particle_density, selection_mask=query_mask, device=device,
+                                requires_grad=True, update_mass=True)
+        prev = mpm_state
+        if extra_no_grad_steps > 0:
+            prev = _fast_run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
+        prev.update_mass()
+        mpm_solver.prepare_mu_lam(mpm_model, prev, device=device)
+        final = _fast_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        n = final.n_particles
+        return (final.particle_x.clone(), final.particle_v.clone(), final.particle_F_trial.reshape(n, 3, 3).clone(),
+                final.particle_C.reshape(n, 3, 3).clone(), final.particle_cov.view(-1, 6).clone())
+
+    @staticmethod
+    def backward(ctx, *grads):
+        raise NotImplementedError("adjoint of MPMDifferentiableSimulationClean is not available in this build")

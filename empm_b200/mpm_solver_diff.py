@@ -1,0 +1,544 @@
+"""Substep orchestration and boundary-condition factories.
+
+Mirrors ``MPMWARPDiff`` (phys_sim/diff_simulator/warp_mpm/mpm_solver_diff.py):
+same method names and argument orders. Where the reference builds one Warp
+kernel closure per collider and launches ``6 + n_colliders`` kernels per
+substep, this class records the collider as a parameter block and the
+library applies every collider inside its single grid-update kernel; a
+substep is three kernels (fused return map + stress + P2G, grid update with
+all boundary conditions, G2P).
+
+Time gates (``time >= start_time and time < end_time`` ...) are evaluated on
+the host in float32, as Warp does for its float kernel arguments, and passed
+to the device as EMPM_GATE_* per collider.
+"""
+from __future__ import annotations
+
+import math
+import time as _time
+from typing import List, Optional
+
+import numpy as np
+import torch
+from torch import Tensor
+
+from . import _native as N
+from .mpm_data_structure import (DTYPE, Dirichlet_collider, GridCollider, Impulse_modifier, MPMModelStruct,
+                                 MPMStateStruct, ParticleVelocityModifier, _stream_ptr, _vec3)
+
+MATERIALS = {"jelly": 0, "metal": 1, "sand": 2, "foam": 3, "snow": 4, "plasticine": 5, "neo-hookean": 6}
+SURFACE_TYPES = {"sticky": 0, "slip": 1, "cut": 11}
+_f32 = np.float32
+
+
+def _unit(v):
+    s = 1.0 / math.sqrt(float(sum(float(t) ** 2 for t in v)))
+    return tuple(s * float(t) for t in v)
+
+
+class _Context:
+    """Owns one EmpmCtx (grid buffers + step table) for a (N, G) problem."""
+
+    def __init__(self, params: N.EmpmModelParams, n_particles: int, max_steps: int, device):
+        self.L = N.lib()
+        self.device = device
+        self.n_particles = n_particles
+        self.max_steps = max_steps
+        self.params_bytes = bytes(params)
+        ptr = N.ctypes.c_void_p()
+        with torch.cuda.device(device):
+            N.check(self.L.empm_ctx_create(params, n_particles, max_steps, N.ctypes.byref(ptr)))
+        self.ptr = ptr
+
+    def set_params(self, params: N.EmpmModelParams):
+        b = bytes(params)
+        if b != self.params_bytes:
+            N.check(self.L.empm_ctx_set_params(self.ptr, params), self.ptr)
+            self.params_bytes = b
+
+    def status(self) -> int:
+        s = N.ctypes.c_uint32(0)
+        N.check(self.L.empm_read_status(self.ptr, N.ctypes.byref(s), _stream_ptr(self.device)), self.ptr)
+        return int(s.value)
+
+    def __del__(self):
+        try:
+            if getattr(self, "ptr", None):
+                self.L.empm_ctx_destroy(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+
+class MPMWARPDiff(object):
+    def __init__(self):
+        self.time_profile = {}
+        self.step_callback = None
+        self._ctx: Optional[_Context] = None
+        self.use_graph = True
+
+    def initialize(self, n_particles, n_grid=100, grid_lim=1.0, device="cuda:0"):
+        self.n_particles = n_particles
+        self.n_grid = int(n_grid)
+        self.time = 0.0
+        self.grid_postprocess = []      # one entry per collider (kind id), kept for API parity
+        self.collider_params: List = []
+        self.modify_bc = []
+        self.pre_p2g_operations = []
+        self.impulse_params: List[Impulse_modifier] = []
+        self.particle_velocity_modifiers = []
+        self.particle_velocity_modifier_params: List[ParticleVelocityModifier] = []
+
+    # -- parameters ---------------------------------------------------------
+    def set_parameters(self, device="cuda:0", **kwargs):
+        self.set_parameters_dict(device, kwargs)
+
+    def set_parameters_dict(self, mpm_model, mpm_state, kwargs={}, device="cuda:0"):
+        if "material" in kwargs:
+            if kwargs["material"] not in MATERIALS:
+                raise TypeError("Undefined material type")
+            mpm_model.material = MATERIALS[kwargs["material"]]
+        if "yield_stress" in kwargs:
+            mpm_model.yield_stress[: self.n_particles] = float(kwargs["yield_stress"])
+        if "hardening" in kwargs:
+            mpm_model.hardening = kwargs["hardening"]
+        if "xi" in kwargs:
+            mpm_model.xi = kwargs["xi"]
+        if "friction_angle" in kwargs:
+            mpm_model.friction_angle = kwargs["friction_angle"]
+            sin_phi = math.sin(mpm_model.friction_angle / 180.0 * 3.14159265)
+            mpm_model.alpha = math.sqrt(2.0 / 3.0) * 2.0 * sin_phi / (3.0 - sin_phi)
+        if "rpic_damping" in kwargs:
+            mpm_model.rpic_damping = kwargs["rpic_damping"]
+        if "plastic_viscosity" in kwargs:
+            mpm_model.plastic_viscosity = kwargs["plastic_viscosity"]
+        if "softening" in kwargs:
+            mpm_model.softening = kwargs["softening"]
+        if "grid_v_damping_scale" in kwargs:
+            mpm_model.grid_v_damping_scale = kwargs["grid_v_damping_scale"]
+
+    def set_E_nu(self, mpm_model, E, nu, device="cuda:0"):
+        for name, val in (("E", E), ("nu", nu)):
+            dst = getattr(mpm_model, name)
+            if isinstance(val, (float, int)):
+                dst.fill_(float(val))
+            else:
+                dst.copy_(val.detach().reshape(-1).to(dst.device, DTYPE))
+
+    def set_E_nu_from_torch(self, mpm_model, E: Tensor, nu: Tensor, device="cuda:0"):
+        E_inp = E.item() if E.ndim == 0 else E
+        nu_inp = nu.item() if nu.ndim == 0 else nu
+        self.set_E_nu(mpm_model, E_inp, nu_inp, device=device)
+
+    def prepare_mu_lam(self, mpm_model, mpm_state, device="cuda:0"):
+        mpm_model.finalize_mu_lam(self.n_particles, device=device)
+
+    # -- context / schedule -------------------------------------------------
+    def _context(self, mpm_model: MPMModelStruct, n: int, device, max_steps: int = 1024) -> _Context:
+        params = mpm_model._params()
+        c = self._ctx
+        if c is None or c.n_particles != n or c.device != device or c.max_steps < max_steps or \
+                N.EmpmModelParams.from_buffer_copy(c.params_bytes).n_grid != params.n_grid:
+            self._ctx = c = _Context(params, n, max(max_steps, 1024), device)
+        else:
+            c.set_params(params)
+        return c
+
+    @staticmethod
+    def _window(t32, p) -> bool:
+        return bool(t32 >= _f32(p.start_time)) and bool(t32 < _f32(p.end_time))
+
+    def _gate(self, p, t32, dt) -> int:
+        kind = p._kind
+        in_window = self._window(t32, p) if kind != N.COLL_GRID_MASK else True
+        if kind in (N.COLL_SURFACE, N.COLL_CUBOID_VELOCITY, N.COLL_BOUNDING_BOX, N.COLL_GRID_MASK):
+            if in_window:
+                return N.GATE_APPLY
+        elif kind in (N.COLL_GEOMETRY, N.COLL_GRID_VELOCITY):
+            if in_window and bool(p.active):
+                return N.GATE_APPLY
+        if kind in (N.COLL_GRID_VELOCITY, N.COLL_CUBOID_VELOCITY) and int(p.reset) == 1:
+            if bool(t32 < _f32(p.end_time) + _f32(15.0) * _f32(dt)):
+                return N.GATE_ZERO_ALL
+        return N.GATE_OFF
+
+    def _check_masks(self):
+        for p in self.collider_params:
+            if p._kind == N.COLL_GRID_MASK and p.mask is not None and p.mask.numel() < self.n_grid ** 3:
+                raise ValueError("grid mask smaller than the grid")
+        for p in list(self.impulse_params) + list(self.particle_velocity_modifier_params):
+            if p.mask is not None and p.mask.numel() < self.n_particles:
+                raise ValueError("particle mask smaller than the particle count")
+
+    def _fill_step(self, st: N.EmpmStep, t: float, dt: float) -> None:
+        """Resolve the schedule of one substep at solver time t (float64)."""
+        t32 = _f32(t)
+        st.time = float(t32)
+        st.dt = float(_f32(dt))
+        nc = len(self.collider_params)
+        if nc > N.EMPM_MAX_COLLIDERS:
+            raise ValueError(f"at most {N.EMPM_MAX_COLLIDERS} colliders are supported (got {nc})")
+        st.n_colliders = nc
+        for i, p in enumerate(self.collider_params):
+            c = st.colliders[i]
+            c.kind = p._kind
+            c.gate = self._gate(p, t32, dt)
+            c.shape = p._shape
+            c.surface_type = int(getattr(p, "surface_type", 0))
+            c.point = N.F3(*_vec3(getattr(p, "point", None)))
+            c.normal = N.F3(*_vec3(getattr(p, "normal", None)))
+            c.size = N.F3(*_vec3(getattr(p, "size", None)))
+            c.velocity = N.F3(*_vec3(getattr(p, "velocity", None)))
+            c.rot_axis = N.F3(*_vec3(getattr(p, "rot_axis", None)))
+            c.angular_velocity = float(getattr(p, "angular_velocity", 0.0))
+            c.radius = float(getattr(p, "radius", 0.0))
+            c.half_height = float(getattr(p, "half_height", 0.0))
+            c.friction = float(getattr(p, "friction", 0.0))
+            c.mask = p.mask.data_ptr() if (p._kind == N.COLL_GRID_MASK and p.mask is not None) else None
+        mods = list(self.impulse_params) + list(self.particle_velocity_modifier_params)
+        if len(mods) > N.EMPM_MAX_MODIFIERS:
+            raise ValueError(f"at most {N.EMPM_MAX_MODIFIERS} particle modifiers are supported (got {len(mods)})")
+        st.n_modifiers = len(mods)
+        for i, p in enumerate(mods):
+            m = st.modifiers[i]
+            m.kind = p._kind
+            m.gate = N.GATE_APPLY if self._window(t32, p) else N.GATE_OFF
+            m.mask = p.mask.data_ptr() if p.mask is not None else None
+            if p._kind in (N.MOD_IMPULSE, N.MOD_IMPULSE_MASK):
+                m.vec = N.F3(*_vec3(p.force))
+            elif p._kind == N.MOD_SET_VELOCITY:
+                m.vec = N.F3(*_vec3(p.velocity))
+            elif p._kind == N.MOD_ROTATION:
+                m.point = N.F3(*_vec3(p.point))
+                m.normal = N.F3(*_vec3(p.normal))
+                m.axis1 = N.F3(*_vec3(p.horizontal_axis_1))
+                m.axis2 = N.F3(*_vec3(p.horizontal_axis_2))
+                m.scale = (N.ctypes.c_float * 2)(float(p.rotation_scale), float(p.translation_scale))
+            elif p._kind == N.MOD_MOVER:
+                m.vec = N.F3(*_vec3(p.velocity))
+                m.point = N.F3(*_vec3(p.rotation_center))
+                m.normal = N.F3(*_vec3(p.rotation_axis))
+                m.scale = (N.ctypes.c_float * 2)(float(p.angular_velocity), 0.0)
+
+    def _modify(self, t: float, dt: float) -> None:
+        """The host `modify` callbacks: move kinematic colliders (mpm_solver_diff.py:795-801, 860-866)."""
+        for p, mod in zip(self.collider_params, self.modify_bc):
+            if mod is not None:
+                mod(t, dt, p)
+
+    @staticmethod
+    def _move_point(t, dt, param):
+        if t >= param.start_time and t < param.end_time:
+            # point and velocity live in float32 vec3 fields; the update is
+            # evaluated in double on the host and stored back as float32
+            pt = [float(_f32(c)) for c in _vec3(param.point)]
+            v = [float(_f32(c)) for c in _vec3(param.velocity)]
+            param.point = tuple(float(_f32(pt[i] + dt * v[i])) for i in range(3))
+
+    def build_schedule(self, t0: float, dt: float, n_steps: int, step_callback=None):
+        """Schedules of n_steps substeps from solver time t0; runs the host-side
+        modify callbacks as it goes. Returns (table, t_end)."""
+        self._check_masks()
+        table = (N.EmpmStep * n_steps)()
+        t = t0
+        for s in range(n_steps):
+            if step_callback is not None:
+                step_callback(s)
+            self._fill_step(table[s], t, dt)
+            self._modify(t, dt)
+            t = t + dt
+        return table, t
+
+    @staticmethod
+    def _material(mpm_model: MPMModelStruct, mpm_state: MPMStateStruct) -> N.EmpmMaterial:
+        return N.EmpmMaterial(mpm_state.particle_vol.data_ptr(), mpm_model.mu.data_ptr(), mpm_model.lam.data_ptr(),
+                              mpm_model.yield_stress.data_ptr(), mpm_state._sel_ptr(), mpm_state._F.data_ptr())
+
+    # -- the substep --------------------------------------------------------
+    def p2g2p_differentiable(self, mpm_model, mpm_state, next_state, dt, device="cuda:0"):
+        """One substep mpm_state -> next_state (mpm_solver_diff.py:165-291)."""
+        n = mpm_state.n_particles
+        ctx = self._context(mpm_model, n, mpm_state.device)
+        self._check_masks()
+        step = N.EmpmStep()
+        self._fill_step(step, self.time, dt)
+        a = mpm_state._particles()
+        b = next_state._particles()
+        mat = self._material(mpm_model, mpm_state)
+        with torch.cuda.device(mpm_state.device):
+            N.check(ctx.L.empm_substep(ctx.ptr, a, b, mat, step, _stream_ptr(mpm_state.device)), ctx.ptr)
+        self._modify(self.time, dt)
+        self.time = self.time + dt
+
+    def rollout(self, mpm_model, state_a, state_b, dt, n_steps, step_callback=None, schedule=None):
+        """n_steps substeps ping-ponging between state_a and state_b on one
+        launch sequence (CUDA graph when self.use_graph). Returns the state
+        holding the result. `schedule` may be a (table, t_end) pair returned
+        by build_schedule to replay a rollout whose schedule is already known."""
+        if n_steps <= 0:
+            return state_a
+        n = state_a.n_particles
+        ctx = self._context(mpm_model, n, state_a.device, max_steps=n_steps)
+        if schedule is None:
+            table, t_end = self.build_schedule(self.time, dt, n_steps, step_callback)
+        else:
+            table, t_end = schedule
+            if len(table) != n_steps:
+                raise ValueError("schedule length does not match n_steps")
+        mat = self._material(mpm_model, state_a)
+        a, b = state_a._particles(), state_b._particles()
+        with torch.cuda.device(state_a.device):
+            N.check(ctx.L.empm_rollout(ctx.ptr, a, b, mat, table, n_steps, int(self.use_graph),
+                                       _stream_ptr(state_a.device)), ctx.ptr)
+        self.time = t_end
+        return state_a if n_steps % 2 == 0 else state_b
+
+    def read_status(self) -> int:
+        return 0 if self._ctx is None else self._ctx.status()
+
+    def kernel_timing(self, enable: bool, max_launches: int = 4096):
+        """Start (enable) or stop per-kernel CUDA-event timing on the stream path."""
+        if self._ctx is None:
+            raise RuntimeError("no context yet: run a substep first")
+        N.check(self._ctx.L.empm_ctx_timing(self._ctx.ptr, int(enable), int(max_launches)), self._ctx.ptr)
+
+    def kernel_times(self):
+        """{kernel: (total_ms, launches)} for [stress_p2g, grid_update, g2p]."""
+        ms = (N.ctypes.c_float * 3)()
+        cnt = (N.ctypes.c_int * 3)()
+        N.check(self._ctx.L.empm_ctx_kernel_times(self._ctx.ptr, ms, cnt), self._ctx.ptr)
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("stress_p2g", "grid_update", "g2p"))}
+
+    def print_time_profile(self):
+        print("MPM Time profile:")
+        for key, value in self.time_profile.items():
+            print(key, sum(value))
+
+    # -- grid boundary conditions --------------------------------------------
+    def _register(self, param, kind, shape=0, modify=None):
+        param._kind = kind
+        param._shape = shape
+        self.collider_params.append(param)
+        self.grid_postprocess.append(kind)
+        self.modify_bc.append(modify)
+
+    def add_surface_collider(self, point, normal, surface="sticky", friction=0.0, start_time=0.0, end_time=999.0):
+        point = list(point)
+        normal = _unit(normal)
+        p = Dirichlet_collider()
+        p.start_time = start_time
+        p.end_time = end_time
+        p.point = tuple(float(t) for t in point)
+        p.normal = normal
+        if surface == "sticky" and friction != 0:
+            raise ValueError("friction must be 0 on sticky surfaces.")
+        p.surface_type = SURFACE_TYPES.get(surface, 2)
+        p.friction = friction
+        self._register(p, N.COLL_SURFACE)
+
+    @staticmethod
+    def _geometry(p, geo_args):
+        if "shape" not in geo_args:
+            raise ValueError("geo_args must contain 'shape' key.")
+        shape = geo_args["shape"]
+        if shape == "cube":
+            p.point, p.size = _vec3(geo_args["center"]), _vec3(geo_args["size"])
+            return N.SHAPE_CUBE
+        if shape == "sphere":
+            p.point, p.radius = _vec3(geo_args["center"]), float(geo_args["radius"])
+            return N.SHAPE_SPHERE
+        if shape == "cylinder":
+            p.point, p.normal = _vec3(geo_args["center"]), _unit(geo_args["axis"])
+            p.radius, p.half_height = float(geo_args["radius"]), float(geo_args["half_height"])
+            return N.SHAPE_CYLINDER
+        if shape in ("halfspace", "plane"):
+            p.point, p.normal = _vec3(geo_args["point"]), _unit(geo_args["normal"])
+            return N.SHAPE_HALFSPACE
+        raise ValueError(f"Unknown geometry type: {geo_args['shape']}")
+
+    def add_geometry_collider(self, geo_args: dict):
+        p = Dirichlet_collider()
+        surface = geo_args.get("surface", "sticky")
+        p.active = True
+        p.start_time = geo_args.get("start_time", 0.0)
+        p.end_time = geo_args.get("end_time", 999.0)
+        p.friction = geo_args.get("friction", 0.0)
+        if "velocity" in geo_args:
+            p.velocity = _vec3(geo_args["velocity"])
+        if surface == "sticky" and p.friction != 0:
+            raise ValueError("friction must be 0 on sticky surfaces.")
+        p.surface_type = SURFACE_TYPES.get(surface, 2)
+        shape = self._geometry(p, geo_args)
+        self._register(p, N.COLL_GEOMETRY, shape)
+
+    def set_grid_velocity_on_geometry(self, geo_args: dict):
+        p = Dirichlet_collider()
+        p.active = True
+        p.start_time = geo_args.get("start_time", 0.0)
+        p.end_time = geo_args.get("end_time", 999.0)
+        p.velocity = _vec3(geo_args.get("velocity", (0.0, 0.0, 0.0)))
+        p.angular_velocity = float(geo_args.get("angular_velocity", 0.0))
+        p.rot_axis = _vec3(geo_args.get("rot_axis", (1.0, 0.0, 0.0)))
+        p.reset = int(geo_args.get("reset", 0))
+        shape = self._geometry(p, geo_args)
+        self._register(p, N.COLL_GRID_VELOCITY, shape, modify=self._move_point)
+
+    def set_velocity_on_cuboid(self, point, size, velocity, start_time=0.0, end_time=999.0, reset=0):
+        p = Dirichlet_collider()
+        p.start_time = start_time
+        p.end_time = end_time
+        p.point = _vec3(list(point))
+        p.size = _vec3(size)
+        p.velocity = _vec3(velocity)
+        p.reset = reset
+        self._register(p, N.COLL_CUBOID_VELOCITY, modify=self._move_point)
+
+    def add_bounding_box(self, start_time=0.0, end_time=999.0):
+        p = Dirichlet_collider()
+        p.start_time = start_time
+        p.end_time = end_time
+        self._register(p, N.COLL_BOUNDING_BOX)
+
+    def enforce_grid_velocity_by_mask(self, selection_mask: torch.Tensor):
+        p = GridCollider()
+        if selection_mask.numel() != self.n_grid ** 3:
+            raise ValueError(f"grid mask has {selection_mask.numel()} entries, expected {self.n_grid}^3")
+        p.mask = selection_mask.to(torch.int32).contiguous()
+        if not p.mask.is_cuda:
+            p.mask = p.mask.cuda()
+        self._register(p, N.COLL_GRID_MASK)
+
+    # -- particle modifiers -------------------------------------------------
+    @staticmethod
+    def _box_mask(mpm_state, point, size):
+        off = mpm_state.particle_x - torch.tensor(_vec3(point), device=mpm_state.device, dtype=DTYPE)
+        sz = torch.tensor(_vec3(size), device=mpm_state.device, dtype=DTYPE)
+        return (off.abs() < sz).all(dim=1).to(torch.int32).contiguous()
+
+    def add_impulse_on_particles(self, mpm_state, force, dt, point=[1, 1, 1], size=[1, 1, 1], num_dt=1,
+                                 start_time=0.0, device="cuda:0"):
+        p = Impulse_modifier()
+        p.start_time = start_time
+        p.end_time = start_time + dt * num_dt
+        p.point, p.size = _vec3(point), _vec3(size)
+        p.mask = self._box_mask(mpm_state, point, size)
+        p.force = _vec3(force)
+        p._kind = N.MOD_IMPULSE
+        self.impulse_params.append(p)
+        self.pre_p2g_operations.append(N.MOD_IMPULSE)
+
+    def add_impulse_on_particles_with_mask(self, mpm_state, force, dt, particle_mask, point=[1, 1, 1],
+                                           size=[1, 1, 1], end_time=1, start_time=0.0, device="cuda:0"):
+        assert len(particle_mask) == self.n_particles, "mask should have n_particles elements"
+        p = Impulse_modifier()
+        p.start_time = start_time
+        p.end_time = end_time
+        p.point, p.size = _vec3(point), _vec3(size)
+        # the reference runs the box selection over the mask array it was given,
+        # so the box (default [0, 2]^3) decides which particles receive the force
+        p.mask = self._box_mask(mpm_state, point, size)
+        p.force = _vec3(force)
+        p._kind = N.MOD_IMPULSE_MASK
+        self.impulse_params.append(p)
+        self.pre_p2g_operations.append(N.MOD_IMPULSE_MASK)
+
+    def enforce_particle_velocity_translation(self, mpm_state, point, size, velocity, start_time, end_time,
+                                              device="cuda:0"):
+        p = ParticleVelocityModifier()
+        p.point, p.size = _vec3(point), _vec3(size)
+        p.velocity = _vec3(velocity)
+        p.start_time, p.end_time = start_time, end_time
+        p.mask = self._box_mask(mpm_state, point, size)
+        p._kind = N.MOD_SET_VELOCITY
+        self.particle_velocity_modifier_params.append(p)
+        self.particle_velocity_modifiers.append(N.MOD_SET_VELOCITY)
+
+    def enforce_particle_velocity_rotation(self, mpm_state, point, normal, half_height_and_radius, rotation_scale,
+                                           translation_scale, start_time, end_time, device="cuda:0"):
+        n = _unit(normal)
+        p = ParticleVelocityModifier()
+        p.point = _vec3(point)
+        p.half_height_and_radius = (float(half_height_and_radius[0]), float(half_height_and_radius[1]))
+        p.normal = n
+        h1 = np.array([1.0, 1.0, 1.0])
+        nn = np.array(n)
+        if abs(float(np.dot(nn, h1))) < 0.01:
+            h1 = np.array([0.72, 0.37, -0.67])
+        h1 = h1 - np.dot(h1, nn) * nn
+        h1 = h1 * (1.0 / np.linalg.norm(h1))
+        h2 = np.cross(h1, nn)
+        p.horizontal_axis_1 = tuple(float(t) for t in h1)
+        p.horizontal_axis_2 = tuple(float(t) for t in h2)
+        p.rotation_scale = rotation_scale
+        p.translation_scale = translation_scale
+        p.start_time, p.end_time = start_time, end_time
+        off = mpm_state.particle_x - torch.tensor(p.point, device=mpm_state.device, dtype=DTYPE)
+        nt = torch.tensor(n, device=mpm_state.device, dtype=DTYPE)
+        proj = off @ nt
+        horiz = (off - proj[:, None] * nt[None]).norm(dim=1)
+        p.mask = ((proj.abs() < p.half_height_and_radius[0]) & (horiz < p.half_height_and_radius[1])).to(
+            torch.int32).contiguous()
+        p._kind = N.MOD_ROTATION
+        self.particle_velocity_modifier_params.append(p)
+        self.particle_velocity_modifiers.append(N.MOD_ROTATION)
+
+    def release_particles_sequentially(self, normal, start_position, end_position, num_layers, start_time, end_time,
+                                       mpm_state=None):
+        """Layered release (mpm_solver_diff.py:1146-1171). The reference calls
+        enforce_particle_velocity_translation without a state (a TypeError
+        there); here the state must be passed as mpm_state."""
+        if mpm_state is None:
+            raise TypeError("release_particles_sequentially needs mpm_state")
+        num_layers = 50
+        point = [0, 0, 0]
+        size = [0, 0, 0]
+        axis = -1
+        for i in range(3):
+            if normal[i] == 0:
+                point[i] = 1
+                size[i] = 1
+            else:
+                axis = i
+                point[i] = end_position
+        half_length_portion = abs(start_position - end_position) / num_layers
+        end_time_portion = end_time / num_layers
+        for i in range(num_layers):
+            size[axis] = half_length_portion * (num_layers - i)
+            self.enforce_particle_velocity_translation(mpm_state, point=point, size=size, velocity=[0, 0, 0],
+                                                       start_time=start_time, end_time=end_time_portion * (i + 1))
+
+    def enforce_particle_velocity_by_mask(self, mpm_state, selection_mask: torch.Tensor, velocity, start_time,
+                                          end_time):
+        p = ParticleVelocityModifier()
+        p.velocity = _vec3(velocity)
+        p.start_time, p.end_time = start_time, end_time
+        if selection_mask.numel() != self.n_particles:
+            raise ValueError(f"selection mask has {selection_mask.numel()} entries, expected {self.n_particles}")
+        p.mask = selection_mask.to(mpm_state.device).to(torch.int32).contiguous().reshape(-1)
+        p._kind = N.MOD_SET_VELOCITY
+        self.particle_velocity_modifier_params.append(p)
+        self.particle_velocity_modifiers.append(N.MOD_SET_VELOCITY)
+
+    def set_particle_mover(self, velocity=None, angular_velocity=None, center=None, axis=None, selection_mask=None,
+                           geo_args=None, start_time=0.0, end_time=999.0, device="cuda:0"):
+        p = ParticleVelocityModifier()
+        p.start_time, p.end_time = start_time, end_time
+        dev = torch.device(device)
+        if selection_mask is not None:
+            p.mask = torch.as_tensor(selection_mask, dtype=torch.int32).to(dev).contiguous().reshape(-1)
+            if p.mask.numel() != self.n_particles:
+                raise ValueError(f"selection mask has {p.mask.numel()} entries, expected {self.n_particles}")
+        else:
+            p.mask = torch.ones(self.n_particles, dtype=torch.int32, device=dev)
+        if velocity is not None:
+            p.velocity = _vec3(velocity)
+        if angular_velocity is not None and center is not None and axis is not None:
+            p.rotation_axis = _vec3(axis)
+            p.rotation_center = _vec3(center)
+            p.angular_velocity = float(angular_velocity)
+        p._kind = N.MOD_MOVER
+        self.particle_velocity_modifier_params.append(p)
+        self.particle_velocity_modifiers.append(N.MOD_MOVER)
+
+    def restart_and_compute_F_C(self, mpm_model, mpm_state, target_pos, device):
+        raise NotImplementedError("restart_and_compute_F_C (static-pose restart) is not implemented yet")

@@ -1,0 +1,153 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+The reference publishes no benchmark inputs and its dataset is not
+available, so every configuration is synthetic (numpy.random.default_rng):
+
+  c1  plain forward: 20,000 particles uniform in [0.35, 0.65]^3, 48^3 grid,
+      fixed-corotated jelly E=2e4 nu=0.3 rho=1e3, dt=2e-4 x 200 substeps,
+      gravity (0,-9.8,0), sticky floor at y=3dx, slip walls (bounding box)
+  c2  large single forward: 500,000 particles in two boxes, 128^3 grid,
+      plasticine with per-particle E log-U[1e3,1e5], nu U[0.2,0.45],
+      yield U[5e2,5e3], softening 0.1; a 0.1^3 box collider centred at
+      (0.30, 0.45, 0.30) moves at (0,-0.5,0) for the first 500 substeps and
+      (0,+0.5,0) after; dt=1e-4 x 1000 substeps; floor and walls as c1
+  c3  differentiable: 200,000 particles in [0.35,0.65]^3, v0 ~ N(0, 0.05),
+      96^3 grid, plasticine; target (E=3e4, nu=0.35, yield=2e3), guess
+      (1e4, 0.25, 1e3); dt=2e-4 x 400 substeps, checkpoint every 20
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional
+
+import numpy as np
+
+
+@dataclass
+class Workload:
+    name: str
+    n: int
+    G: int
+    dt: float
+    T: int
+    material: str
+    x: np.ndarray
+    v: np.ndarray
+    vol: np.ndarray
+    rho: np.ndarray
+    E: np.ndarray
+    nu: np.ndarray
+    ys: np.ndarray
+    gravity: tuple = (0.0, -9.8, 0.0)
+    colliders: List[dict] = field(default_factory=list)
+    velocity_schedule: Optional[Callable[[int], tuple]] = None   # cuboid velocity per substep
+    description: str = ""
+
+    @property
+    def particle_substeps(self) -> int:
+        return self.n * self.T
+
+
+def _floor_walls(G):
+    return [dict(kind="surface", point=[0.0, 3.0 / G, 0.0], normal=[0.0, 1.0, 0.0], surface="sticky"),
+            dict(kind="bbox")]
+
+
+def c1(seed: int = 1, n: int = 20_000, G: int = 48, T: int = 200) -> Workload:
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.35, 0.65, (n, 3)).astype(np.float32)
+    return Workload(
+        name="c1", n=n, G=G, dt=2e-4, T=T, material="jelly", x=x, v=np.zeros((n, 3), np.float32),
+        vol=np.full(n, np.float32(0.027 / n), np.float32), rho=np.full(n, np.float32(1e3), np.float32),
+        E=np.full(n, np.float32(2e4), np.float32), nu=np.full(n, np.float32(0.3), np.float32),
+        ys=np.zeros(n, np.float32), colliders=_floor_walls(G),
+        description=f"plain forward: {n} particles, {G}^3 grid, jelly (FCR), dt=2e-4 x {T} substeps")
+
+
+def c2(seed: int = 2, n: int = 500_000, G: int = 128, T: int = 1000) -> Workload:
+    rng = np.random.default_rng(seed)
+    h = n // 2
+    x = np.concatenate([rng.uniform((0.15, 0.10, 0.15), (0.45, 0.40, 0.45), (h, 3)),
+                        rng.uniform((0.55, 0.10, 0.55), (0.85, 0.40, 0.85), (n - h, 3))]).astype(np.float32)
+    E = np.exp(rng.uniform(np.log(1e3), np.log(1e5), n)).astype(np.float32)
+    nu = rng.uniform(0.2, 0.45, n).astype(np.float32)
+    ys = rng.uniform(5e2, 5e3, n).astype(np.float32)
+    half = T // 2
+    colliders = _floor_walls(G)
+    colliders.insert(1, dict(kind="cuboid", point=[0.30, 0.45, 0.30], size=[0.05, 0.05, 0.05],
+                             velocity=[0.0, -0.5, 0.0]))
+    return Workload(
+        name="c2", n=n, G=G, dt=1e-4, T=T, material="plasticine", x=x, v=np.zeros((n, 3), np.float32),
+        vol=np.full(n, np.float32(0.054 / n), np.float32), rho=np.full(n, np.float32(1e3), np.float32),
+        E=E, nu=nu, ys=ys, colliders=colliders,
+        velocity_schedule=lambda s: (0.0, -0.5, 0.0) if s < half else (0.0, 0.5, 0.0),
+        description=f"large single forward: {n} particles in two boxes, {G}^3 grid, plasticine "
+                    f"(von Mises + FCR), moving 0.1^3 box collider, dt=1e-4 x {T} substeps")
+
+
+def c3(seed: int = 3, n: int = 200_000, G: int = 96, T: int = 400, guess: bool = True) -> Workload:
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.35, 0.65, (n, 3)).astype(np.float32)
+    v = (rng.standard_normal((n, 3)) * 0.05).astype(np.float32)
+    E, nu, ys = (1e4, 0.25, 1e3) if guess else (3e4, 0.35, 2e3)
+    return Workload(
+        name="c3", n=n, G=G, dt=2e-4, T=T, material="plasticine", x=x, v=v,
+        vol=np.full(n, np.float32(0.027 / n), np.float32), rho=np.full(n, np.float32(1e3), np.float32),
+        E=np.full(n, np.float32(E), np.float32), nu=np.full(n, np.float32(nu), np.float32),
+        ys=np.full(n, np.float32(ys), np.float32), colliders=_floor_walls(G),
+        description=f"differentiable rollout: {n} particles, {G}^3 grid, plasticine, dt=2e-4 x {T} substeps")
+
+
+def build_product(w: Workload, device="cuda:0"):
+    """(solver, model, state_a, state_b) of the reference-facing API for w."""
+    import torch
+
+    from .mpm_data_structure import MPMModelStruct, MPMStateStruct
+    from .mpm_solver_diff import MPMWARPDiff
+
+    dev = torch.device(device)
+
+    def t(a):
+        return torch.as_tensor(np.ascontiguousarray(a), device=dev)
+
+    st = MPMStateStruct()
+    st.init(w.n, device=dev)
+    st.from_torch(t(w.x), t(w.vol), None, t(w.v), n_grid=w.G, device=dev)
+    st.reset_density(t(w.rho), update_mass=True)
+    md = MPMModelStruct()
+    md.init(w.n, device=dev)
+    md.init_other_params(n_grid=w.G)
+    md.gravitational_accelaration = w.gravity
+    solver = MPMWARPDiff()
+    solver.initialize(w.n, n_grid=w.G, device=dev)
+    solver.set_parameters_dict(md, st, {"material": w.material})
+    md.E.copy_(t(w.E))
+    md.nu.copy_(t(w.nu))
+    md.finalize_mu_lam(w.n)
+    md.yield_stress.copy_(t(w.ys))
+    for c in w.colliders:
+        if c["kind"] == "surface":
+            solver.add_surface_collider(c["point"], c["normal"], c.get("surface", "sticky"), 0.0)
+        elif c["kind"] == "cuboid":
+            solver.set_velocity_on_cuboid(c["point"], c["size"], c["velocity"])
+        elif c["kind"] == "bbox":
+            solver.add_bounding_box()
+        else:
+            raise ValueError(c["kind"])
+    other = st.partial_clone()
+    return solver, md, st, other
+
+
+def cuboid_callback(w: Workload, solver):
+    """Host callback applying w.velocity_schedule to the cuboid collider."""
+    if w.velocity_schedule is None:
+        return None
+    idx = [i for i, c in enumerate(w.colliders) if c["kind"] == "cuboid"]
+    if not idx:
+        return None
+    k = idx[0]
+
+    def cb(step):
+        solver.collider_params[k].velocity = w.velocity_schedule(step)
+
+    return cb

@@ -213,6 +213,29 @@ int  empm_read_status(EmpmCtx* ctx, uint32_t* status, void* stream);
 /* Last error message of the context (or of the library when ctx is NULL). */
 int  empm_last_error(EmpmCtx* ctx, char* buf, int len);
 
+/* ---- diagnostics (used by the parity tests) ------------------------------ */
+
+/* Return map + Kirchhoff stress of the material switch for n particles, on
+ * the device, in the reference's [N,3,3] row-major layout: the body of
+ * compute_stress_from_F_trial (mpm_utils.py:602-665). mu, lam, yield_stress
+ * are updated in place as the reference's return maps do. */
+int  empm_debug_stress(const EmpmModelParams* params, const float* F_trial9, float* mu, float* lam,
+                       float* yield_stress, float dt, float* F_out9, float* stress_out9, int n, void* stream);
+
+/* Per-kernel timing with CUDA events on the launch stream (stream path of
+ * empm_substep / empm_rollout only; graph replays are not instrumented).
+ * enable != 0 starts a fresh measurement with room for max_launches launches
+ * per kernel; empm_ctx_kernel_times synchronises and returns, for the three
+ * kernels of a substep [stress+P2G, grid update, G2P], the summed duration in
+ * milliseconds and the number of launches timed. */
+int  empm_ctx_timing(EmpmCtx* ctx, int enable, int max_launches);
+int  empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3);
+
+/* Device pointers of the context's grid buffers (float4[G^3] each): the P2G
+ * accumulator (zero between substeps) and the node velocities written by the
+ * last grid update (w = node mass). */
+int  empm_ctx_grid(EmpmCtx* ctx, float** momentum, float** velocity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,54 +14,7 @@ import numpy as np
 
 from oracle import oracle as O
 
-SURFACE_TYPES = {"sticky": 0, "slip": 1, "cut": 11}
-
-
-def _unit(v):
-    s = 1.0 / math.sqrt(float(sum(t * t for t in v)))
-    return tuple(s * t for t in v)
-
-
-def oracle_colliders(specs, mask=None):
-    out = []
-    for s in specs:
-        k = s["kind"]
-        if k == "surface":
-            out.append(O.OrColliderSpec(O.SURFACE, surface_type=SURFACE_TYPES.get(s.get("surface", "sticky"), 2),
-                                        point=tuple(s["point"]), normal=_unit(s["normal"]),
-                                        start_time=s.get("start_time", 0.0), end_time=s.get("end_time", 999.0)))
-        elif k in ("geometry", "grid_velocity"):
-            c = O.OrColliderSpec(O.GEOMETRY if k == "geometry" else O.GRID_VELOCITY)
-            c.surface_type = SURFACE_TYPES.get(s.get("surface", "sticky"), 2)
-            shape = s["shape"]
-            if shape == "cube":
-                c.shape, c.point, c.size = O.CUBE, tuple(s["center"]), tuple(s["size"])
-            elif shape == "sphere":
-                c.shape, c.point, c.radius = O.SPHERE, tuple(s["center"]), s["radius"]
-            elif shape == "cylinder":
-                c.shape, c.point, c.normal = O.CYLINDER, tuple(s["center"]), _unit(s["axis"])
-                c.radius, c.half_height = s["radius"], s["half_height"]
-            else:
-                c.shape, c.point, c.normal = O.HALFSPACE, tuple(s["point"]), _unit(s["normal"])
-            c.velocity = tuple(s.get("velocity", (0.0, 0.0, 0.0)))
-            c.angular_velocity = s.get("angular_velocity", 0.0)
-            c.rot_axis = tuple(s.get("rot_axis", (1.0, 0.0, 0.0)))
-            c.start_time = s.get("start_time", 0.0)
-            c.end_time = s.get("end_time", 999.0)
-            c.reset = s.get("reset", 0)
-            c.active = s.get("active", True)
-            out.append(c)
-        elif k == "cuboid":
-            out.append(O.OrColliderSpec(O.CUBOID_VELOCITY, point=tuple(s["point"]), size=tuple(s["size"]),
-                                        velocity=tuple(s["velocity"]), start_time=s.get("start_time", 0.0),
-                                        end_time=s.get("end_time", 999.0), reset=s.get("reset", 0)))
-        elif k == "bbox":
-            out.append(O.OrColliderSpec(O.BOUNDING_BOX))
-        elif k == "grid_mask":
-            out.append(O.OrColliderSpec(O.GRID_MASK, mask=np.ascontiguousarray(mask.reshape(-1), dtype=np.int32)))
-        else:
-            raise ValueError(k)
-    return out
+from oracle.specs import SURFACE_TYPES, _unit, oracle_colliders  # noqa: F401
 
 
 MATERIAL_IDS = {"jelly": 0, "metal": 1, "sand": 2, "foam": 3, "snow": 4, "plasticine": 5, "neo-hookean": 6}

@@ -1,0 +1,52 @@
+"""CPU-side checks of the C ABI: the library loads, exports every symbol that
+include/empm_b200.h declares, and rejects bad arguments before touching the
+device. No compute runs here."""
+import ctypes
+
+import pytest
+
+from empm_b200 import _native as N
+
+
+def test_library_exports_header_symbols():
+    L = N.lib()
+    declared = N.header_symbols()
+    assert "empm_substep" in declared and "empm_rollout" in declared
+    for name in declared:
+        assert hasattr(L, name), f"{name} declared in include/empm_b200.h but not exported"
+
+
+def test_version():
+    assert N.lib().empm_version() >= 100
+
+
+def test_struct_sizes_match_header():
+    # the library static_asserts the same numbers
+    assert ctypes.sizeof(N.EmpmCollider) == 104
+    assert ctypes.sizeof(N.EmpmModifier) == 88
+    assert ctypes.sizeof(N.EmpmStep) == 2384
+
+
+def test_ctx_create_rejects_bad_params_without_gpu():
+    L = N.lib()
+    out = ctypes.c_void_p()
+    assert L.empm_ctx_create(None, 10, 4, ctypes.byref(out)) == -1
+    p = N.EmpmModelParams()
+    p.n_grid = 2          # below the minimum
+    p.grid_lim = 1.0
+    assert L.empm_ctx_create(p, 10, 4, ctypes.byref(out)) == -1
+    assert "n_grid" in N.last_error()
+    p.n_grid = 32
+    p.material = 9        # unknown material id
+    assert L.empm_ctx_create(p, 10, 4, ctypes.byref(out)) == -4
+    p.material = 0
+    assert L.empm_ctx_create(p, 10, 0, ctypes.byref(out)) == -1   # max_steps < 1
+
+
+def test_null_context_is_rejected():
+    L = N.lib()
+    st = N.EmpmStep()
+    assert L.empm_substep(None, None, None, None, st, None) == -1
+    assert L.empm_rollout(None, None, None, None, None, 1, 0, None) == -1
+    with pytest.raises(N.EmpmError):
+        N.check(L.empm_ctx_destroy(None) - 1)
