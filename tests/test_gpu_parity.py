@@ -285,7 +285,7 @@ def test_status_word_flags_cfl_and_nan():
     rng = np.random.default_rng(5)
     x = rng.uniform(0.4, 0.6, (n, 3)).astype(np.float32)
     v = np.zeros((n, 3), np.float32)
-    v[0] = (200.0, 0.0, 0.0)      # |v| dt = 0.2 > dx = 1/16
+    v[:, 0] = 200.0               # the whole body moves: |v| dt = 0.2 > dx = 1/16 after G2P
     Ft = np.tile(np.eye(3, dtype=np.float32), (n, 1, 1))
     Ft[1, 0, 0] = np.nan
     st, md = _product_state(x, v, np.zeros((n, 3, 3), np.float32), Ft, np.full(n, 1e4, np.float32),
