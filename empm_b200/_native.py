@@ -19,6 +19,7 @@ EMPM_STATUS_NAN, EMPM_STATUS_CFL, EMPM_STATUS_OUT_OF_BAND = 1, 2, 4
 COLL_SURFACE, COLL_GEOMETRY, COLL_GRID_VELOCITY, COLL_CUBOID_VELOCITY, COLL_BOUNDING_BOX, COLL_GRID_MASK = 1, 2, 3, 4, 5, 6
 SHAPE_CUBE, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_HALFSPACE = 1, 2, 3, 4
 GATE_OFF, GATE_APPLY, GATE_ZERO_ALL = 0, 1, 2
+OPT_SORT_EVERY, OPT_P2G_TILE, OPT_G2P_TILE, OPT_TILE_CAP = 1, 2, 3, 4
 MOD_IMPULSE, MOD_IMPULSE_MASK, MOD_SET_VELOCITY, MOD_ROTATION, MOD_MOVER = 1, 2, 3, 4, 5
 
 F3 = ctypes.c_float * 3
@@ -105,6 +106,7 @@ def lib():
         "empm_debug_stress": ([ctypes.POINTER(EmpmModelParams), P, P, P, P, ctypes.c_float, P, P, I, P], I),
         "empm_ctx_grid": ([P, ctypes.POINTER(P), ctypes.POINTER(P)], I),
         "empm_ctx_timing": ([P, I, I], I),
+        "empm_ctx_set_option": ([P, I, I], I),
         "empm_ctx_kernel_times": ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
     }
     for name, (args, res) in sig.items():
@@ -133,3 +135,14 @@ def header_symbols():
     path = os.path.join(os.path.dirname(_HERE), "include", "empm_b200.h")
     src = open(path).read()
     return sorted(set(re.findall(r"^\s*int\s+(empm_\w+)\s*\(", src, flags=re.M)))
+
+
+def grid_dense_index(G: int):
+    """Blocked-layout address of every node (i, j, k) of a G^3 grid, as a
+    [G, G, G] int64 numpy array (see empm_ctx_grid)."""
+    import numpy as np
+
+    nb = (G + 3) // 4
+    i, j, k = np.meshgrid(np.arange(G), np.arange(G), np.arange(G), indexing="ij")
+    blk = ((i >> 2) * nb + (j >> 2)) * nb + (k >> 2)
+    return (blk << 6) | ((i & 3) << 4) | ((j & 3) << 2) | (k & 3)

@@ -1,0 +1,540 @@
+// kernels.cuh — __global__ kernels of one MLS-MPM substep.
+//
+// Two launch paths share the per-particle / per-node device functions of
+// substep.cuh:
+//   * the direct path (empm_substep): particles in the caller's order, one
+//     particle per thread, 16-byte vector reductions straight into the grid;
+//   * the sorted path (empm_rollout): particles cell-block sorted every
+//     `sort_every` substeps; P2G accumulates each chunk of sorted particles
+//     into a shared-memory tile of nodes and flushes it with one vector
+//     reduction per node; G2P stages the chunk's node tile in shared memory;
+//     the grid update visits only the 4^3 node blocks P2G touched.
+#pragma once
+#include <limits.h>
+#include "../../include/empm_b200.h"
+#include "grid.cuh"
+#include "substep.cuh"
+
+namespace empm {
+
+// -------------------------------------------------------------------------
+// common argument blocks
+// -------------------------------------------------------------------------
+struct ParticleArrays {
+    float4*  x;      // (x, y, z, mass)
+    float4*  v;      // (vx, vy, vz, 0)
+    F9Planes C;
+    F9Planes F;      // F_trial
+};
+
+struct MaterialArrays {
+    const float* vol;
+    float*       mu;
+    float*       lam;
+    float*       ys;
+    const int*   sel;   // NULL = all simulated
+    const int*   pid;   // caller index of each particle (NULL = identity)
+};
+
+struct StepConsts {
+    int   n;
+    int   G;
+    int   NB;
+    float dx, inv_dx;
+    float grid_lim;
+    float rpic;
+    MaterialScalars ms;
+    const EmpmStep* step;
+    unsigned* status;
+};
+
+struct ChunkList {
+    const int2* chunks;    // (first sorted index, count)
+    const int*  nchunks;   // device count
+};
+
+__device__ __forceinline__ float sel3(const float (&a)[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
+
+// p2g_node with runtime stencil offsets (no local-memory indexing)
+__device__ __forceinline__ float4 p2g_node_dyn(const P2GParticle& q, int i, int j, int k, float dx, float inv_dx,
+                                               float dt) {
+    const Stencil& st = q.st;
+    const float wx = sel3(st.w[0], i), wy = sel3(st.w[1], j), wz = sel3(st.w[2], k);
+    const float dwx = sel3(st.dw[0], i), dwy = sel3(st.dw[1], j), dwz = sel3(st.dw[2], k);
+    const V3 dpos = v3(((float)i - st.fx[0]) * dx, ((float)j - st.fx[1]) * dx, ((float)k - st.fx[2]) * dx);
+    const float weight = wx * wy * wz;
+    const V3 dweight = v3(dwx * wy * wz, wx * dwy * wz, wx * wy * dwz) * inv_dx;
+    const float wm = weight * q.wm_scale;
+    const V3 force = q.Sv * dweight;
+    const V3 add = wm * (q.v + q.Cd * dpos) + dt * force;
+    return make_float4(add.x, add.y, add.z, wm);
+}
+
+// Stress + everything P2G needs for particle p (modifiers applied, material
+// write-back, elastic F handed to G2P). Returns false for unsimulated particles.
+__device__ __forceinline__ bool prepare_particle(const ParticleArrays& P, const MaterialArrays& M, F9Planes Fe,
+                                                 const StepConsts& c, int p, P2GParticle& q) {
+    if (M.sel && __ldg(M.sel + p) != 0) return false;
+    const EmpmStep& st = *c.step;
+    const float4 xm = __ldg(P.x + p);
+    const float4 vv = __ldg(P.v + p);
+    const V3 x = v3(xm.x, xm.y, xm.z);
+    V3 v = v3(vv.x, vv.y, vv.z);
+    if (st.n_modifiers > 0) {
+        const int mi = M.pid ? __ldg(M.pid + p) : p;
+        if (apply_modifiers(st, mi, x, xm.w, v)) P.v[p] = make_float4(v.x, v.y, v.z, vv.w);
+    }
+    float mu = __ldg(M.mu + p), lam = __ldg(M.lam + p), ys = __ldg(M.ys + p);
+    const ConstitutiveOut co = constitutive(f9_load(P.F, p), mu, lam, ys, st.dt, c.ms);
+    f9_store(Fe, p, co.F);
+    if (co.mat_changed) { M.mu[p] = mu; M.lam[p] = lam; M.ys[p] = ys; }
+    q.st = make_stencil(x, c.inv_dx);
+    q.wm_scale = xm.w;
+    q.v = v;
+    q.Cd = damp_affine(f9_load(P.C, p), c.rpic);
+    q.Sv = (-__ldg(M.vol + p)) * co.tau;
+    return true;
+}
+
+__device__ __forceinline__ void mark_stencil_blocks(unsigned char* flags, const Stencil& st, int G, int NB) {
+    const int lo[3] = {max(st.b[0], 0), max(st.b[1], 0), max(st.b[2], 0)};
+    const int hi[3] = {min(st.b[0] + 2, G - 1), min(st.b[1] + 2, G - 1), min(st.b[2] + 2, G - 1)};
+    for (int bi = lo[0] >> 2; bi <= hi[0] >> 2; ++bi)
+        for (int bj = lo[1] >> 2; bj <= hi[1] >> 2; ++bj)
+            for (int bk = lo[2] >> 2; bk <= hi[2] >> 2; ++bk) flags[(bi * NB + bj) * NB + bk] = 1;
+}
+
+// direct scatter of one prepared particle into the blocked grid
+__device__ __forceinline__ void scatter_global(const P2GParticle& q, const StepConsts& c, float4* grid,
+                                               unsigned char* flags) {
+    const int G = c.G;
+    const bool in_grid = stencil_in_grid(q.st, G);
+    if (!in_grid) atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
+    const float dt = c.step->dt;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
+                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) continue;
+                red_add_v4(grid + node_addr(ix, iy, iz, c.NB), p2g_node(q, i, j, k, c.dx, c.inv_dx, dt));
+            }
+    mark_stencil_blocks(flags, q.st, G, c.NB);
+}
+
+// -------------------------------------------------------------------------
+// direct path
+// -------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_p2g_direct(ParticleArrays P, MaterialArrays M, F9Planes Fe, StepConsts c,
+                                                    float4* grid, unsigned char* flags) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= c.n) return;
+    P2GParticle q;
+    if (!prepare_particle(P, M, Fe, c, p, q)) return;
+    scatter_global(q, c, grid, flags);
+}
+
+// -------------------------------------------------------------------------
+// grid update over touched 4^3 blocks (both paths)
+// -------------------------------------------------------------------------
+struct GridUpdateArgs {
+    float4*        mom;      // accumulation; zeroed here for the next substep
+    float4*        vel;      // node velocity after the boundary conditions (w = node mass)
+    unsigned char* flags;    // touched blocks; cleared here
+    int            G, NB;
+    float          dx;
+    V3             g;
+    float          damping;
+    const EmpmStep* step;
+};
+
+__global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs a) {
+    const int nblocks = a.NB * a.NB * a.NB;
+    const int group = threadIdx.x >> 6;   // 4 node blocks per iteration
+    const int lane = threadIdx.x & 63;
+    const EmpmStep& st = *a.step;
+    for (int base = blockIdx.x * 4; base < nblocks; base += gridDim.x * 4) {
+        const int b = base + group;
+        const bool active = b < nblocks && a.flags[b] != 0;
+        __syncthreads();   // every group has read its flag before any is cleared
+        if (active) {
+            const long long node = ((long long)b << 6) | lane;
+            const float4 m = a.mom[node];
+            a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+            V3 v = grid_velocity(m, st.dt, a.g, a.damping);
+            if (st.n_colliders > 0) {
+                int i, j, k;
+                node_coords(node, a.NB, i, j, k);
+                if (i < a.G && j < a.G && k < a.G) {
+                    const long long dense = ((long long)i * a.G + j) * a.G + k;
+                    apply_colliders(st, i, j, k, a.G, a.dx, dense, v);
+                }
+            }
+            a.vel[node] = make_float4(v.x, v.y, v.z, m.w);
+            if (lane == 0) a.flags[b] = 0;
+        }
+    }
+}
+
+// -------------------------------------------------------------------------
+// G2P (shared by both paths through the fetch functor)
+// -------------------------------------------------------------------------
+template <typename Fetch>
+__device__ __forceinline__ void g2p_particle(const ParticleArrays& P, F9Planes Fe, const MaterialArrays& M,
+                                             const ParticleArrays& out, const StepConsts& c, int p, Fetch fetch) {
+    if (M.sel && __ldg(M.sel + p) != 0) {
+        __stcs(out.x + p, make_float4(0.f, 0.f, 0.f, __ldg(P.x + p).w));
+        __stcs(out.v + p, make_float4(0.f, 0.f, 0.f, 0.f));
+        f9_store(out.C, p, m3_zero());
+        f9_store(out.F, p, m3_identity());
+        return;
+    }
+    const float dt = c.step->dt;
+    const float4 xm = __ldg(P.x + p);
+    const V3 x = v3(xm.x, xm.y, xm.z);
+    const Stencil st = make_stencil(x, c.inv_dx);
+    const bool in_grid = stencil_in_grid(st, c.G);
+    const G2POut o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+    const float dx = 1.f / c.inv_dx;
+    const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
+    V3 nx = x + dt * o.v;
+    nx = v3(fminf(fmaxf(nx.x, lo), hi), fminf(fmaxf(nx.y, lo), hi), fminf(fmaxf(nx.z, lo), hi));
+    const M3 Fn = (m3_identity() + dt * o.gradv) * f9_load(Fe, p);
+    __stcs(out.x + p, make_float4(nx.x, nx.y, nx.z, xm.w));
+    __stcs(out.v + p, make_float4(o.v.x, o.v.y, o.v.z, 0.f));
+    f9_store(out.C, p, o.C);
+    f9_store(out.F, p, Fn);
+    unsigned flags = 0;
+    if (!finite3(o.v) || !finite3(nx) || !isfinite(Fn.m[0] + Fn.m[4] + Fn.m[8])) flags |= EMPM_STATUS_NAN;
+    if (fmaxf(fmaxf(fabsf(o.v.x), fabsf(o.v.y)), fabsf(o.v.z)) * dt > dx) flags |= EMPM_STATUS_CFL;
+    if (!in_grid) flags |= EMPM_STATUS_OUT_OF_BAND;
+    if (flags) atomicOr(c.status, flags);
+}
+
+struct GlobalFetch {
+    const float4* vel;
+    int G, NB;
+    __device__ __forceinline__ V3 operator()(const Stencil& st, bool in_grid, int i, int j, int k) const {
+        const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
+        if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) return v3(0.f, 0.f, 0.f);
+        const float4 g = __ldg(vel + node_addr(ix, iy, iz, NB));
+        return v3(g.x, g.y, g.z);
+    }
+};
+
+__global__ void __launch_bounds__(128) k_g2p_direct(ParticleArrays P, F9Planes Fe, MaterialArrays M,
+                                                    ParticleArrays out, StepConsts c, const float4* vel) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= c.n) return;
+    GlobalFetch f{vel, c.G, c.NB};
+    g2p_particle(P, Fe, M, out, c, p, f);
+}
+
+// -------------------------------------------------------------------------
+// sorted path: cell-block keys, scan, permutation
+// -------------------------------------------------------------------------
+__device__ __forceinline__ int particle_block(float4 xm, float inv_dx, int G, int NB) {
+    int b[3];
+    const float gp[3] = {xm.x * inv_dx, xm.y * inv_dx, xm.z * inv_dx};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int t = (int)(gp[a] - 0.5f);
+        t = t < 0 ? 0 : (t >= G ? G - 1 : t);
+        b[a] = t;
+    }
+    return block_of(b[0], b[1], b[2], NB);
+}
+
+__global__ void k_sort_keys(const float4* x, int n, float inv_dx, int G, int NB, int* keys, int* ranks, int* counts) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int b = particle_block(__ldg(x + p), inv_dx, G, NB);
+    keys[p] = b;
+    ranks[p] = atomicAdd(counts + b, 1);
+}
+
+// Single-CTA exclusive scan over the block counts; writes the block start
+// offsets, the chunk list (chunks never span two blocks) and its length, and
+// zeroes the counts for the next sort. 1024 threads, contiguous segments.
+__global__ void __launch_bounds__(1024) k_sort_scan(int* counts, int* offsets, int nblocks, int chunk, int2* chunks,
+                                                    int* nchunks) {
+    __shared__ int s_warp_p[32], s_warp_c[32];
+    const int t = threadIdx.x;
+    const int seg = (nblocks + 1023) / 1024;
+    const int b0 = min(t * seg, nblocks), b1 = min(b0 + seg, nblocks);
+    int sp = 0, sc = 0;
+    for (int b = b0; b < b1; ++b) {
+        const int cnt = counts[b];
+        sp += cnt;
+        sc += (cnt + chunk - 1) / chunk;
+    }
+    // CTA exclusive scan of (sp, sc)
+    const int lane = t & 31, w = t >> 5;
+    int ip = sp, ic = sc;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int np = __shfl_up_sync(0xffffffffu, ip, d), nc = __shfl_up_sync(0xffffffffu, ic, d);
+        if (lane >= d) { ip += np; ic += nc; }
+    }
+    if (lane == 31) { s_warp_p[w] = ip; s_warp_c[w] = ic; }
+    __syncthreads();
+    if (w == 0) {
+        int vp = s_warp_p[lane], vc = s_warp_c[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int np = __shfl_up_sync(0xffffffffu, vp, d), nc = __shfl_up_sync(0xffffffffu, vc, d);
+            if (lane >= d) { vp += np; vc += nc; }
+        }
+        s_warp_p[lane] = vp;
+        s_warp_c[lane] = vc;
+    }
+    __syncthreads();
+    int off_p = ip - sp + (w > 0 ? s_warp_p[w - 1] : 0);
+    int off_c = ic - sc + (w > 0 ? s_warp_c[w - 1] : 0);
+    for (int b = b0; b < b1; ++b) {
+        const int cnt = counts[b];
+        offsets[b] = off_p;
+        for (int k = 0; k * chunk < cnt; ++k) chunks[off_c + k] = make_int2(off_p + k * chunk, min(chunk, cnt - k * chunk));
+        off_p += cnt;
+        off_c += (cnt + chunk - 1) / chunk;
+        counts[b] = 0;
+    }
+    if (t == 1023) *nchunks = off_c;
+}
+
+struct PermuteArgs {
+    ParticleArrays src, dst;
+    const float* vol_s; float* vol_d;
+    const float* mu_s;  float* mu_d;
+    const float* lam_s; float* lam_d;
+    const float* ys_s;  float* ys_d;
+    const int*   sel_s; int*   sel_d;
+    const int*   pid_s; int*   pid_d;   // pid_s NULL: source is in caller order
+    const int*   keys;
+    const int*   ranks;
+    const int*   offsets;
+    int n;
+};
+
+// src order -> sorted order: dst = offsets[keys[p]] + ranks[p]
+__global__ void k_sort_scatter(const PermuteArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const int d = __ldg(a.offsets + __ldg(a.keys + p)) + __ldg(a.ranks + p);
+    a.dst.x[d] = __ldg(a.src.x + p);
+    a.dst.v[d] = __ldg(a.src.v + p);
+    f9_store(a.dst.C, d, f9_load(a.src.C, p));
+    f9_store(a.dst.F, d, f9_load(a.src.F, p));
+    a.vol_d[d] = __ldg(a.vol_s + p);
+    a.mu_d[d] = __ldg(a.mu_s + p);
+    a.lam_d[d] = __ldg(a.lam_s + p);
+    a.ys_d[d] = __ldg(a.ys_s + p);
+    a.sel_d[d] = a.sel_s ? __ldg(a.sel_s + p) : 0;
+    a.pid_d[d] = a.pid_s ? __ldg(a.pid_s + p) : p;
+}
+
+struct UnsortArgs {
+    ParticleArrays src, dst;      // sorted -> caller order
+    F9Planes Fe_s, Fe_d;          // elastic F of the last substep
+    const float* mu_s;  float* mu_d;
+    const float* lam_s; float* lam_d;
+    const float* ys_s;  float* ys_d;
+    const int*   pid;
+    int n;
+};
+
+__global__ void k_unsort(const UnsortArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const int d = __ldg(a.pid + p);
+    a.dst.x[d] = __ldg(a.src.x + p);
+    a.dst.v[d] = __ldg(a.src.v + p);
+    f9_store(a.dst.C, d, f9_load(a.src.C, p));
+    f9_store(a.dst.F, d, f9_load(a.src.F, p));
+    f9_store(a.Fe_d, d, f9_load(a.Fe_s, p));
+    a.mu_d[d] = __ldg(a.mu_s + p);
+    a.lam_d[d] = __ldg(a.lam_s + p);
+    a.ys_d[d] = __ldg(a.ys_s + p);
+}
+
+// -------------------------------------------------------------------------
+// sorted path: tiled P2G and G2P over chunks of sorted particles
+// -------------------------------------------------------------------------
+constexpr int TILE_THREADS = 256;     // = chunk size
+
+struct TileBox {
+    int o[3];   // origin node
+    int e[3];   // extent in nodes
+    int count;  // e0 * e1 * e2
+};
+
+// bounding box of the chunk's stencils (base .. base + 2) in shared memory
+__device__ __forceinline__ TileBox chunk_box(bool active, const int (&b)[3], int* s_min, int* s_max) {
+    if (threadIdx.x < 3) { s_min[threadIdx.x] = INT_MAX; s_max[threadIdx.x] = INT_MIN; }
+    __syncthreads();
+    int mn[3], mx[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) { mn[a] = active ? b[a] : INT_MAX; mx[a] = active ? b[a] : INT_MIN; }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], d));
+            mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], d));
+        }
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { atomicMin(s_min + a, mn[a]); atomicMax(s_max + a, mx[a]); }
+    __syncthreads();
+    TileBox tb;
+    tb.count = 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        tb.o[a] = s_min[a];
+        tb.e[a] = s_max[a] - s_min[a] + 3;
+        tb.count *= tb.e[a];
+    }
+    if (s_min[0] == INT_MAX) tb.count = 0;
+    return tb;
+}
+
+struct TiledArgs {
+    ParticleArrays P;
+    MaterialArrays M;
+    F9Planes Fe;
+    StepConsts c;
+    ChunkList cl;
+    float4* grid;             // P2G: accumulation; G2P: node velocities
+    unsigned char* flags;     // P2G marks touched blocks
+    ParticleArrays out;       // G2P output
+    int tile_cap;             // nodes in the shared tile
+};
+
+__global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a) {
+    extern __shared__ float4 tile[];
+    __shared__ int s_min[3], s_max[3];
+    const int nch = *a.cl.nchunks;
+    const StepConsts& c = a.c;
+    const float dt = c.step->dt;
+    for (int ci = blockIdx.x; ci < nch; ci += gridDim.x) {
+        const int2 ch = a.cl.chunks[ci];
+        const int p = ch.x + (int)threadIdx.x;
+        bool active = threadIdx.x < (unsigned)ch.y;
+        int base[3] = {0, 0, 0};
+        if (active) {
+            const float4 xm = __ldg(a.P.x + p);
+            base[0] = (int)(xm.x * c.inv_dx - 0.5f);
+            base[1] = (int)(xm.y * c.inv_dx - 0.5f);
+            base[2] = (int)(xm.z * c.inv_dx - 0.5f);
+            if (a.M.sel && __ldg(a.M.sel + p) != 0) active = false;
+        }
+        const TileBox tb = chunk_box(active, base, s_min, s_max);
+        const bool use_tile = tb.count > 0 && tb.count <= a.tile_cap;
+        if (use_tile)
+            for (int t = threadIdx.x; t < tb.count; t += TILE_THREADS) tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncthreads();
+        if (active) {
+            P2GParticle q;
+            if (prepare_particle(a.P, a.M, a.Fe, c, p, q)) {
+                if (use_tile) {
+                    // stagger the 27 stencil offsets across lanes so particles of the
+                    // same cell do not hit the same shared-memory node together
+                    int s = (int)(threadIdx.x % 27u);
+                    int i = s / 9, j = (s / 3) % 3, k = s % 3;
+                    const int li0 = q.st.b[0] - tb.o[0], lj0 = q.st.b[1] - tb.o[1], lk0 = q.st.b[2] - tb.o[2];
+                    for (int it = 0; it < 27; ++it) {
+                        const float4 v = p2g_node_dyn(q, i, j, k, c.dx, c.inv_dx, dt);
+                        float* dst = reinterpret_cast<float*>(tile + ((li0 + i) * tb.e[1] + (lj0 + j)) * tb.e[2] + (lk0 + k));
+                        atomicAdd(dst + 0, v.x);
+                        atomicAdd(dst + 1, v.y);
+                        atomicAdd(dst + 2, v.z);
+                        atomicAdd(dst + 3, v.w);
+                        if (++k == 3) { k = 0; if (++j == 3) { j = 0; if (++i == 3) i = 0; } }
+                    }
+                } else {
+                    scatter_global(q, c, a.grid, a.flags);
+                }
+            }
+        }
+        __syncthreads();
+        if (use_tile) {
+            const int e12 = tb.e[1] * tb.e[2];
+            for (int t = threadIdx.x; t < tb.count; t += TILE_THREADS) {
+                const float4 v = tile[t];
+                if (v.w == 0.f && v.x == 0.f && v.y == 0.f && v.z == 0.f) continue;
+                const int gi = tb.o[0] + t / e12, gj = tb.o[1] + (t / tb.e[2]) % tb.e[1], gk = tb.o[2] + t % tb.e[2];
+                if (gi < 0 || gj < 0 || gk < 0 || gi >= c.G || gj >= c.G || gk >= c.G) {
+                    atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
+                    continue;
+                }
+                red_add_v4(a.grid + node_addr(gi, gj, gk, c.NB), v);
+            }
+            // mark the 4^3 blocks the tile overlaps
+            const int lo[3] = {max(tb.o[0], 0) >> 2, max(tb.o[1], 0) >> 2, max(tb.o[2], 0) >> 2};
+            const int hi[3] = {min(tb.o[0] + tb.e[0] - 1, c.G - 1) >> 2, min(tb.o[1] + tb.e[1] - 1, c.G - 1) >> 2,
+                               min(tb.o[2] + tb.e[2] - 1, c.G - 1) >> 2};
+            const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1, n2 = hi[2] - lo[2] + 1;
+            const int nmark = (n0 > 0 && n1 > 0 && n2 > 0) ? n0 * n1 * n2 : 0;
+            for (int t = threadIdx.x; t < nmark; t += TILE_THREADS) {
+                const int bi = lo[0] + t / (n1 * n2), bj = lo[1] + (t / n2) % n1, bk = lo[2] + t % n2;
+                a.flags[(bi * c.NB + bj) * c.NB + bk] = 1;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+struct TileFetch {
+    const float4* tile;
+    int o0, o1, o2, e1, e2;
+    __device__ __forceinline__ V3 operator()(const Stencil& st, bool, int i, int j, int k) const {
+        const float4 g = tile[((st.b[0] + i - o0) * e1 + (st.b[1] + j - o1)) * e2 + (st.b[2] + k - o2)];
+        return v3(g.x, g.y, g.z);
+    }
+};
+
+__global__ void __launch_bounds__(TILE_THREADS, 2) k_g2p_tiled(const TiledArgs a) {
+    extern __shared__ float4 tile[];
+    __shared__ int s_min[3], s_max[3];
+    const int nch = *a.cl.nchunks;
+    const StepConsts& c = a.c;
+    for (int ci = blockIdx.x; ci < nch; ci += gridDim.x) {
+        const int2 ch = a.cl.chunks[ci];
+        const int p = ch.x + (int)threadIdx.x;
+        const bool active = threadIdx.x < (unsigned)ch.y;
+        bool stenciled = active;
+        int base[3] = {0, 0, 0};
+        if (active) {
+            if (a.M.sel && __ldg(a.M.sel + p) != 0) stenciled = false;
+            const float4 xm = __ldg(a.P.x + p);
+            base[0] = (int)(xm.x * c.inv_dx - 0.5f);
+            base[1] = (int)(xm.y * c.inv_dx - 0.5f);
+            base[2] = (int)(xm.z * c.inv_dx - 0.5f);
+        }
+        const TileBox tb = chunk_box(stenciled, base, s_min, s_max);
+        const bool use_tile = tb.count > 0 && tb.count <= a.tile_cap && tb.o[0] >= 0 && tb.o[1] >= 0 && tb.o[2] >= 0 &&
+                              tb.o[0] + tb.e[0] <= c.G && tb.o[1] + tb.e[1] <= c.G && tb.o[2] + tb.e[2] <= c.G;
+        if (use_tile) {
+            const int e12 = tb.e[1] * tb.e[2];
+            for (int t = threadIdx.x; t < tb.count; t += TILE_THREADS) {
+                const int gi = tb.o[0] + t / e12, gj = tb.o[1] + (t / tb.e[2]) % tb.e[1], gk = tb.o[2] + t % tb.e[2];
+                tile[t] = __ldg(a.grid + node_addr(gi, gj, gk, c.NB));
+            }
+        }
+        __syncthreads();
+        if (active) {
+            if (use_tile) {
+                TileFetch f{tile, tb.o[0], tb.o[1], tb.o[2], tb.e[1], tb.e[2]};
+                g2p_particle(a.P, a.Fe, a.M, a.out, c, p, f);
+            } else {
+                GlobalFetch f{a.grid, c.G, c.NB};
+                g2p_particle(a.P, a.Fe, a.M, a.out, c, p, f);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace empm

@@ -5,159 +5,12 @@
 #include <string.h>
 #include <stdarg.h>
 #include "../../include/empm_b200.h"
-#include "substep.cuh"
+#include "kernels.cuh"
 #include "ctx.hpp"
 
 using namespace empm;
 
 namespace {
-
-struct P2GArgs {
-    const float4* x;
-    float4*       v;        // old state's v (modifiers write back in place)
-    F9Planes      C;
-    F9Planes      F;        // F_trial
-    F9Planes      Fe;       // receives the elastic F
-    const float*  vol;
-    float*        mu;
-    float*        lam;
-    float*        ys;
-    const int*    sel;
-    float4*       grid;     // momentum + mass accumulation
-    unsigned*     status;
-    int           n;
-    int           G;
-    float         dx, inv_dx;
-    float         rpic;
-    MaterialScalars ms;
-    const EmpmStep* step;
-};
-
-// Fused return map + stress + APIC P2G scatter, one particle per thread,
-// 16-byte vector reductions into the node float4 (px, py, pz, m).
-__global__ void __launch_bounds__(128) k_stress_p2g(const P2GArgs a) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
-    if (a.sel && __ldg(a.sel + p) != 0) return;
-    const EmpmStep& st = *a.step;
-    const float4 xm = __ldg(a.x + p);
-    const float4 vv = __ldg(a.v + p);
-    const V3 x = v3(xm.x, xm.y, xm.z);
-    V3 v = v3(vv.x, vv.y, vv.z);
-    const float mass = xm.w;
-    if (st.n_modifiers > 0 && apply_modifiers(st, p, x, mass, v))
-        a.v[p] = make_float4(v.x, v.y, v.z, vv.w);
-
-    float mu = __ldg(a.mu + p), lam = __ldg(a.lam + p), ys = __ldg(a.ys + p);
-    const ConstitutiveOut co = constitutive(f9_load(a.F, p), mu, lam, ys, st.dt, a.ms);
-    f9_store(a.Fe, p, co.F);
-    if (co.mat_changed) { a.mu[p] = mu; a.lam[p] = lam; a.ys[p] = ys; }
-
-    P2GParticle q;
-    q.st = make_stencil(x, a.inv_dx);
-    q.wm_scale = mass;
-    q.v = v;
-    q.Cd = damp_affine(f9_load(a.C, p), a.rpic);
-    q.Sv = (-__ldg(a.vol + p)) * co.tau;
-    const bool in_grid = stencil_in_grid(q.st, a.G);
-    if (!in_grid) atomicOr(a.status, EMPM_STATUS_OUT_OF_BAND);
-    const int G = a.G;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
-                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) continue;
-                const float4 c = p2g_node(q, i, j, k, a.dx, a.inv_dx, st.dt);
-                red_add_v4(a.grid + ((long long)ix * G + iy) * G + iz, c);
-            }
-}
-
-struct GridArgs {
-    float4*  mom;    // read, then zeroed for the next substep
-    float4*  vel;    // node velocity after BCs (w = node mass)
-    int      G;
-    float    dx;
-    V3       g;
-    float    damping;
-    const EmpmStep* step;
-};
-
-__global__ void __launch_bounds__(256) k_grid_update(const GridArgs a) {
-    const long long total = (long long)a.G * a.G * a.G;
-    const EmpmStep& st = *a.step;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const float4 m = a.mom[idx];
-        a.mom[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
-        V3 v = grid_velocity(m, st.dt, a.g, a.damping);
-        if (st.n_colliders > 0) {
-            const int k = (int)(idx % a.G);
-            const int j = (int)((idx / a.G) % a.G);
-            const int i = (int)(idx / ((long long)a.G * a.G));
-            apply_colliders(st, i, j, k, a.G, a.dx, idx, v);
-        }
-        a.vel[idx] = make_float4(v.x, v.y, v.z, m.w);
-    }
-}
-
-struct G2PArgs {
-    const float4* x;
-    F9Planes      Fe;
-    const int*    sel;
-    const float4* vel;
-    float4*       x_out;
-    float4*       v_out;
-    F9Planes      C_out;
-    F9Planes      F_out;
-    unsigned*     status;
-    int           n;
-    int           G;
-    float         inv_dx;
-    float         grid_lim;
-    const EmpmStep* step;
-};
-
-__global__ void __launch_bounds__(128) k_g2p(const G2PArgs a) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
-    if (a.sel && __ldg(a.sel + p) != 0) {
-        // the reference leaves unsimulated particles at partial_clone's values
-        __stcs(a.x_out + p, make_float4(0.f, 0.f, 0.f, __ldg(a.x + p).w));
-        __stcs(a.v_out + p, make_float4(0.f, 0.f, 0.f, 0.f));
-        f9_store(a.C_out, p, m3_zero());
-        f9_store(a.F_out, p, m3_identity());
-        return;
-    }
-    const float dt = a.step->dt;
-    const float4 xm = __ldg(a.x + p);
-    const V3 x = v3(xm.x, xm.y, xm.z);
-    const Stencil st = make_stencil(x, a.inv_dx);
-    const int G = a.G;
-    const bool in_grid = stencil_in_grid(st, G);
-    const G2POut o = g2p_gather(st, a.inv_dx, [&](int i, int j, int k) {
-        const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
-        if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) return v3(0.f, 0.f, 0.f);
-        const float4 g = __ldg(a.vel + ((long long)ix * G + iy) * G + iz);
-        return v3(g.x, g.y, g.z);
-    });
-    const float dx = 1.f / a.inv_dx;
-    const float lo = dx * 2.f, hi = a.grid_lim - dx * 2.f;
-    V3 nx = x + dt * o.v;
-    nx = v3(fminf(fmaxf(nx.x, lo), hi), fminf(fmaxf(nx.y, lo), hi), fminf(fmaxf(nx.z, lo), hi));
-    const M3 Fn = (m3_identity() + dt * o.gradv) * f9_load(a.Fe, p);
-    __stcs(a.x_out + p, make_float4(nx.x, nx.y, nx.z, xm.w));
-    __stcs(a.v_out + p, make_float4(o.v.x, o.v.y, o.v.z, 0.f));
-    f9_store(a.C_out, p, o.C);
-    f9_store(a.F_out, p, Fn);
-    unsigned flags = 0;
-    if (!finite3(o.v) || !finite3(nx) || !isfinite(Fn.m[0] + Fn.m[4] + Fn.m[8])) flags |= EMPM_STATUS_NAN;
-    if (fmaxf(fmaxf(fabsf(o.v.x), fabsf(o.v.y)), fabsf(o.v.z)) * dt > dx) flags |= EMPM_STATUS_CFL;
-    if (!in_grid) flags |= EMPM_STATUS_OUT_OF_BAND;
-    if (flags) atomicOr(a.status, flags);
-}
 
 // ---- layout conversion and preparation kernels ---------------------------
 
@@ -256,6 +109,18 @@ static int validate_params(EmpmCtx* ctx, const EmpmModelParams* p) {
     return EMPM_OK;
 }
 
+static void free_sorted(SortedBuffers& sb) {
+    for (int i = 0; i < 2; ++i) {
+        if (sb.part[i]) cudaFree(sb.part[i]);
+        if (sb.matf[i]) cudaFree(sb.matf[i]);
+        if (sb.mati[i]) cudaFree(sb.mati[i]);
+        sb.part[i] = nullptr; sb.matf[i] = nullptr; sb.mati[i] = nullptr;
+    }
+    void* ptrs[] = {sb.fe, sb.keys, sb.ranks, sb.counts, sb.offsets, sb.chunks, sb.nchunks};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    sb = SortedBuffers();
+}
+
 extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, int max_steps, EmpmCtx** out) {
     EmpmCtx* ctx = nullptr;
     if (!out) return empm_set_error(nullptr, EMPM_ERR_INVALID, "out is NULL");
@@ -268,15 +133,19 @@ extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, i
     ctx->params = *params;
     ctx->n_particles = n_particles;
     ctx->max_steps = max_steps;
-    const long long G = params->n_grid;
-    const size_t grid_bytes = (size_t)(G * G * G) * sizeof(float4);
+    ctx->NB = grid_nb(params->n_grid);
+    const size_t nblocks = (size_t)ctx->NB * ctx->NB * ctx->NB;
+    const size_t grid_bytes = nblocks * 64 * sizeof(float4);
     cudaError_t e = cudaGetDevice(&ctx->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_mom, grid_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_vel, grid_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->flags, nblocks);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_steps, sizeof(EmpmStep) * (size_t)max_steps);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_mom, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_vel, 0, grid_bytes);
+    if (e == cudaSuccess) e = cudaMemset(ctx->flags, 0, nblocks);
     if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_a, cudaEventDisableTiming);
@@ -295,14 +164,35 @@ extern "C" int empm_ctx_destroy(EmpmCtx* ctx) {
     if (!ctx) return EMPM_OK;
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     for (cudaEvent_t ev : ctx->timing_events) cudaEventDestroy(ev);
+    free_sorted(ctx->sb);
     if (ctx->grid_mom) cudaFree(ctx->grid_mom);
     if (ctx->grid_vel) cudaFree(ctx->grid_vel);
+    if (ctx->flags) cudaFree(ctx->flags);
     if (ctx->d_steps) cudaFree(ctx->d_steps);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
     if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
     delete ctx;
+    return EMPM_OK;
+}
+
+extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    switch (option) {
+        case EMPM_OPT_SORT_EVERY:
+            if (value < 0) return empm_set_error(ctx, EMPM_ERR_INVALID, "sort_every must be >= 0");
+            ctx->sort_every = value;
+            break;
+        case EMPM_OPT_P2G_TILE: ctx->p2g_tile = value != 0; break;
+        case EMPM_OPT_G2P_TILE: ctx->g2p_tile = value != 0; break;
+        case EMPM_OPT_TILE_CAP:
+            if (value < 27 || value > 4096) return empm_set_error(ctx, EMPM_ERR_INVALID, "tile_cap %d out of [27, 4096]", value);
+            ctx->tile_cap = value;
+            break;
+        default: return empm_set_error(ctx, EMPM_ERR_INVALID, "unknown option %d", option);
+    }
+    ctx->graph_valid = false;
     return EMPM_OK;
 }
 
@@ -375,85 +265,271 @@ static void timing_mark(EmpmCtx* ctx, int kernel, int which, cudaStream_t stream
     if (which == 1) ctx->timing_count[kernel] = idx + 1;
 }
 
-// Enqueue the three kernels of substep `s` (schedule at d_steps + s).
-static int launch_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out, const EmpmMaterial* mat,
-                          const EmpmStep* d_step, cudaStream_t stream) {
+static StepConsts step_consts(EmpmCtx* ctx, const EmpmStep* d_step) {
     const EmpmModelParams& P = ctx->params;
+    StepConsts c;
+    c.n = ctx->n_particles;
+    c.G = P.n_grid;
+    c.NB = ctx->NB;
+    c.dx = P.grid_lim / (float)P.n_grid;
+    c.inv_dx = (float)P.n_grid / P.grid_lim;
+    c.grid_lim = P.grid_lim;
+    c.rpic = P.rpic_damping;
+    c.ms.material = P.material;
+    c.ms.softening = P.softening;
+    c.ms.hardening = P.hardening;
+    c.ms.xi = P.xi;
+    c.ms.plastic_viscosity = P.plastic_viscosity;
+    c.ms.alpha = P.alpha;
+    c.step = d_step;
+    c.status = ctx->d_status;
+    return c;
+}
+
+static ParticleArrays particle_arrays(const EmpmParticles* p, int n) {
+    ParticleArrays a;
+    a.x = reinterpret_cast<float4*>(p->x);
+    a.v = reinterpret_cast<float4*>(p->v);
+    a.C = f9_planes(p->C, n);
+    a.F = f9_planes(p->F, n);
+    return a;
+}
+
+// x4 | v4 | C | F packed in one allocation; plane offsets use n rounded up
+// to a multiple of 4 so that every float4 plane starts on a 16-byte boundary
+static size_t padded4(int n) { return ((size_t)n + 3) & ~(size_t)3; }
+
+static ParticleArrays particle_arrays(float* base, int n) {
+    const size_t np = padded4(n);
+    ParticleArrays a;
+    a.x = reinterpret_cast<float4*>(base);
+    a.v = reinterpret_cast<float4*>(base + 4 * np);
+    a.C = f9_planes(base + 8 * np, n);
+    a.F = f9_planes(base + 17 * np, n);
+    return a;
+}
+
+static int launch_grid_update(EmpmCtx* ctx, const EmpmStep* d_step, cudaStream_t stream) {
+    const EmpmModelParams& P = ctx->params;
+    GridUpdateArgs g;
+    g.mom = ctx->grid_mom;
+    g.vel = ctx->grid_vel;
+    g.flags = ctx->flags;
+    g.G = P.n_grid;
+    g.NB = ctx->NB;
+    g.dx = P.grid_lim / (float)P.n_grid;
+    g.g = v3(P.gravity[0], P.gravity[1], P.gravity[2]);
+    g.damping = P.grid_v_damping_scale;
+    g.step = d_step;
+    const long long nblocks = (long long)ctx->NB * ctx->NB * ctx->NB;
+    int nb = blocks_for(nblocks, 4);
+    if (nb > ctx->sm_count * 8) nb = ctx->sm_count * 8;
+    timing_mark(ctx, 1, 0, stream);
+    k_grid_update_sparse<<<nb, 256, 0, stream>>>(g);
+    timing_mark(ctx, 1, 1, stream);
+    CK(cudaGetLastError(), "k_grid_update_sparse");
+    return EMPM_OK;
+}
+
+// Direct path: particles in the caller's order, one particle per thread.
+static int launch_substep_direct(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out, const EmpmMaterial* mat,
+                                 const EmpmStep* d_step, cudaStream_t stream) {
     const int n = ctx->n_particles;
-    const int G = P.n_grid;
-    const float dx = P.grid_lim / (float)G;
-    const float inv_dx = (float)G / P.grid_lim;
-    MaterialScalars ms;
-    ms.material = P.material;
-    ms.softening = P.softening;
-    ms.hardening = P.hardening;
-    ms.xi = P.xi;
-    ms.plastic_viscosity = P.plastic_viscosity;
-    ms.alpha = P.alpha;
+    const StepConsts c = step_consts(ctx, d_step);
+    const ParticleArrays Pin = particle_arrays(in, n);
+    const ParticleArrays Pout = particle_arrays(out, n);
+    MaterialArrays M;
+    M.vol = mat->vol;
+    M.mu = mat->mu;
+    M.lam = mat->lam;
+    M.ys = mat->yield_stress;
+    M.sel = mat->selection;
+    M.pid = nullptr;
+    const F9Planes Fe = f9_planes(mat->F_elastic, n);
     if (n > 0) {
-        P2GArgs a;
-        a.x = reinterpret_cast<const float4*>(in->x);
-        a.v = reinterpret_cast<float4*>(in->v);
-        a.C = f9_planes(in->C, n);
-        a.F = f9_planes(in->F, n);
-        a.Fe = f9_planes(mat->F_elastic, n);
-        a.vol = mat->vol;
-        a.mu = mat->mu;
-        a.lam = mat->lam;
-        a.ys = mat->yield_stress;
-        a.sel = mat->selection;
-        a.grid = ctx->grid_mom;
-        a.status = ctx->d_status;
-        a.n = n;
-        a.G = G;
-        a.dx = dx;
-        a.inv_dx = inv_dx;
-        a.rpic = P.rpic_damping;
-        a.ms = ms;
-        a.step = d_step;
         timing_mark(ctx, 0, 0, stream);
-        k_stress_p2g<<<blocks_for(n, 128), 128, 0, stream>>>(a);
+        k_p2g_direct<<<blocks_for(n, 128), 128, 0, stream>>>(Pin, M, Fe, c, ctx->grid_mom, ctx->flags);
         timing_mark(ctx, 0, 1, stream);
-        CK(cudaGetLastError(), "k_stress_p2g");
+        CK(cudaGetLastError(), "k_p2g_direct");
     }
-    {
-        GridArgs g;
-        g.mom = ctx->grid_mom;
-        g.vel = ctx->grid_vel;
-        g.G = G;
-        g.dx = dx;
-        g.g = v3(P.gravity[0], P.gravity[1], P.gravity[2]);
-        g.damping = P.grid_v_damping_scale;
-        g.step = d_step;
-        const long long total = (long long)G * G * G;
-        int nb = blocks_for(total, 256);
-        if (nb > 148 * 16) nb = 148 * 16;
-        timing_mark(ctx, 1, 0, stream);
-        k_grid_update<<<nb, 256, 0, stream>>>(g);
-        timing_mark(ctx, 1, 1, stream);
-        CK(cudaGetLastError(), "k_grid_update");
-    }
+    int rc = launch_grid_update(ctx, d_step, stream);
+    if (rc) return rc;
     if (n > 0) {
-        G2PArgs a;
-        a.x = reinterpret_cast<const float4*>(in->x);
-        a.Fe = f9_planes(mat->F_elastic, n);
-        a.sel = mat->selection;
-        a.vel = ctx->grid_vel;
-        a.x_out = reinterpret_cast<float4*>(out->x);
-        a.v_out = reinterpret_cast<float4*>(out->v);
-        a.C_out = f9_planes(out->C, n);
-        a.F_out = f9_planes(out->F, n);
-        a.status = ctx->d_status;
-        a.n = n;
-        a.G = G;
-        a.inv_dx = inv_dx;
-        a.grid_lim = P.grid_lim;
-        a.step = d_step;
         timing_mark(ctx, 2, 0, stream);
-        k_g2p<<<blocks_for(n, 128), 128, 0, stream>>>(a);
+        k_g2p_direct<<<blocks_for(n, 128), 128, 0, stream>>>(Pin, Fe, M, Pout, c, ctx->grid_vel);
         timing_mark(ctx, 2, 1, stream);
-        CK(cudaGetLastError(), "k_g2p");
+        CK(cudaGetLastError(), "k_g2p_direct");
     }
+    return EMPM_OK;
+}
+
+static int ensure_sorted_buffers(EmpmCtx* ctx) {
+    SortedBuffers& sb = ctx->sb;
+    const int n = ctx->n_particles;
+    if (sb.allocated && sb.n == n) return EMPM_OK;
+    free_sorted(sb);
+    const size_t nblocks = (size_t)ctx->NB * ctx->NB * ctx->NB;
+    sb.max_chunks = (int)((size_t)n / TILE_THREADS + nblocks + 1);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        e = cudaMalloc(&sb.part[i], sizeof(float) * 26 * padded4(n) + 64);
+        if (e == cudaSuccess) e = cudaMalloc(&sb.matf[i], sizeof(float) * 4 * (size_t)n + 64);
+        if (e == cudaSuccess) e = cudaMalloc(&sb.mati[i], sizeof(int) * 2 * (size_t)n + 64);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&sb.fe, sizeof(float) * 9 * (size_t)n + 64);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.keys, sizeof(int) * (size_t)n + 64);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.ranks, sizeof(int) * (size_t)n + 64);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.counts, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.offsets, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.chunks, sizeof(int2) * (size_t)sb.max_chunks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.nchunks, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(sb.counts, 0, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMemset(sb.nchunks, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        free_sorted(sb);
+        return empm_check_cuda(ctx, e, "sorted-path buffers");
+    }
+    sb.allocated = true;
+    sb.n = n;
+    return EMPM_OK;
+}
+
+struct SortedState {
+    int pc = 0;   // particle buffer holding the current state
+    int mc = 0;   // material buffer of the current sort epoch
+};
+
+static MaterialArrays sorted_material(EmpmCtx* ctx, int mc) {
+    const int n = ctx->n_particles;
+    MaterialArrays M;
+    float* f = ctx->sb.matf[mc];
+    int* i = ctx->sb.mati[mc];
+    M.vol = f;
+    M.mu = f + n;
+    M.lam = f + 2 * (size_t)n;
+    M.ys = f + 3 * (size_t)n;
+    M.sel = i;
+    M.pid = i + n;
+    return M;
+}
+
+// sort `src` (caller order when src_mat is given, else the current sorted
+// state) into the other sorted buffers
+static int launch_sort(EmpmCtx* ctx, SortedState& ss, const ParticleArrays* user_src, const EmpmMaterial* user_mat,
+                       cudaStream_t stream) {
+    SortedBuffers& sb = ctx->sb;
+    const int n = ctx->n_particles;
+    const int G = ctx->params.n_grid;
+    const float inv_dx = (float)G / ctx->params.grid_lim;
+    const int nblocks = ctx->NB * ctx->NB * ctx->NB;
+    PermuteArgs a;
+    if (user_src) {
+        a.src = *user_src;
+        a.vol_s = user_mat->vol;
+        a.mu_s = user_mat->mu;
+        a.lam_s = user_mat->lam;
+        a.ys_s = user_mat->yield_stress;
+        a.sel_s = user_mat->selection;
+        a.pid_s = nullptr;
+    } else {
+        a.src = particle_arrays(sb.part[ss.pc], n);
+        const MaterialArrays M = sorted_material(ctx, ss.mc);
+        a.vol_s = M.vol; a.mu_s = M.mu; a.lam_s = M.lam; a.ys_s = M.ys; a.sel_s = M.sel; a.pid_s = M.pid;
+    }
+    const int dp = user_src ? ss.pc : 1 - ss.pc;
+    const int dm = user_src ? ss.mc : 1 - ss.mc;
+    a.dst = particle_arrays(sb.part[dp], n);
+    const MaterialArrays D = sorted_material(ctx, dm);
+    a.vol_d = const_cast<float*>(D.vol); a.mu_d = D.mu; a.lam_d = D.lam; a.ys_d = D.ys;
+    a.sel_d = const_cast<int*>(D.sel); a.pid_d = const_cast<int*>(D.pid);
+    a.keys = sb.keys;
+    a.ranks = sb.ranks;
+    a.offsets = sb.offsets;
+    a.n = n;
+    k_sort_keys<<<blocks_for(n, 256), 256, 0, stream>>>(reinterpret_cast<const float4*>(a.src.x), n, inv_dx, G,
+                                                        ctx->NB, sb.keys, sb.ranks, sb.counts);
+    CK(cudaGetLastError(), "k_sort_keys");
+    k_sort_scan<<<1, 1024, 0, stream>>>(sb.counts, sb.offsets, nblocks, TILE_THREADS, sb.chunks, sb.nchunks);
+    CK(cudaGetLastError(), "k_sort_scan");
+    k_sort_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(a);
+    CK(cudaGetLastError(), "k_sort_scatter");
+    ss.pc = dp;
+    ss.mc = dm;
+    return EMPM_OK;
+}
+
+static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, const EmpmStep* d_step, cudaStream_t stream) {
+    SortedBuffers& sb = ctx->sb;
+    const int n = ctx->n_particles;
+    TiledArgs t;
+    t.P = particle_arrays(sb.part[ss.pc], n);
+    t.M = sorted_material(ctx, ss.mc);
+    t.Fe = f9_planes(sb.fe, n);
+    t.c = step_consts(ctx, d_step);
+    t.cl.chunks = sb.chunks;
+    t.cl.nchunks = sb.nchunks;
+    t.grid = ctx->grid_mom;
+    t.flags = ctx->flags;
+    t.out = particle_arrays(sb.part[1 - ss.pc], n);
+    t.tile_cap = ctx->p2g_tile ? ctx->tile_cap : 0;
+    const int persistent = ctx->sm_count * 2;
+    const size_t smem = sizeof(float4) * (size_t)ctx->tile_cap;
+    timing_mark(ctx, 0, 0, stream);
+    k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+    timing_mark(ctx, 0, 1, stream);
+    CK(cudaGetLastError(), "k_p2g_tiled");
+    int rc = launch_grid_update(ctx, d_step, stream);
+    if (rc) return rc;
+    t.grid = ctx->grid_vel;
+    t.tile_cap = ctx->g2p_tile ? ctx->tile_cap : 0;
+    timing_mark(ctx, 2, 0, stream);
+    k_g2p_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+    timing_mark(ctx, 2, 1, stream);
+    CK(cudaGetLastError(), "k_g2p_tiled");
+    ss.pc = 1 - ss.pc;
+    return EMPM_OK;
+}
+
+static bool use_sorted(EmpmCtx* ctx) {
+    const long long nblocks = (long long)ctx->NB * ctx->NB * ctx->NB;
+    return ctx->sort_every > 0 && ctx->n_particles > 0 && nblocks <= (1 << 20);
+}
+
+// The whole launch sequence of a rollout (also what a graph captures).
+static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat, int n_steps,
+                          cudaStream_t stream) {
+    int rc = EMPM_OK;
+    if (!use_sorted(ctx)) {
+        for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
+            const EmpmParticles* in = (i & 1) ? b : a;
+            EmpmParticles* out = (i & 1) ? a : b;
+            rc = launch_substep_direct(ctx, in, out, mat, ctx->d_steps + i, stream);
+        }
+        return rc;
+    }
+    const int n = ctx->n_particles;
+    SortedState ss;
+    const ParticleArrays ua = particle_arrays(a, n);
+    rc = launch_sort(ctx, ss, &ua, mat, stream);
+    for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
+        if (i > 0 && i % ctx->sort_every == 0) rc = launch_sort(ctx, ss, nullptr, nullptr, stream);
+        if (rc == EMPM_OK) rc = launch_substep_sorted(ctx, ss, ctx->d_steps + i, stream);
+    }
+    if (rc) return rc;
+    UnsortArgs u;
+    u.src = particle_arrays(ctx->sb.part[ss.pc], n);
+    u.dst = particle_arrays((n_steps & 1) ? b : a, n);
+    u.Fe_s = f9_planes(ctx->sb.fe, n);
+    u.Fe_d = f9_planes(mat->F_elastic, n);
+    const MaterialArrays M = sorted_material(ctx, ss.mc);
+    u.mu_s = M.mu; u.mu_d = mat->mu;
+    u.lam_s = M.lam; u.lam_d = mat->lam;
+    u.ys_s = M.ys; u.ys_d = mat->yield_stress;
+    u.pid = M.pid;
+    u.n = n;
+    k_unsort<<<blocks_for(n, 256), 256, 0, stream>>>(u);
+    CK(cudaGetLastError(), "k_unsort");
     return EMPM_OK;
 }
 
@@ -483,7 +559,7 @@ extern "C" int empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles
     cudaStream_t s = (cudaStream_t)stream;
     rc = upload_steps(ctx, step, 1, s);
     if (rc) return rc;
-    return launch_substep(ctx, in, out, mat, ctx->d_steps, s);
+    return launch_substep_direct(ctx, in, out, mat, ctx->d_steps, s);
 }
 
 extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
@@ -497,15 +573,11 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
     cudaStream_t s = (cudaStream_t)stream;
     rc = upload_steps(ctx, steps, n_steps, s);
     if (rc) return rc;
-    if (!use_graph) {
-        for (int i = 0; i < n_steps; ++i) {
-            const EmpmParticles* in = (i & 1) ? b : a;
-            EmpmParticles* out = (i & 1) ? a : b;
-            rc = launch_substep(ctx, in, out, mat, ctx->d_steps + i, s);
-            if (rc) return rc;
-        }
-        return EMPM_OK;
+    if (use_sorted(ctx)) {
+        rc = ensure_sorted_buffers(ctx);
+        if (rc) return rc;
     }
+    if (!use_graph) return launch_rollout(ctx, a, b, mat, n_steps, s);
     // CUDA graph path: capture on the context's own stream (legacy stream 0
     // cannot be captured), joined to the caller's stream by events.
     GraphKey key;
@@ -514,6 +586,10 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
     key.b = *b;
     key.mat = *mat;
     key.n_steps = n_steps;
+    key.sort_every = ctx->sort_every;
+    key.p2g_tile = ctx->p2g_tile;
+    key.g2p_tile = ctx->g2p_tile;
+    key.tile_cap = ctx->tile_cap;
     if (!ctx->graph_valid || memcmp(&key, &ctx->graph_key, sizeof(key)) != 0) {
         if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
         ctx->graph_valid = false;
@@ -521,11 +597,7 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
         ctx->timing = false;
         cudaError_t cap = cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal);
         if (cap != cudaSuccess) { ctx->timing = timing_was; CK(cap, "begin capture"); }
-        for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
-            const EmpmParticles* in = (i & 1) ? b : a;
-            EmpmParticles* out = (i & 1) ? a : b;
-            rc = launch_substep(ctx, in, out, mat, ctx->d_steps + i, ctx->own_stream);
-        }
+        rc = launch_rollout(ctx, a, b, mat, n_steps, ctx->own_stream);
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
         ctx->timing = timing_was;

@@ -56,6 +56,13 @@ class _Context:
             N.check(self.L.empm_ctx_set_params(self.ptr, params), self.ptr)
             self.params_bytes = b
 
+    def set_options(self, opts: dict):
+        cur = getattr(self, "_opts", {})
+        for k, v in opts.items():
+            if cur.get(k) != v:
+                N.check(self.L.empm_ctx_set_option(self.ptr, k, v), self.ptr)
+        self._opts = dict(opts)
+
     def status(self) -> int:
         s = N.ctypes.c_uint32(0)
         N.check(self.L.empm_read_status(self.ptr, N.ctypes.byref(s), _stream_ptr(self.device)), self.ptr)
@@ -76,6 +83,11 @@ class MPMWARPDiff(object):
         self.step_callback = None
         self._ctx: Optional[_Context] = None
         self.use_graph = True
+        # launch options of the library (see EMPM_OPT_* in include/empm_b200.h)
+        self.sort_every = 16
+        self.p2g_tile = True
+        self.g2p_tile = True
+        self.tile_cap = 1024
 
     def initialize(self, n_particles, n_grid=100, grid_lim=1.0, device="cuda:0"):
         self.n_particles = n_particles
@@ -142,6 +154,8 @@ class MPMWARPDiff(object):
             self._ctx = c = _Context(params, n, max(max_steps, 1024), device)
         else:
             c.set_params(params)
+        c.set_options({N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_TILE: int(bool(self.p2g_tile)),
+                       N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap)})
         return c
 
     @staticmethod

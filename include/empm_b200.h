@@ -16,7 +16,7 @@
  *         plane B float4[N] = (m11, m12, m20, m21)
  *         plane C float [N] = (m22)
  *         plane A starts at the pointer, B at +16*N bytes, C at +32*N bytes.
- * Grid layout: float4[G*G*G], node (i,j,k) at (i*G + j)*G + k.
+ * Grid layout: float4 per node, 4x4x4-node blocks (see empm_ctx_grid).
  *
  * Reference interfaces replaced (paths relative to the EMPM repository):
  *   empm_substep        <- MPMWARPDiff.p2g2p_differentiable
@@ -201,11 +201,22 @@ int  empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out,
                   const EmpmMaterial* mat, const EmpmStep* step, void* stream);
 
 /* n_steps substeps, ping-ponging between a and b (the result is in a when
- * n_steps is even, else in b). steps is a host array of n_steps schedules
+ * n_steps is even, else in b). With sorting enabled the particles are copied
+ * into cell-block order inside the library at the start, re-sorted every
+ * EMPM_OPT_SORT_EVERY substeps and written back in the caller's order at the
+ * end, together with mu, lam, yield_stress and F_elastic. steps is a host array of n_steps schedules
  * (n_steps <= max_steps of the context). When use_graph != 0 the launch
  * sequence is captured once into a CUDA graph per (a, b, n_steps) and replayed. */
 int  empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
                   const EmpmStep* steps, int n_steps, int use_graph, void* stream);
+
+/* Launch options of a context (empm_ctx_set_option). */
+#define EMPM_OPT_SORT_EVERY  1   /* rollouts re-sort particles by 4^3 cell block every N substeps; 0 = no sorting (default 16) */
+#define EMPM_OPT_P2G_TILE    2   /* 1 = P2G accumulates into shared-memory node tiles (default), 0 = direct reductions */
+#define EMPM_OPT_G2P_TILE    3   /* 1 = G2P stages the node tile in shared memory (default), 0 = direct gathers */
+#define EMPM_OPT_TILE_CAP    4   /* nodes per shared-memory tile, 27..3072 (default 1024 = 16 KiB) */
+
+int  empm_ctx_set_option(EmpmCtx* ctx, int option, int value);
 
 /* Device status word (EMPM_STATUS_* bits), read synchronously and cleared. */
 int  empm_read_status(EmpmCtx* ctx, uint32_t* status, void* stream);
@@ -231,9 +242,12 @@ int  empm_debug_stress(const EmpmModelParams* params, const float* F_trial9, flo
 int  empm_ctx_timing(EmpmCtx* ctx, int enable, int max_launches);
 int  empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3);
 
-/* Device pointers of the context's grid buffers (float4[G^3] each): the P2G
- * accumulator (zero between substeps) and the node velocities written by the
- * last grid update (w = node mass). */
+/* Device pointers of the context's grid buffers: float4 per node in the
+ * blocked layout (4x4x4-node blocks of 64 consecutive float4, block (bi,bj,bk)
+ * at (bi*NB + bj)*NB + bk with NB = ceil(G/4), node (i&3,j&3,k&3) at
+ * (i&3)*16 + (j&3)*4 + (k&3) inside it): the P2G accumulator (zero between
+ * substeps) and the node velocities of the last grid update (w = node mass).
+ * Only nodes of blocks touched by the last substep's particles are current. */
 int  empm_ctx_grid(EmpmCtx* ctx, float** momentum, float** velocity);
 
 #ifdef __cplusplus

@@ -135,9 +135,13 @@ def test_single_substep_vs_oracle(material):
     # grid velocities after the boundary conditions
     mom, vel = ctypes.c_void_p(), ctypes.c_void_p()
     N.check(N.lib().empm_ctx_grid(solver._ctx.ptr, ctypes.byref(mom), ctypes.byref(vel)))
-    g_vel = _wrap_device(vel.value, 4 * G ** 3).view(G ** 3, 4).clone()
+    nb = (G + 3) // 4
+    g_blk = _wrap_device(vel.value, 4 * nb ** 3 * 64).view(-1, 4).double().cpu().numpy()
+    g_vel = g_blk[N.grid_dense_index(G).reshape(-1)]
+    touched = sim.grid_m > 0   # only nodes in some particle's stencil are updated
     _rel_close(g_vel[:, 3], sim.grid_m, 1e-5, 1e-12, "node mass")
-    _rel_close(g_vel[:, :3].reshape(-1), sim.grid_v_out, 1e-4, 1.0, "node velocity")
+    _rel_close(g_vel[touched, :3].reshape(-1), sim.grid_v_out.reshape(-1, 3)[touched].reshape(-1), 1e-4, 1.0,
+               "node velocity")
     _rel_close(st.particle_F.reshape(n, 9), sim.F, 2e-5, 1.0, "elastic F")
     _rel_close(md.yield_stress, sim.ys, 1e-5, 1.0, "yield")
     _rel_close(md.mu, sim.mu, 1e-6, 1.0, "mu")
@@ -249,7 +253,8 @@ def test_conservation_full_size():
     torch.cuda.synchronize()
     mom, vel = ctypes.c_void_p(), ctypes.c_void_p()
     N.check(N.lib().empm_ctx_grid(solver._ctx.ptr, ctypes.byref(mom), ctypes.byref(vel)))
-    g = _wrap_device(vel.value, 4 * G ** 3).view(G ** 3, 4).double()
+    nb = (G + 3) // 4
+    g = _wrap_device(vel.value, 4 * nb ** 3 * 64).view(-1, 4).double()
     m_p = st.particle_mass.double()
     assert float(g[:, 3].sum()) == pytest.approx(float(m_p.sum()), rel=1e-5)
     p_grid = (g[:, :3] * g[:, 3:4]).sum(0)
@@ -299,3 +304,90 @@ def test_status_word_flags_cfl_and_nan():
     assert status & N.EMPM_STATUS_CFL
     assert status & N.EMPM_STATUS_NAN
     assert solver.read_status() == 0   # reading clears the word
+
+
+@pytest.mark.parametrize("sort_every,p2g_tile,g2p_tile,tile_cap", [
+    (0, False, False, 1024),   # direct path
+    (1, True, True, 1024),
+    (4, True, False, 1024),
+    (16, False, True, 1024),
+    (16, True, True, 1024),
+    (16, True, True, 64),      # tiny tile: forces the fallback path for most chunks
+])
+def test_sorted_path_vs_oracle(sort_every, p2g_tile, g2p_tile, tile_cap):
+    n, G, T, dt = 20000, 48, 120, 2e-4
+    x, v, vol, rho, E, nu, ys = _c1_like(n, G, 11, 5, T, dt, plastic=True)
+    v = (np.random.default_rng(12).standard_normal((n, 3)) * 0.5).astype(np.float32)
+    gravity = (0.0, -9.8, 0.0)
+    specs = [dict(kind="surface", point=[0.0, 3.0 / G, 0.0], normal=[0.0, 1.0, 0.0]),
+             dict(kind="cuboid", point=[0.5, 0.68, 0.5], size=[0.08, 0.05, 0.08], velocity=[0.0, -1.0, 0.0]),
+             dict(kind="bbox")]
+    sim = O.OracleSim(x, v, vol, rho.astype(np.float64) * vol, E, nu, n_grid=G, material=5, gravity=gravity,
+                      yield_stress=ys)
+    sim.colliders = S.oracle_colliders(specs)
+    sim.rollout(dt, T)
+    st, md = _product_state(x, v, np.zeros((n, 3, 3), np.float32), np.tile(np.eye(3, dtype=np.float32), (n, 1, 1)),
+                            E, nu, ys, vol, rho, G, 5, gravity)
+    solver = MPMWARPDiff()
+    solver.initialize(n, n_grid=G)
+    solver.sort_every, solver.p2g_tile, solver.g2p_tile, solver.tile_cap = sort_every, p2g_tile, g2p_tile, tile_cap
+    solver.add_surface_collider((0.0, 3.0 / G, 0.0), (0.0, 1.0, 0.0), "sticky", 0.0)
+    solver.set_velocity_on_cuboid([0.5, 0.68, 0.5], [0.08, 0.05, 0.08], [0.0, -1.0, 0.0])
+    solver.add_bounding_box()
+    other = st.partial_clone()
+    res = solver.rollout(md, st, other, dt, T)
+    torch.cuda.synchronize()
+    err = max_abs(res.particle_x, sim.x)
+    print(f"sort_every={sort_every} tiles=({p2g_tile},{g2p_tile}) cap={tile_cap}: max pos err {err:.3e}")
+    assert err <= POS_GATE
+    _rel_close(md.yield_stress, sim.ys, 2e-3, 1.0, "yield")
+    _rel_close(res.particle_F_trial.reshape(n, 9), sim.F_trial, 2e-3, 1.0, "F_trial")
+    assert solver.read_status() & (N.EMPM_STATUS_NAN | N.EMPM_STATUS_OUT_OF_BAND) == 0
+
+
+def test_sorted_path_modifiers_and_selection():
+    """Particle modifiers (masks indexed by the caller's particle order) and an
+    unsimulated selection on the sorted path against the oracle."""
+    n, G, T, dt = 4000, 24, 30, 2e-4
+    rng = np.random.default_rng(21)
+    x = rng.uniform(0.3, 0.7, (n, 3)).astype(np.float32)
+    v = np.zeros((n, 3), np.float32)
+    vol = np.full(n, np.float32(0.064 / n), np.float32)
+    rho = np.full(n, np.float32(1e3), np.float32)
+    E = np.full(n, np.float32(3e4), np.float32)
+    nu = np.full(n, np.float32(0.3), np.float32)
+    sel = (rng.uniform(size=n) < 0.05).astype(np.int32)
+    st, md = _product_state(x, v, np.zeros((n, 3, 3), np.float32), np.tile(np.eye(3, dtype=np.float32), (n, 1, 1)),
+                            E, nu, np.zeros(n, np.float32), vol, rho, G, 0, (0.0, -9.8, 0.0))
+    st.set_selection(_t(sel, torch.int32))
+    solver = MPMWARPDiff()
+    solver.initialize(n, n_grid=G)
+    solver.sort_every = 4
+    solver.add_impulse_on_particles(st, force=[0.0, 0.0, 5e-3], dt=dt, point=[0.45, 0.45, 0.45], size=[0.1, 0.1, 0.1],
+                                    num_dt=10)
+    solver.enforce_particle_velocity_translation(st, point=[0.6, 0.6, 0.6], size=[0.08, 0.08, 0.08],
+                                                 velocity=[0.3, 0.0, 0.0], start_time=0.0, end_time=0.004)
+    mover_mask = (rng.uniform(size=n) < 0.2).astype(np.int32)
+    solver.set_particle_mover(velocity=[0.0, 0.0, -0.01], angular_velocity=2.0, center=[0.5, 0.5, 0.5],
+                              axis=[0.0, 1.0, 0.0], selection_mask=mover_mask, device=DEV)
+    solver.add_bounding_box()
+    other = st.partial_clone()
+    res = solver.rollout(md, st, other, dt, T)
+    torch.cuda.synchronize()
+    sim = O.OracleSim(x, v, vol, rho.astype(np.float64) * vol, E, nu, n_grid=G, material=0, gravity=(0.0, -9.8, 0.0),
+                      selection=sel)
+    box = lambda p, s: (np.abs(x - np.array(p)) < np.array(s)).all(1).astype(np.int32)  # noqa: E731
+    sim.modifiers = [
+        O.OrModifierSpec(O.MOD_IMPULSE, vec=(0.0, 0.0, 5e-3), start_time=0.0, end_time=0.0 + dt * 10,
+                         mask=box([0.45] * 3, [0.1] * 3)),
+        O.OrModifierSpec(O.MOD_SET_VELOCITY, vec=(0.3, 0.0, 0.0), start_time=0.0, end_time=0.004,
+                         mask=box([0.6] * 3, [0.08] * 3)),
+        O.OrModifierSpec(O.MOD_MOVER, vec=(0.0, 0.0, -0.01), point=(0.5, 0.5, 0.5), normal=(0.0, 1.0, 0.0),
+                         scale=(2.0, 0.0), mask=mover_mask),
+    ]
+    sim.colliders = S.oracle_colliders([dict(kind="bbox")])
+    sim.rollout(dt, T)
+    err = max_abs(res.particle_x, sim.x)
+    print(f"modifiers+selection: max pos err {err:.3e}")
+    assert err <= POS_GATE
+    assert float(res.particle_x[torch.from_numpy(sel).bool().to(DEV)].abs().max()) == 0.0
