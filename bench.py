@@ -127,10 +127,17 @@ def dist_setup(args):
     return world, rank, local
 
 
-def get_workload(name):
+def get_workload(name, particles=None, grid=None, substeps=None):
     from empm_b200 import workloads as W
 
-    return {"c1": W.c1, "c2": W.c2}[name]()
+    kw = {}
+    if particles:
+        kw["n"] = particles
+    if grid:
+        kw["G"] = grid
+    if substeps:
+        kw["T"] = substeps
+    return {"c1": W.c1, "c2": W.c2}[name](**kw)
 
 
 def cpu_baseline(w, budget_s=12.0, max_substeps=40):
@@ -161,7 +168,7 @@ def run_reference(args):
     from oracle import oracle as O
     from oracle import specs as OS
 
-    w = get_workload(args.workload)
+    w = get_workload(args.workload, args.particles, args.grid, args.substeps)
     sim = OS.sim_from_workload(w, precision="fp32_omp")
     cb = OS.workload_callback(w)
     per_step = args.ref_substeps
@@ -205,8 +212,12 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     from empm_b200 import workloads as W
 
-    w = get_workload(args.workload)
+    w = get_workload(args.workload, args.particles, args.grid, args.substeps)
     solver, md, st, other = W.build_product(w, device=dev)
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap"):
+        val = getattr(args, opt)
+        if val is not None:
+            setattr(solver, opt, val)
     cb = W.cuboid_callback(w, solver)
     schedule = solver.build_schedule(0.0, w.dt, w.T, cb)
     init = dict(x=st._x4.clone(), v=st._v4.clone(), C=st._C.clone(), F=st._F_trial.clone(), mu=md.mu.clone(),
@@ -358,6 +369,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-substeps", type=int, default=2, help="substeps per step of the reference arm")
+    ap.add_argument("--particles", type=int, default=None, help="override the workload's particle count")
+    ap.add_argument("--grid", type=int, default=None, help="override the workload's grid resolution")
+    ap.add_argument("--substeps", type=int, default=None, help="override the workload's substeps per step")
+    ap.add_argument("--sort-every", dest="sort_every", type=int, default=None)
+    ap.add_argument("--p2g-mode", dest="p2g_mode", type=int, default=None, help="0 direct, 1 tile, 2 warp-aggregated")
+    ap.add_argument("--g2p-tile", dest="g2p_tile", type=int, default=None)
+    ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

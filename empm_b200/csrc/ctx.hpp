@@ -10,7 +10,7 @@ struct GraphKey {
     EmpmMaterial  mat;
     int           n_steps;
     int           sort_every;
-    int           p2g_tile;
+    int           p2g_mode;
     int           g2p_tile;
     int           tile_cap;
 };
@@ -25,8 +25,10 @@ struct SortedBuffers {
     int*   mati[2] = {nullptr, nullptr};   // sel | pid
     int*   keys = nullptr;
     int*   ranks = nullptr;
-    int*   counts = nullptr;               // [NB^3], zero between sorts
-    int*   offsets = nullptr;              // [NB^3]
+    int*   counts = nullptr;               // [NB^3] particles per block, zero between sorts
+    int*   offsets = nullptr;              // [NB^3] block start offsets
+    int*   cell_counts = nullptr;          // [NB^3 * 64], zero between sorts
+    int*   cell_offsets = nullptr;         // [NB^3 * 64]
     int2*  chunks = nullptr;               // [max_chunks]
     int*   nchunks = nullptr;
     int    max_chunks = 0;
@@ -52,7 +54,7 @@ struct EmpmCtx {
     bool         graph_valid = false;
     // launch options (empm_ctx_set_option)
     int          sort_every = 16;          // 0 = direct path for rollouts too
-    int          p2g_tile = 1;
+    int          p2g_mode = 2;             // 0 direct reductions, 1 shared-memory tile, 2 warp-aggregated
     int          g2p_tile = 1;
     int          tile_cap = 1024;          // nodes per shared-memory tile (16 B each)
     SortedBuffers sb;

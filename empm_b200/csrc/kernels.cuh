@@ -247,12 +247,50 @@ __device__ __forceinline__ int particle_block(float4 xm, float inv_dx, int G, in
     return block_of(b[0], b[1], b[2], NB);
 }
 
-__global__ void k_sort_keys(const float4* x, int n, float inv_dx, int G, int NB, int* keys, int* ranks, int* counts) {
+// Sort key of a particle: its base cell in block-major order,
+// (block << 6) | in-block cell, so one counting sort orders particles by
+// 4^3 block and, inside a block, by cell. Out-of-band cells are clamped.
+__device__ __forceinline__ int particle_cell_key(float4 xm, float inv_dx, int G, int NB) {
+    int b[3];
+    const float gp[3] = {xm.x * inv_dx, xm.y * inv_dx, xm.z * inv_dx};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int t = (int)(gp[a] - 0.5f);
+        t = t < 0 ? 0 : (t >= G ? G - 1 : t);
+        b[a] = t;
+    }
+    return (block_of(b[0], b[1], b[2], NB) << 6) | ((b[0] & 3) << 4) | ((b[1] & 3) << 2) | (b[2] & 3);
+}
+
+__global__ void k_sort_keys(const float4* x, int n, float inv_dx, int G, int NB, int* keys, int* ranks,
+                            int* cell_counts, int* block_counts) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    const int b = particle_block(__ldg(x + p), inv_dx, G, NB);
-    keys[p] = b;
-    ranks[p] = atomicAdd(counts + b, 1);
+    const int key = particle_cell_key(__ldg(x + p), inv_dx, G, NB);
+    keys[p] = key;
+    ranks[p] = atomicAdd(cell_counts + key, 1);
+    atomicAdd(block_counts + (key >> 6), 1);
+}
+
+// Cell offsets: one warp per 4^3 block, exclusive scan of its 64 cell counts
+// added to the block's start offset; zeroes the cell counts for the next sort.
+__global__ void k_cell_scan(int* cell_counts, const int* block_offsets, int* cell_offsets, int nblocks) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nblocks) return;
+    const long long c0 = (long long)warp * 64 + 2 * lane;
+    const int a = cell_counts[c0], b = cell_counts[c0 + 1];
+    int incl = a + b;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    const int excl = incl - (a + b) + block_offsets[warp];
+    cell_offsets[c0] = excl;
+    cell_offsets[c0 + 1] = excl + a;
+    cell_counts[c0] = 0;
+    cell_counts[c0 + 1] = 0;
 }
 
 // Single-CTA exclusive scan over the block counts; writes the block start
@@ -314,11 +352,11 @@ struct PermuteArgs {
     const int*   pid_s; int*   pid_d;   // pid_s NULL: source is in caller order
     const int*   keys;
     const int*   ranks;
-    const int*   offsets;
+    const int*   offsets;    // cell offsets
     int n;
 };
 
-// src order -> sorted order: dst = offsets[keys[p]] + ranks[p]
+// src order -> sorted order: dst = cell_offsets[keys[p]] + ranks[p]
 __global__ void k_sort_scatter(const PermuteArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
@@ -484,6 +522,56 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a
         }
         __syncthreads();
     }
+}
+
+// P2G on cell-sorted particles with warp-aggregated reductions: lanes whose
+// particles share a base cell form a contiguous segment; for each of the 27
+// stencil nodes the segment's contributions are summed with shuffles and only
+// the segment head issues the 16-byte reduction to the grid.
+__global__ void __launch_bounds__(256) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, StepConsts c,
+                                                     float4* grid, unsigned char* flags) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    P2GParticle q;
+    bool valid = false;
+    if (p < c.n) valid = prepare_particle(P, M, Fe, c, p, q);
+    // a segment is a run of lanes with the same validity and base cell; lanes
+    // without a particle contribute zeros and never write
+    const int b0 = valid ? q.st.b[0] : lane, b1 = valid ? q.st.b[1] : 0, b2 = valid ? q.st.b[2] : 0;
+    const int u0 = __shfl_up_sync(0xffffffffu, b0, 1), u1 = __shfl_up_sync(0xffffffffu, b1, 1),
+              u2 = __shfl_up_sync(0xffffffffu, b2, 1);
+    const int uv = __shfl_up_sync(0xffffffffu, (int)valid, 1);
+    const bool head = lane == 0 || uv != (int)valid || u0 != b0 || u1 != b1 || u2 != b2;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const unsigned above = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
+    const int end = above ? (__ffs(above) - 2) : 31;
+    const int seglen = head ? end - lane + 1 : 1;
+    const int maxlen = __reduce_max_sync(0xffffffffu, seglen);
+    const int G = c.G;
+    const bool in_grid = valid && stencil_in_grid(q.st, G);
+    if (valid && !in_grid) atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
+    const float dt = c.step->dt;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float4 v = valid ? p2g_node(q, i, j, k, c.dx, c.inv_dx, dt) : make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int d = 1; d < maxlen; d <<= 1) {
+                    const float tx = __shfl_down_sync(0xffffffffu, v.x, d);
+                    const float ty = __shfl_down_sync(0xffffffffu, v.y, d);
+                    const float tz = __shfl_down_sync(0xffffffffu, v.z, d);
+                    const float tw = __shfl_down_sync(0xffffffffu, v.w, d);
+                    if (lane + d <= end) { v.x += tx; v.y += ty; v.z += tz; v.w += tw; }
+                }
+                if (head && valid) {
+                    const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
+                    if (in_grid || (ix >= 0 && iy >= 0 && iz >= 0 && ix < G && iy < G && iz < G))
+                        red_add_v4(grid + node_addr(ix, iy, iz, c.NB), v);
+                }
+            }
+    if (head && valid) mark_stencil_blocks(flags, q.st, G, c.NB);
 }
 
 struct TileFetch {

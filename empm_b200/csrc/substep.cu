@@ -116,7 +116,8 @@ static void free_sorted(SortedBuffers& sb) {
         if (sb.mati[i]) cudaFree(sb.mati[i]);
         sb.part[i] = nullptr; sb.matf[i] = nullptr; sb.mati[i] = nullptr;
     }
-    void* ptrs[] = {sb.fe, sb.keys, sb.ranks, sb.counts, sb.offsets, sb.chunks, sb.nchunks};
+    void* ptrs[] = {sb.fe, sb.keys, sb.ranks, sb.counts, sb.offsets, sb.cell_counts, sb.cell_offsets,
+                    sb.chunks, sb.nchunks};
     for (void* q : ptrs) if (q) cudaFree(q);
     sb = SortedBuffers();
 }
@@ -184,7 +185,10 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
             if (value < 0) return empm_set_error(ctx, EMPM_ERR_INVALID, "sort_every must be >= 0");
             ctx->sort_every = value;
             break;
-        case EMPM_OPT_P2G_TILE: ctx->p2g_tile = value != 0; break;
+        case EMPM_OPT_P2G_MODE:
+            if (value < 0 || value > 2) return empm_set_error(ctx, EMPM_ERR_INVALID, "p2g mode %d not in 0..2", value);
+            ctx->p2g_mode = value;
+            break;
         case EMPM_OPT_G2P_TILE: ctx->g2p_tile = value != 0; break;
         case EMPM_OPT_TILE_CAP:
             if (value < 27 || value > 4096) return empm_set_error(ctx, EMPM_ERR_INVALID, "tile_cap %d out of [27, 4096]", value);
@@ -381,6 +385,9 @@ static int ensure_sorted_buffers(EmpmCtx* ctx) {
     if (e == cudaSuccess) e = cudaMalloc(&sb.ranks, sizeof(int) * (size_t)n + 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.counts, sizeof(int) * nblocks);
     if (e == cudaSuccess) e = cudaMalloc(&sb.offsets, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.cell_counts, sizeof(int) * nblocks * 64);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.cell_offsets, sizeof(int) * nblocks * 64);
+    if (e == cudaSuccess) e = cudaMemset(sb.cell_counts, 0, sizeof(int) * nblocks * 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.chunks, sizeof(int2) * (size_t)sb.max_chunks);
     if (e == cudaSuccess) e = cudaMalloc(&sb.nchunks, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(sb.counts, 0, sizeof(int) * nblocks);
@@ -445,13 +452,16 @@ static int launch_sort(EmpmCtx* ctx, SortedState& ss, const ParticleArrays* user
     a.sel_d = const_cast<int*>(D.sel); a.pid_d = const_cast<int*>(D.pid);
     a.keys = sb.keys;
     a.ranks = sb.ranks;
-    a.offsets = sb.offsets;
+    a.offsets = sb.cell_offsets;
     a.n = n;
     k_sort_keys<<<blocks_for(n, 256), 256, 0, stream>>>(reinterpret_cast<const float4*>(a.src.x), n, inv_dx, G,
-                                                        ctx->NB, sb.keys, sb.ranks, sb.counts);
+                                                        ctx->NB, sb.keys, sb.ranks, sb.cell_counts, sb.counts);
     CK(cudaGetLastError(), "k_sort_keys");
     k_sort_scan<<<1, 1024, 0, stream>>>(sb.counts, sb.offsets, nblocks, TILE_THREADS, sb.chunks, sb.nchunks);
     CK(cudaGetLastError(), "k_sort_scan");
+    k_cell_scan<<<blocks_for((long long)nblocks * 32, 256), 256, 0, stream>>>(sb.cell_counts, sb.offsets,
+                                                                              sb.cell_offsets, nblocks);
+    CK(cudaGetLastError(), "k_cell_scan");
     k_sort_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(a);
     CK(cudaGetLastError(), "k_sort_scatter");
     ss.pc = dp;
@@ -472,21 +482,29 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, const EmpmStep* 
     t.grid = ctx->grid_mom;
     t.flags = ctx->flags;
     t.out = particle_arrays(sb.part[1 - ss.pc], n);
-    t.tile_cap = ctx->p2g_tile ? ctx->tile_cap : 0;
+    t.tile_cap = ctx->p2g_mode == 1 ? ctx->tile_cap : 0;
     const int persistent = ctx->sm_count * 2;
     const size_t smem = sizeof(float4) * (size_t)ctx->tile_cap;
     timing_mark(ctx, 0, 0, stream);
-    k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+    if (ctx->p2g_mode == 2) {
+        k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, stream>>>(t.P, t.M, t.Fe, t.c, ctx->grid_mom, ctx->flags);
+    } else {
+        k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+    }
     timing_mark(ctx, 0, 1, stream);
-    CK(cudaGetLastError(), "k_p2g_tiled");
+    CK(cudaGetLastError(), "k_p2g_sorted");
     int rc = launch_grid_update(ctx, d_step, stream);
     if (rc) return rc;
     t.grid = ctx->grid_vel;
     t.tile_cap = ctx->g2p_tile ? ctx->tile_cap : 0;
     timing_mark(ctx, 2, 0, stream);
-    k_g2p_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+    if (ctx->g2p_tile) {
+        k_g2p_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+    } else {
+        k_g2p_direct<<<blocks_for(n, 128), 128, 0, stream>>>(t.P, t.Fe, t.M, t.out, t.c, ctx->grid_vel);
+    }
     timing_mark(ctx, 2, 1, stream);
-    CK(cudaGetLastError(), "k_g2p_tiled");
+    CK(cudaGetLastError(), "k_g2p_sorted");
     ss.pc = 1 - ss.pc;
     return EMPM_OK;
 }
@@ -587,7 +605,7 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
     key.mat = *mat;
     key.n_steps = n_steps;
     key.sort_every = ctx->sort_every;
-    key.p2g_tile = ctx->p2g_tile;
+    key.p2g_mode = ctx->p2g_mode;
     key.g2p_tile = ctx->g2p_tile;
     key.tile_cap = ctx->tile_cap;
     if (!ctx->graph_valid || memcmp(&key, &ctx->graph_key, sizeof(key)) != 0) {

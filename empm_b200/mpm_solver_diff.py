@@ -85,7 +85,7 @@ class MPMWARPDiff(object):
         self.use_graph = True
         # launch options of the library (see EMPM_OPT_* in include/empm_b200.h)
         self.sort_every = 16
-        self.p2g_tile = True
+        self.p2g_mode = 2          # 0 direct, 1 shared-memory tile, 2 warp-aggregated
         self.g2p_tile = True
         self.tile_cap = 1024
 
@@ -154,7 +154,7 @@ class MPMWARPDiff(object):
             self._ctx = c = _Context(params, n, max(max_steps, 1024), device)
         else:
             c.set_params(params)
-        c.set_options({N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_TILE: int(bool(self.p2g_tile)),
+        c.set_options({N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_MODE: int(self.p2g_mode),
                        N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap)})
         return c
 

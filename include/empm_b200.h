@@ -212,7 +212,9 @@ int  empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMa
 
 /* Launch options of a context (empm_ctx_set_option). */
 #define EMPM_OPT_SORT_EVERY  1   /* rollouts re-sort particles by 4^3 cell block every N substeps; 0 = no sorting (default 16) */
-#define EMPM_OPT_P2G_TILE    2   /* 1 = P2G accumulates into shared-memory node tiles (default), 0 = direct reductions */
+#define EMPM_OPT_P2G_MODE    2   /* sorted-path P2G: 0 = one 16-byte reduction per particle and node,
+                                    1 = shared-memory node tile per chunk, 2 = warp-aggregated reductions
+                                    over same-cell particles (default) */
 #define EMPM_OPT_G2P_TILE    3   /* 1 = G2P stages the node tile in shared memory (default), 0 = direct gathers */
 #define EMPM_OPT_TILE_CAP    4   /* nodes per shared-memory tile, 27..3072 (default 1024 = 16 KiB) */
 

@@ -306,15 +306,16 @@ def test_status_word_flags_cfl_and_nan():
     assert solver.read_status() == 0   # reading clears the word
 
 
-@pytest.mark.parametrize("sort_every,p2g_tile,g2p_tile,tile_cap", [
-    (0, False, False, 1024),   # direct path
-    (1, True, True, 1024),
-    (4, True, False, 1024),
-    (16, False, True, 1024),
-    (16, True, True, 1024),
-    (16, True, True, 64),      # tiny tile: forces the fallback path for most chunks
+@pytest.mark.parametrize("sort_every,p2g_mode,g2p_tile,tile_cap", [
+    (0, 0, False, 1024),       # direct path
+    (1, 2, True, 1024),
+    (4, 1, False, 1024),
+    (16, 0, True, 1024),
+    (16, 1, True, 1024),
+    (16, 2, False, 1024),
+    (16, 1, True, 64),         # tiny tile: forces the fallback path for most chunks
 ])
-def test_sorted_path_vs_oracle(sort_every, p2g_tile, g2p_tile, tile_cap):
+def test_sorted_path_vs_oracle(sort_every, p2g_mode, g2p_tile, tile_cap):
     n, G, T, dt = 20000, 48, 120, 2e-4
     x, v, vol, rho, E, nu, ys = _c1_like(n, G, 11, 5, T, dt, plastic=True)
     v = (np.random.default_rng(12).standard_normal((n, 3)) * 0.5).astype(np.float32)
@@ -330,7 +331,7 @@ def test_sorted_path_vs_oracle(sort_every, p2g_tile, g2p_tile, tile_cap):
                             E, nu, ys, vol, rho, G, 5, gravity)
     solver = MPMWARPDiff()
     solver.initialize(n, n_grid=G)
-    solver.sort_every, solver.p2g_tile, solver.g2p_tile, solver.tile_cap = sort_every, p2g_tile, g2p_tile, tile_cap
+    solver.sort_every, solver.p2g_mode, solver.g2p_tile, solver.tile_cap = sort_every, p2g_mode, g2p_tile, tile_cap
     solver.add_surface_collider((0.0, 3.0 / G, 0.0), (0.0, 1.0, 0.0), "sticky", 0.0)
     solver.set_velocity_on_cuboid([0.5, 0.68, 0.5], [0.08, 0.05, 0.08], [0.0, -1.0, 0.0])
     solver.add_bounding_box()
@@ -338,7 +339,7 @@ def test_sorted_path_vs_oracle(sort_every, p2g_tile, g2p_tile, tile_cap):
     res = solver.rollout(md, st, other, dt, T)
     torch.cuda.synchronize()
     err = max_abs(res.particle_x, sim.x)
-    print(f"sort_every={sort_every} tiles=({p2g_tile},{g2p_tile}) cap={tile_cap}: max pos err {err:.3e}")
+    print(f"sort_every={sort_every} p2g_mode={p2g_mode} g2p_tile={g2p_tile} cap={tile_cap}: max pos err {err:.3e}")
     assert err <= POS_GATE
     _rel_close(md.yield_stress, sim.ys, 2e-3, 1.0, "yield")
     _rel_close(res.particle_F_trial.reshape(n, 9), sim.F_trial, 2e-3, 1.0, "F_trial")
