@@ -1,21 +1,26 @@
-// ctx.hpp — the opaque EmpmCtx behind the C ABI.
+// ctx.hpp — the opaque EmpmCtx behind the C ABI: one batch of independent
+// simulation instances (a single simulation is a batch of one).
 #pragma once
 #include <cuda_runtime.h>
 #include <vector>
 #include "../../include/empm_b200.h"
+
+namespace empm { struct InstanceConsts; }
 
 struct GraphKey {
     EmpmParticles a;
     EmpmParticles b;
     EmpmMaterial  mat;
     int           n_steps;
+    int           n_tables;
     int           sort_every;
     int           p2g_mode;
     int           g2p_tile;
     int           tile_cap;
+    unsigned long long params_version;
 };
 
-// Particle and material buffers of the sorted path (cell-block order).
+// Particle and material buffers of the sorted path (cell order).
 struct SortedBuffers {
     bool   allocated = false;
     int    n = 0;
@@ -25,26 +30,38 @@ struct SortedBuffers {
     int*   mati[2] = {nullptr, nullptr};   // sel | pid
     int*   keys = nullptr;
     int*   ranks = nullptr;
-    int*   counts = nullptr;               // [NB^3] particles per block, zero between sorts
-    int*   offsets = nullptr;              // [NB^3] block start offsets
-    int*   cell_counts = nullptr;          // [NB^3 * 64], zero between sorts
-    int*   cell_offsets = nullptr;         // [NB^3 * 64]
+    int*   block_counts = nullptr;         // [nblocks], zero between sorts
+    int*   block_offsets = nullptr;        // [nblocks]
+    int*   chunk_counts = nullptr;         // [nblocks]
+    int*   chunk_offsets = nullptr;        // [nblocks]
+    int*   cell_counts = nullptr;          // [nblocks * 64], zero between sorts
+    int*   cell_offsets = nullptr;         // [nblocks * 64]
     int2*  chunks = nullptr;               // [max_chunks]
     int*   nchunks = nullptr;
     int    max_chunks = 0;
+    void*  scan_tmp = nullptr;             // CUB scan scratch
+    size_t scan_tmp_bytes = 0;
 };
 
 struct EmpmCtx {
-    EmpmModelParams params{};
+    // instances
+    int          n_inst = 0;
+    std::vector<EmpmModelParams> params;   // per instance
+    std::vector<int> counts;               // particles per instance
+    std::vector<int> poff;                 // first particle of each instance
+    std::vector<int> boff;                 // first global 4^3 block of each instance
+    int          n_particles = 0;          // total
+    long long    nblocks = 0;              // total 4^3 grid blocks
+    empm::InstanceConsts* d_inst = nullptr;
+    unsigned long long params_version = 0;
+    // device
     int          device = 0;
     int          sm_count = 148;
-    int          n_particles = 0;
-    int          max_steps = 0;
-    int          NB = 0;                   // 4^3 node blocks per axis
+    int          max_tables = 0;           // capacity of the step-table array, in tables of n_inst steps
     float4*      grid_mom = nullptr;       // P2G accumulation (px, py, pz, m), blocked layout; zero between substeps
     float4*      grid_vel = nullptr;       // node velocity after the grid update, blocked layout
     unsigned char* flags = nullptr;        // touched node blocks of the current substep
-    EmpmStep*    d_steps = nullptr;        // device copy of the step schedule
+    EmpmStep*    d_steps = nullptr;        // device copy of the step schedules
     unsigned*    d_status = nullptr;       // EMPM_STATUS_* bits
     cudaStream_t own_stream = nullptr;     // capture stream for the graph path
     cudaEvent_t  ev_a = nullptr;
@@ -55,7 +72,7 @@ struct EmpmCtx {
     // launch options (empm_ctx_set_option)
     int          sort_every = 16;          // 0 = direct path for rollouts too
     int          p2g_mode = 2;             // 0 direct reductions, 1 shared-memory tile, 2 warp-aggregated
-    int          g2p_tile = 1;
+    int          g2p_tile = 0;
     int          tile_cap = 1024;          // nodes per shared-memory tile (16 B each)
     SortedBuffers sb;
     // per-kernel event timing (stream path only)

@@ -1,14 +1,22 @@
-// kernels.cuh — __global__ kernels of one MLS-MPM substep.
+// kernels.cuh — __global__ kernels of one MLS-MPM substep over a batch of
+// independent simulation instances (a single simulation is a batch of one).
 //
-// Two launch paths share the per-particle / per-node device functions of
-// substep.cuh:
-//   * the direct path (empm_substep): particles in the caller's order, one
-//     particle per thread, 16-byte vector reductions straight into the grid;
-//   * the sorted path (empm_rollout): particles cell-block sorted every
-//     `sort_every` substeps; P2G accumulates each chunk of sorted particles
-//     into a shared-memory tile of nodes and flushes it with one vector
-//     reduction per node; G2P stages the chunk's node tile in shared memory;
-//     the grid update visits only the 4^3 node blocks P2G touched.
+// Batch layout: the particles of instance i occupy [poff_i, poff_i + n_i) of
+// every particle array, both in the caller's order and in the library's
+// cell-sorted order (the sort key starts with the instance's grid blocks, so
+// a sort never moves a particle across instances); the grids are the
+// instances' blocked grids one after the other, instance i starting at the
+// global 4^3 block boff_i. Every kernel looks its instance up in a small
+// device table by particle index or block index.
+//
+// Launch paths:
+//   * direct: one particle per thread, 16-byte vector reductions into the grid;
+//   * sorted (rollouts): particles in cell order, re-sorted every few substeps;
+//     P2G sums the contributions of same-cell particles of a warp with
+//     shuffles and issues one reduction per cell and node (default), or
+//     accumulates per chunk in a shared-memory node tile (option);
+//     G2P gathers directly or from a staged shared-memory tile (option);
+//   * the grid update visits only the 4^3 node blocks that P2G touched.
 #pragma once
 #include <limits.h>
 #include "../../include/empm_b200.h"
@@ -18,7 +26,80 @@
 namespace empm {
 
 // -------------------------------------------------------------------------
-// common argument blocks
+// instance table and per-launch context
+// -------------------------------------------------------------------------
+struct InstanceConsts {
+    int   n, poff;            // particles
+    int   G, NB, boff;        // grid: resolution, blocks per axis, first global block
+    float dx, inv_dx, grid_lim, rpic, damping;
+    float g[3];
+    MaterialScalars ms;
+};
+
+struct Launch {
+    const InstanceConsts* inst;
+    int             n_inst;
+    int             n_total;       // particles over all instances
+    int             nblocks;       // grid blocks over all instances
+    const EmpmStep* steps;         // device step tables: steps[table * n_inst + instance]
+    int             table;         // step table of this substep
+    unsigned*       status;
+};
+
+// per-instance view used by the particle/node device functions
+struct StepConsts {
+    int   G, NB, boff;
+    float dx, inv_dx, grid_lim, rpic;
+    MaterialScalars ms;
+    const EmpmStep* step;
+    unsigned* status;
+};
+
+__device__ __forceinline__ int find_instance_particle(const Launch& L, int p) {
+    int lo = 0, hi = L.n_inst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&L.inst[mid].poff) <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int find_instance_block(const Launch& L, int b) {
+    int lo = 0, hi = L.n_inst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&L.inst[mid].boff) <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ StepConsts consts_of(const Launch& L, int i) {
+    const InstanceConsts* I = L.inst + i;
+    StepConsts c;
+    c.G = __ldg(&I->G);
+    c.NB = __ldg(&I->NB);
+    c.boff = __ldg(&I->boff);
+    c.dx = __ldg(&I->dx);
+    c.inv_dx = __ldg(&I->inv_dx);
+    c.grid_lim = __ldg(&I->grid_lim);
+    c.rpic = __ldg(&I->rpic);
+    c.ms.material = __ldg(&I->ms.material);
+    c.ms.softening = __ldg(&I->ms.softening);
+    c.ms.hardening = __ldg(&I->ms.hardening);
+    c.ms.xi = __ldg(&I->ms.xi);
+    c.ms.plastic_viscosity = __ldg(&I->ms.plastic_viscosity);
+    c.ms.alpha = __ldg(&I->ms.alpha);
+    c.step = L.steps + (size_t)L.table * L.n_inst + i;
+    c.status = L.status;
+    return c;
+}
+
+__device__ __forceinline__ long long gaddr(const StepConsts& c, int i, int j, int k) {
+    return ((long long)(c.boff + block_of(i, j, k, c.NB)) << 6) | ((i & 3) << 4) | ((j & 3) << 2) | (k & 3);
+}
+
+// -------------------------------------------------------------------------
+// particle arrays
 // -------------------------------------------------------------------------
 struct ParticleArrays {
     float4*  x;      // (x, y, z, mass)
@@ -35,40 +116,6 @@ struct MaterialArrays {
     const int*   sel;   // NULL = all simulated
     const int*   pid;   // caller index of each particle (NULL = identity)
 };
-
-struct StepConsts {
-    int   n;
-    int   G;
-    int   NB;
-    float dx, inv_dx;
-    float grid_lim;
-    float rpic;
-    MaterialScalars ms;
-    const EmpmStep* step;
-    unsigned* status;
-};
-
-struct ChunkList {
-    const int2* chunks;    // (first sorted index, count)
-    const int*  nchunks;   // device count
-};
-
-__device__ __forceinline__ float sel3(const float (&a)[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
-
-// p2g_node with runtime stencil offsets (no local-memory indexing)
-__device__ __forceinline__ float4 p2g_node_dyn(const P2GParticle& q, int i, int j, int k, float dx, float inv_dx,
-                                               float dt) {
-    const Stencil& st = q.st;
-    const float wx = sel3(st.w[0], i), wy = sel3(st.w[1], j), wz = sel3(st.w[2], k);
-    const float dwx = sel3(st.dw[0], i), dwy = sel3(st.dw[1], j), dwz = sel3(st.dw[2], k);
-    const V3 dpos = v3(((float)i - st.fx[0]) * dx, ((float)j - st.fx[1]) * dx, ((float)k - st.fx[2]) * dx);
-    const float weight = wx * wy * wz;
-    const V3 dweight = v3(dwx * wy * wz, wx * dwy * wz, wx * wy * dwz) * inv_dx;
-    const float wm = weight * q.wm_scale;
-    const V3 force = q.Sv * dweight;
-    const V3 add = wm * (q.v + q.Cd * dpos) + dt * force;
-    return make_float4(add.x, add.y, add.z, wm);
-}
 
 // Stress + everything P2G needs for particle p (modifiers applied, material
 // write-back, elastic F handed to G2P). Returns false for unsimulated particles.
@@ -96,12 +143,13 @@ __device__ __forceinline__ bool prepare_particle(const ParticleArrays& P, const 
     return true;
 }
 
-__device__ __forceinline__ void mark_stencil_blocks(unsigned char* flags, const Stencil& st, int G, int NB) {
+__device__ __forceinline__ void mark_stencil_blocks(unsigned char* flags, const Stencil& st, const StepConsts& c) {
+    const int G = c.G;
     const int lo[3] = {max(st.b[0], 0), max(st.b[1], 0), max(st.b[2], 0)};
     const int hi[3] = {min(st.b[0] + 2, G - 1), min(st.b[1] + 2, G - 1), min(st.b[2] + 2, G - 1)};
     for (int bi = lo[0] >> 2; bi <= hi[0] >> 2; ++bi)
         for (int bj = lo[1] >> 2; bj <= hi[1] >> 2; ++bj)
-            for (int bk = lo[2] >> 2; bk <= hi[2] >> 2; ++bk) flags[(bi * NB + bj) * NB + bk] = 1;
+            for (int bk = lo[2] >> 2; bk <= hi[2] >> 2; ++bk) flags[c.boff + (bi * c.NB + bj) * c.NB + bk] = 1;
 }
 
 // direct scatter of one prepared particle into the blocked grid
@@ -110,27 +158,23 @@ __device__ __forceinline__ void scatter_global(const P2GParticle& q, const StepC
     const int G = c.G;
     const bool in_grid = stencil_in_grid(q.st, G);
     if (!in_grid) atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
-    const float dt = c.step->dt;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
-                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) continue;
-                red_add_v4(grid + node_addr(ix, iy, iz, c.NB), p2g_node(q, i, j, k, c.dx, c.inv_dx, dt));
-            }
-    mark_stencil_blocks(flags, q.st, G, c.NB);
+    const P2GPre pre = p2g_pre(q, c.dx, c.inv_dx, c.step->dt);
+    p2g_emit(pre, [&](int i, int j, int k, float4 v) {
+        const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
+        if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) return;
+        red_add_v4(grid + gaddr(c, ix, iy, iz), v);
+    });
+    mark_stencil_blocks(flags, q.st, c);
 }
 
 // -------------------------------------------------------------------------
 // direct path
 // -------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_p2g_direct(ParticleArrays P, MaterialArrays M, F9Planes Fe, StepConsts c,
+__global__ void __launch_bounds__(128) k_p2g_direct(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
                                                     float4* grid, unsigned char* flags) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= c.n) return;
+    if (p >= L.n_total) return;
+    const StepConsts c = consts_of(L, find_instance_particle(L, p));
     P2GParticle q;
     if (!prepare_particle(P, M, Fe, c, p, q)) return;
     scatter_global(q, c, grid, flags);
@@ -143,33 +187,32 @@ struct GridUpdateArgs {
     float4*        mom;      // accumulation; zeroed here for the next substep
     float4*        vel;      // node velocity after the boundary conditions (w = node mass)
     unsigned char* flags;    // touched blocks; cleared here
-    int            G, NB;
-    float          dx;
-    V3             g;
-    float          damping;
-    const EmpmStep* step;
+    Launch         L;
 };
 
 __global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs a) {
-    const int nblocks = a.NB * a.NB * a.NB;
+    const int nblocks = a.L.nblocks;
     const int group = threadIdx.x >> 6;   // 4 node blocks per iteration
     const int lane = threadIdx.x & 63;
-    const EmpmStep& st = *a.step;
     for (int base = blockIdx.x * 4; base < nblocks; base += gridDim.x * 4) {
         const int b = base + group;
         const bool active = b < nblocks && a.flags[b] != 0;
         __syncthreads();   // every group has read its flag before any is cleared
         if (active) {
+            const int inst = find_instance_block(a.L, b);
+            const InstanceConsts* I = a.L.inst + inst;
+            const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
+            const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
             const long long node = ((long long)b << 6) | lane;
             const float4 m = a.mom[node];
             a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
-            V3 v = grid_velocity(m, st.dt, a.g, a.damping);
+            V3 v = grid_velocity(m, st.dt, v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2])), __ldg(&I->damping));
             if (st.n_colliders > 0) {
                 int i, j, k;
-                node_coords(node, a.NB, i, j, k);
-                if (i < a.G && j < a.G && k < a.G) {
-                    const long long dense = ((long long)i * a.G + j) * a.G + k;
-                    apply_colliders(st, i, j, k, a.G, a.dx, dense, v);
+                node_coords(((long long)(b - boff) << 6) | lane, NB, i, j, k);
+                if (i < G && j < G && k < G) {
+                    const long long dense = ((long long)i * G + j) * G + k;
+                    apply_colliders(st, i, j, k, G, __ldg(&I->dx), dense, v);
                 }
             }
             a.vel[node] = make_float4(v.x, v.y, v.z, m.w);
@@ -215,69 +258,72 @@ __device__ __forceinline__ void g2p_particle(const ParticleArrays& P, F9Planes F
 
 struct GlobalFetch {
     const float4* vel;
-    int G, NB;
+    const StepConsts* c;
     __device__ __forceinline__ V3 operator()(const Stencil& st, bool in_grid, int i, int j, int k) const {
         const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
+        const int G = c->G;
         if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) return v3(0.f, 0.f, 0.f);
-        const float4 g = __ldg(vel + node_addr(ix, iy, iz, NB));
+        const float4 g = __ldg(vel + gaddr(*c, ix, iy, iz));
         return v3(g.x, g.y, g.z);
     }
 };
 
 __global__ void __launch_bounds__(128) k_g2p_direct(ParticleArrays P, F9Planes Fe, MaterialArrays M,
-                                                    ParticleArrays out, StepConsts c, const float4* vel) {
+                                                    ParticleArrays out, Launch L, const float4* vel) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= c.n) return;
-    GlobalFetch f{vel, c.G, c.NB};
+    if (p >= L.n_total) return;
+    const StepConsts c = consts_of(L, find_instance_particle(L, p));
+    GlobalFetch f{vel, &c};
     g2p_particle(P, Fe, M, out, c, p, f);
 }
 
 // -------------------------------------------------------------------------
-// sorted path: cell-block keys, scan, permutation
+// sorted path: cell keys, counting sort, permutation
 // -------------------------------------------------------------------------
-__device__ __forceinline__ int particle_block(float4 xm, float inv_dx, int G, int NB) {
-    int b[3];
-    const float gp[3] = {xm.x * inv_dx, xm.y * inv_dx, xm.z * inv_dx};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        int t = (int)(gp[a] - 0.5f);
-        t = t < 0 ? 0 : (t >= G ? G - 1 : t);
-        b[a] = t;
-    }
-    return block_of(b[0], b[1], b[2], NB);
-}
-
-// Sort key of a particle: its base cell in block-major order,
-// (block << 6) | in-block cell, so one counting sort orders particles by
-// 4^3 block and, inside a block, by cell. Out-of-band cells are clamped.
-__device__ __forceinline__ int particle_cell_key(float4 xm, float inv_dx, int G, int NB) {
-    int b[3];
-    const float gp[3] = {xm.x * inv_dx, xm.y * inv_dx, xm.z * inv_dx};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        int t = (int)(gp[a] - 0.5f);
-        t = t < 0 ? 0 : (t >= G ? G - 1 : t);
-        b[a] = t;
-    }
-    return (block_of(b[0], b[1], b[2], NB) << 6) | ((b[0] & 3) << 4) | ((b[1] & 3) << 2) | (b[2] & 3);
-}
-
-__global__ void k_sort_keys(const float4* x, int n, float inv_dx, int G, int NB, int* keys, int* ranks,
-                            int* cell_counts, int* block_counts) {
+// Sort key of a particle: its base cell in block-major order over the whole
+// batch, ((boff + block) << 6) | in-block cell, so one counting sort orders
+// particles by instance, 4^3 block and cell. Out-of-band cells are clamped.
+__global__ void k_sort_keys(const float4* x, Launch L, int* keys, int* ranks, int* cell_counts, int* block_counts) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
-    const int key = particle_cell_key(__ldg(x + p), inv_dx, G, NB);
+    if (p >= L.n_total) return;
+    const int inst = find_instance_particle(L, p);
+    const InstanceConsts* I = L.inst + inst;
+    const int G = __ldg(&I->G), NB = __ldg(&I->NB);
+    const float inv_dx = __ldg(&I->inv_dx);
+    const float4 xm = __ldg(x + p);
+    const float gp[3] = {xm.x * inv_dx, xm.y * inv_dx, xm.z * inv_dx};
+    int b[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int t = (int)(gp[a] - 0.5f);
+        b[a] = t < 0 ? 0 : (t >= G ? G - 1 : t);
+    }
+    const int blk = __ldg(&I->boff) + block_of(b[0], b[1], b[2], NB);
+    const int key = (blk << 6) | ((b[0] & 3) << 4) | ((b[1] & 3) << 2) | (b[2] & 3);
     keys[p] = key;
     ranks[p] = atomicAdd(cell_counts + key, 1);
-    atomicAdd(block_counts + (key >> 6), 1);
+    atomicAdd(block_counts + blk, 1);
 }
 
-// Cell offsets: one warp per 4^3 block, exclusive scan of its 64 cell counts
-// added to the block's start offset; zeroes the cell counts for the next sort.
-__global__ void k_cell_scan(int* cell_counts, const int* block_offsets, int* cell_offsets, int nblocks) {
+// number of chunks (<= `chunk` particles, never spanning two blocks) per block
+__global__ void k_chunk_counts(const int* block_counts, int* chunk_counts, int nblocks, int chunk) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    chunk_counts[b] = (block_counts[b] + chunk - 1) / chunk;
+}
+
+// Cell offsets: one warp per block, exclusive scan of its 64 cell counts on
+// top of the block's start offset; writes the block's chunks; zeroes the
+// counts for the next sort. Empty blocks only report the chunk total.
+__global__ void k_cell_scan(int* cell_counts, int* block_counts, const int* block_offsets, const int* chunk_offsets,
+                            const int* chunk_counts, int* cell_offsets, int2* chunks, int* nchunks, int nblocks,
+                            int chunk) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= nblocks) return;
+    const int cnt = block_counts[warp];
+    if (warp == nblocks - 1 && lane == 0) *nchunks = chunk_offsets[warp] + chunk_counts[warp];
+    if (cnt == 0) return;
     const long long c0 = (long long)warp * 64 + 2 * lane;
     const int a = cell_counts[c0], b = cell_counts[c0 + 1];
     int incl = a + b;
@@ -286,60 +332,16 @@ __global__ void k_cell_scan(int* cell_counts, const int* block_offsets, int* cel
         const int t = __shfl_up_sync(0xffffffffu, incl, d);
         if (lane >= d) incl += t;
     }
-    const int excl = incl - (a + b) + block_offsets[warp];
+    const int off = block_offsets[warp];
+    const int excl = incl - (a + b) + off;
     cell_offsets[c0] = excl;
     cell_offsets[c0 + 1] = excl + a;
     cell_counts[c0] = 0;
     cell_counts[c0 + 1] = 0;
-}
-
-// Single-CTA exclusive scan over the block counts; writes the block start
-// offsets, the chunk list (chunks never span two blocks) and its length, and
-// zeroes the counts for the next sort. 1024 threads, contiguous segments.
-__global__ void __launch_bounds__(1024) k_sort_scan(int* counts, int* offsets, int nblocks, int chunk, int2* chunks,
-                                                    int* nchunks) {
-    __shared__ int s_warp_p[32], s_warp_c[32];
-    const int t = threadIdx.x;
-    const int seg = (nblocks + 1023) / 1024;
-    const int b0 = min(t * seg, nblocks), b1 = min(b0 + seg, nblocks);
-    int sp = 0, sc = 0;
-    for (int b = b0; b < b1; ++b) {
-        const int cnt = counts[b];
-        sp += cnt;
-        sc += (cnt + chunk - 1) / chunk;
-    }
-    // CTA exclusive scan of (sp, sc)
-    const int lane = t & 31, w = t >> 5;
-    int ip = sp, ic = sc;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int np = __shfl_up_sync(0xffffffffu, ip, d), nc = __shfl_up_sync(0xffffffffu, ic, d);
-        if (lane >= d) { ip += np; ic += nc; }
-    }
-    if (lane == 31) { s_warp_p[w] = ip; s_warp_c[w] = ic; }
-    __syncthreads();
-    if (w == 0) {
-        int vp = s_warp_p[lane], vc = s_warp_c[lane];
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int np = __shfl_up_sync(0xffffffffu, vp, d), nc = __shfl_up_sync(0xffffffffu, vc, d);
-            if (lane >= d) { vp += np; vc += nc; }
-        }
-        s_warp_p[lane] = vp;
-        s_warp_c[lane] = vc;
-    }
-    __syncthreads();
-    int off_p = ip - sp + (w > 0 ? s_warp_p[w - 1] : 0);
-    int off_c = ic - sc + (w > 0 ? s_warp_c[w - 1] : 0);
-    for (int b = b0; b < b1; ++b) {
-        const int cnt = counts[b];
-        offsets[b] = off_p;
-        for (int k = 0; k * chunk < cnt; ++k) chunks[off_c + k] = make_int2(off_p + k * chunk, min(chunk, cnt - k * chunk));
-        off_p += cnt;
-        off_c += (cnt + chunk - 1) / chunk;
-        counts[b] = 0;
-    }
-    if (t == 1023) *nchunks = off_c;
+    const int co = chunk_offsets[warp];
+    for (int k = lane; k * chunk < cnt; k += 32) chunks[co + k] = make_int2(off + k * chunk, min(chunk, cnt - k * chunk));
+    __syncwarp();
+    if (lane == 0) block_counts[warp] = 0;
 }
 
 struct PermuteArgs {
@@ -398,9 +400,86 @@ __global__ void k_unsort(const UnsortArgs a) {
 }
 
 // -------------------------------------------------------------------------
-// sorted path: tiled P2G and G2P over chunks of sorted particles
+// sorted path, default P2G: warp-aggregated reductions
+// -------------------------------------------------------------------------
+// Lanes whose particles share an instance and base cell form a contiguous
+// segment of the warp (cell-sorted order); for each of the 27 stencil nodes
+// the segment's contributions are summed with shuffles and only the segment
+// head issues the 16-byte reduction to the grid.
+__global__ void __launch_bounds__(256) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
+                                                     float4* grid, unsigned char* flags) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int inst = p < L.n_total ? find_instance_particle(L, p) : 0;
+    const StepConsts c = consts_of(L, inst);
+    P2GParticle q;
+    bool valid = false;
+    if (p < L.n_total) valid = prepare_particle(P, M, Fe, c, p, q);
+    // a segment is a run of lanes with the same validity, instance and base
+    // cell; lanes without a particle contribute zeros and never write
+    const int b0 = valid ? q.st.b[0] : lane, b1 = valid ? q.st.b[1] : 0, b2 = valid ? q.st.b[2] : 0;
+    const int u0 = __shfl_up_sync(0xffffffffu, b0, 1), u1 = __shfl_up_sync(0xffffffffu, b1, 1),
+              u2 = __shfl_up_sync(0xffffffffu, b2, 1);
+    const int uv = __shfl_up_sync(0xffffffffu, (int)valid, 1);
+    const int ui = __shfl_up_sync(0xffffffffu, inst, 1);
+    const bool head = lane == 0 || uv != (int)valid || ui != inst || u0 != b0 || u1 != b1 || u2 != b2;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const unsigned above = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
+    const int end = above ? (__ffs(above) - 2) : 31;
+    const int seglen = head ? end - lane + 1 : 1;
+    const int maxlen = __reduce_max_sync(0xffffffffu, seglen);
+    const int G = c.G;
+    const bool in_grid = valid && stencil_in_grid(q.st, G);
+    if (valid && !in_grid) atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
+    P2GPre pre;
+    if (valid) {
+        pre = p2g_pre(q, c.dx, c.inv_dx, c.step->dt);
+    } else {
+        pre.st = make_stencil(v3(0.f, 0.f, 0.f), 1.f);
+        pre.m = 0.f;
+        pre.a = v3(0.f, 0.f, 0.f);
+        pre.B = m3_zero();
+        pre.S = m3_zero();
+    }
+    p2g_emit(pre, [&](int i, int j, int k, float4 v) {
+        for (int d = 1; d < maxlen; d <<= 1) {
+            const float tx = __shfl_down_sync(0xffffffffu, v.x, d);
+            const float ty = __shfl_down_sync(0xffffffffu, v.y, d);
+            const float tz = __shfl_down_sync(0xffffffffu, v.z, d);
+            const float tw = __shfl_down_sync(0xffffffffu, v.w, d);
+            if (lane + d <= end) { v.x += tx; v.y += ty; v.z += tz; v.w += tw; }
+        }
+        if (head && valid) {
+            const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
+            if (in_grid || (ix >= 0 && iy >= 0 && iz >= 0 && ix < G && iy < G && iz < G))
+                red_add_v4(grid + gaddr(c, ix, iy, iz), v);
+        }
+    });
+    if (head && valid) mark_stencil_blocks(flags, q.st, c);
+}
+
+// -------------------------------------------------------------------------
+// sorted path, optional: shared-memory node tiles over chunks of particles
 // -------------------------------------------------------------------------
 constexpr int TILE_THREADS = 256;     // = chunk size
+
+struct ChunkList {
+    const int2* chunks;    // (first sorted index, count); never spans two 4^3 blocks
+    const int*  nchunks;   // device count
+};
+
+__device__ __forceinline__ float sel3(const float (&a)[3], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]); }
+
+// one node contribution with runtime stencil offsets (no local-memory indexing)
+__device__ __forceinline__ float4 p2g_node_dyn(const P2GPre& p, int i, int j, int k) {
+    const Stencil& st = p.st;
+    const float wx = sel3(st.w[0], i), wy = sel3(st.w[1], j), wz = sel3(st.w[2], k);
+    const float dwx = sel3(st.dw[0], i), dwy = sel3(st.dw[1], j), dwz = sel3(st.dw[2], k);
+    const V3 a = p.a + (float)i * col(p.B, 0) + (float)j * col(p.B, 1) + (float)k * col(p.B, 2);
+    const float wm = (wx * wy * wz) * p.m;
+    const V3 c = wm * a + (dwx * wy * wz) * col(p.S, 0) + (wx * dwy * wz) * col(p.S, 1) + (wx * wy * dwz) * col(p.S, 2);
+    return make_float4(c.x, c.y, c.z, wm);
+}
 
 struct TileBox {
     int o[3];   // origin node
@@ -442,7 +521,7 @@ struct TiledArgs {
     ParticleArrays P;
     MaterialArrays M;
     F9Planes Fe;
-    StepConsts c;
+    Launch L;
     ChunkList cl;
     float4* grid;             // P2G: accumulation; G2P: node velocities
     unsigned char* flags;     // P2G marks touched blocks
@@ -454,10 +533,10 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a
     extern __shared__ float4 tile[];
     __shared__ int s_min[3], s_max[3];
     const int nch = *a.cl.nchunks;
-    const StepConsts& c = a.c;
-    const float dt = c.step->dt;
     for (int ci = blockIdx.x; ci < nch; ci += gridDim.x) {
         const int2 ch = a.cl.chunks[ci];
+        const StepConsts c = consts_of(a.L, find_instance_particle(a.L, ch.x));
+        const float dt = c.step->dt;
         const int p = ch.x + (int)threadIdx.x;
         bool active = threadIdx.x < (unsigned)ch.y;
         int base[3] = {0, 0, 0};
@@ -477,13 +556,14 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a
             P2GParticle q;
             if (prepare_particle(a.P, a.M, a.Fe, c, p, q)) {
                 if (use_tile) {
+                    const P2GPre pre = p2g_pre(q, c.dx, c.inv_dx, dt);
                     // stagger the 27 stencil offsets across lanes so particles of the
                     // same cell do not hit the same shared-memory node together
                     int s = (int)(threadIdx.x % 27u);
                     int i = s / 9, j = (s / 3) % 3, k = s % 3;
                     const int li0 = q.st.b[0] - tb.o[0], lj0 = q.st.b[1] - tb.o[1], lk0 = q.st.b[2] - tb.o[2];
                     for (int it = 0; it < 27; ++it) {
-                        const float4 v = p2g_node_dyn(q, i, j, k, c.dx, c.inv_dx, dt);
+                        const float4 v = p2g_node_dyn(pre, i, j, k);
                         float* dst = reinterpret_cast<float*>(tile + ((li0 + i) * tb.e[1] + (lj0 + j)) * tb.e[2] + (lk0 + k));
                         atomicAdd(dst + 0, v.x);
                         atomicAdd(dst + 1, v.y);
@@ -507,7 +587,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a
                     atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
                     continue;
                 }
-                red_add_v4(a.grid + node_addr(gi, gj, gk, c.NB), v);
+                red_add_v4(a.grid + gaddr(c, gi, gj, gk), v);
             }
             // mark the 4^3 blocks the tile overlaps
             const int lo[3] = {max(tb.o[0], 0) >> 2, max(tb.o[1], 0) >> 2, max(tb.o[2], 0) >> 2};
@@ -517,61 +597,11 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a
             const int nmark = (n0 > 0 && n1 > 0 && n2 > 0) ? n0 * n1 * n2 : 0;
             for (int t = threadIdx.x; t < nmark; t += TILE_THREADS) {
                 const int bi = lo[0] + t / (n1 * n2), bj = lo[1] + (t / n2) % n1, bk = lo[2] + t % n2;
-                a.flags[(bi * c.NB + bj) * c.NB + bk] = 1;
+                a.flags[c.boff + (bi * c.NB + bj) * c.NB + bk] = 1;
             }
         }
         __syncthreads();
     }
-}
-
-// P2G on cell-sorted particles with warp-aggregated reductions: lanes whose
-// particles share a base cell form a contiguous segment; for each of the 27
-// stencil nodes the segment's contributions are summed with shuffles and only
-// the segment head issues the 16-byte reduction to the grid.
-__global__ void __launch_bounds__(256) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, StepConsts c,
-                                                     float4* grid, unsigned char* flags) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    P2GParticle q;
-    bool valid = false;
-    if (p < c.n) valid = prepare_particle(P, M, Fe, c, p, q);
-    // a segment is a run of lanes with the same validity and base cell; lanes
-    // without a particle contribute zeros and never write
-    const int b0 = valid ? q.st.b[0] : lane, b1 = valid ? q.st.b[1] : 0, b2 = valid ? q.st.b[2] : 0;
-    const int u0 = __shfl_up_sync(0xffffffffu, b0, 1), u1 = __shfl_up_sync(0xffffffffu, b1, 1),
-              u2 = __shfl_up_sync(0xffffffffu, b2, 1);
-    const int uv = __shfl_up_sync(0xffffffffu, (int)valid, 1);
-    const bool head = lane == 0 || uv != (int)valid || u0 != b0 || u1 != b1 || u2 != b2;
-    const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const unsigned above = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
-    const int end = above ? (__ffs(above) - 2) : 31;
-    const int seglen = head ? end - lane + 1 : 1;
-    const int maxlen = __reduce_max_sync(0xffffffffu, seglen);
-    const int G = c.G;
-    const bool in_grid = valid && stencil_in_grid(q.st, G);
-    if (valid && !in_grid) atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
-    const float dt = c.step->dt;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                float4 v = valid ? p2g_node(q, i, j, k, c.dx, c.inv_dx, dt) : make_float4(0.f, 0.f, 0.f, 0.f);
-                for (int d = 1; d < maxlen; d <<= 1) {
-                    const float tx = __shfl_down_sync(0xffffffffu, v.x, d);
-                    const float ty = __shfl_down_sync(0xffffffffu, v.y, d);
-                    const float tz = __shfl_down_sync(0xffffffffu, v.z, d);
-                    const float tw = __shfl_down_sync(0xffffffffu, v.w, d);
-                    if (lane + d <= end) { v.x += tx; v.y += ty; v.z += tz; v.w += tw; }
-                }
-                if (head && valid) {
-                    const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
-                    if (in_grid || (ix >= 0 && iy >= 0 && iz >= 0 && ix < G && iy < G && iz < G))
-                        red_add_v4(grid + node_addr(ix, iy, iz, c.NB), v);
-                }
-            }
-    if (head && valid) mark_stencil_blocks(flags, q.st, G, c.NB);
 }
 
 struct TileFetch {
@@ -587,9 +617,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_g2p_tiled(const TiledArgs a
     extern __shared__ float4 tile[];
     __shared__ int s_min[3], s_max[3];
     const int nch = *a.cl.nchunks;
-    const StepConsts& c = a.c;
     for (int ci = blockIdx.x; ci < nch; ci += gridDim.x) {
         const int2 ch = a.cl.chunks[ci];
+        const StepConsts c = consts_of(a.L, find_instance_particle(a.L, ch.x));
         const int p = ch.x + (int)threadIdx.x;
         const bool active = threadIdx.x < (unsigned)ch.y;
         bool stenciled = active;
@@ -608,7 +638,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_g2p_tiled(const TiledArgs a
             const int e12 = tb.e[1] * tb.e[2];
             for (int t = threadIdx.x; t < tb.count; t += TILE_THREADS) {
                 const int gi = tb.o[0] + t / e12, gj = tb.o[1] + (t / tb.e[2]) % tb.e[1], gk = tb.o[2] + t % tb.e[2];
-                tile[t] = __ldg(a.grid + node_addr(gi, gj, gk, c.NB));
+                tile[t] = __ldg(a.grid + gaddr(c, gi, gj, gk));
             }
         }
         __syncthreads();
@@ -617,7 +647,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_g2p_tiled(const TiledArgs a
                 TileFetch f{tile, tb.o[0], tb.o[1], tb.o[2], tb.e[1], tb.e[2]};
                 g2p_particle(a.P, a.Fe, a.M, a.out, c, p, f);
             } else {
-                GlobalFetch f{a.grid, c.G, c.NB};
+                GlobalFetch f{a.grid, &c};
                 g2p_particle(a.P, a.Fe, a.M, a.out, c, p, f);
             }
         }

@@ -1,10 +1,11 @@
-// substep.cu — single-instance kernels and the C ABI of libempm_b200.so.
+// substep.cu — launch orchestration and the C ABI of libempm_b200.so.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdarg.h>
 #include "../../include/empm_b200.h"
+#include <cub/device/device_scan.cuh>
 #include "kernels.cuh"
 #include "ctx.hpp"
 
@@ -99,7 +100,7 @@ int empm_check_cuda(EmpmCtx* ctx, cudaError_t e, const char* what) {
         if (_rc != EMPM_OK) return _rc;                           \
     } while (0)
 
-extern "C" int empm_version(void) { return 100; }
+extern "C" int empm_version(void) { return 110; }
 
 static int validate_params(EmpmCtx* ctx, const EmpmModelParams* p) {
     if (!p) return empm_set_error(ctx, EMPM_ERR_INVALID, "params is NULL");
@@ -114,46 +115,113 @@ static void free_sorted(SortedBuffers& sb) {
         if (sb.part[i]) cudaFree(sb.part[i]);
         if (sb.matf[i]) cudaFree(sb.matf[i]);
         if (sb.mati[i]) cudaFree(sb.mati[i]);
-        sb.part[i] = nullptr; sb.matf[i] = nullptr; sb.mati[i] = nullptr;
     }
-    void* ptrs[] = {sb.fe, sb.keys, sb.ranks, sb.counts, sb.offsets, sb.cell_counts, sb.cell_offsets,
-                    sb.chunks, sb.nchunks};
+    void* ptrs[] = {sb.fe, sb.keys, sb.ranks, sb.block_counts, sb.block_offsets, sb.chunk_counts, sb.chunk_offsets,
+                    sb.cell_counts, sb.cell_offsets, sb.chunks, sb.nchunks, sb.scan_tmp};
     for (void* q : ptrs) if (q) cudaFree(q);
     sb = SortedBuffers();
 }
 
-extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, int max_steps, EmpmCtx** out) {
-    EmpmCtx* ctx = nullptr;
+static InstanceConsts instance_consts(const EmpmModelParams& P, int n, int poff, int boff) {
+    InstanceConsts I;
+    I.n = n;
+    I.poff = poff;
+    I.G = P.n_grid;
+    I.NB = grid_nb(P.n_grid);
+    I.boff = boff;
+    I.dx = P.grid_lim / (float)P.n_grid;
+    I.inv_dx = (float)P.n_grid / P.grid_lim;
+    I.grid_lim = P.grid_lim;
+    I.rpic = P.rpic_damping;
+    I.damping = P.grid_v_damping_scale;
+    I.g[0] = P.gravity[0];
+    I.g[1] = P.gravity[1];
+    I.g[2] = P.gravity[2];
+    I.ms.material = P.material;
+    I.ms.softening = P.softening;
+    I.ms.hardening = P.hardening;
+    I.ms.xi = P.xi;
+    I.ms.plastic_viscosity = P.plastic_viscosity;
+    I.ms.alpha = P.alpha;
+    return I;
+}
+
+static int upload_instances(EmpmCtx* ctx) {
+    std::vector<InstanceConsts> h(ctx->n_inst);
+    for (int i = 0; i < ctx->n_inst; ++i) h[i] = instance_consts(ctx->params[i], ctx->counts[i], ctx->poff[i], ctx->boff[i]);
+    CK(cudaMemcpy(ctx->d_inst, h.data(), sizeof(InstanceConsts) * h.size(), cudaMemcpyHostToDevice), "upload instances");
+    ctx->params_version++;
+    ctx->graph_valid = false;
+    return EMPM_OK;
+}
+
+static int ensure_step_capacity(EmpmCtx* ctx, int n_tables) {
+    if (n_tables <= ctx->max_tables) return EMPM_OK;
+    if (ctx->d_steps) {
+        CK(cudaDeviceSynchronize(), "sync before step-table growth");
+        cudaFree(ctx->d_steps);
+        ctx->d_steps = nullptr;
+    }
+    CK(cudaMalloc(&ctx->d_steps, sizeof(EmpmStep) * (size_t)n_tables * ctx->n_inst), "step table");
+    ctx->max_tables = n_tables;
+    ctx->graph_valid = false;
+    return EMPM_OK;
+}
+
+extern "C" int empm_batch_create(const EmpmModelParams* params, const int* n_particles, int n_instances, int max_steps,
+                                 EmpmCtx** out) {
     if (!out) return empm_set_error(nullptr, EMPM_ERR_INVALID, "out is NULL");
     *out = nullptr;
-    int rc = validate_params(nullptr, params);
-    if (rc) return rc;
-    if (n_particles < 0) return empm_set_error(nullptr, EMPM_ERR_INVALID, "n_particles < 0");
-    if (max_steps < 1 || max_steps > 100000) return empm_set_error(nullptr, EMPM_ERR_INVALID, "max_steps %d out of [1, 100000]", max_steps);
-    ctx = new EmpmCtx();
-    ctx->params = *params;
-    ctx->n_particles = n_particles;
-    ctx->max_steps = max_steps;
-    ctx->NB = grid_nb(params->n_grid);
-    const size_t nblocks = (size_t)ctx->NB * ctx->NB * ctx->NB;
-    const size_t grid_bytes = nblocks * 64 * sizeof(float4);
+    if (!params || !n_particles || n_instances < 1 || n_instances > 4096)
+        return empm_set_error(nullptr, EMPM_ERR_INVALID, "bad batch arguments (n_instances %d)", n_instances);
+    if (max_steps < 1 || max_steps > 100000)
+        return empm_set_error(nullptr, EMPM_ERR_INVALID, "max_steps %d out of [1, 100000]", max_steps);
+    long long total = 0, blocks = 0;
+    for (int i = 0; i < n_instances; ++i) {
+        int rc = validate_params(nullptr, params + i);
+        if (rc) return rc;
+        if (n_particles[i] < 0) return empm_set_error(nullptr, EMPM_ERR_INVALID, "instance %d: n_particles < 0", i);
+        total += n_particles[i];
+        const long long nb = grid_nb(params[i].n_grid);
+        blocks += nb * nb * nb;
+    }
+    if (total > 0x3fffffffLL) return empm_set_error(nullptr, EMPM_ERR_INVALID, "too many particles (%lld)", total);
+    if (blocks > (1LL << 25)) return empm_set_error(nullptr, EMPM_ERR_INVALID, "grids too large (%lld blocks)", blocks);
+    EmpmCtx* ctx = new EmpmCtx();
+    ctx->n_inst = n_instances;
+    ctx->params.assign(params, params + n_instances);
+    ctx->counts.assign(n_particles, n_particles + n_instances);
+    int po = 0, bo = 0;
+    for (int i = 0; i < n_instances; ++i) {
+        ctx->poff.push_back(po);
+        ctx->boff.push_back(bo);
+        po += n_particles[i];
+        const int nb = grid_nb(params[i].n_grid);
+        bo += nb * nb * nb;
+    }
+    ctx->n_particles = (int)total;
+    ctx->nblocks = blocks;
+    const size_t grid_bytes = (size_t)blocks * 64 * sizeof(float4);
     cudaError_t e = cudaGetDevice(&ctx->device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_inst, sizeof(InstanceConsts) * n_instances);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_mom, grid_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_vel, grid_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->flags, nblocks);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_steps, sizeof(EmpmStep) * (size_t)max_steps);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->flags, (size_t)blocks);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_mom, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_vel, 0, grid_bytes);
-    if (e == cudaSuccess) e = cudaMemset(ctx->flags, 0, nblocks);
+    if (e == cudaSuccess) e = cudaMemset(ctx->flags, 0, (size_t)blocks);
     if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_a, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_b, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) {
-        rc = empm_check_cuda(nullptr, e, "empm_ctx_create");
+    int rc = EMPM_OK;
+    if (e != cudaSuccess) rc = empm_check_cuda(nullptr, e, "empm_batch_create");
+    if (rc == EMPM_OK) rc = upload_instances(ctx);
+    if (rc == EMPM_OK) rc = ensure_step_capacity(ctx, max_steps);
+    if (rc == EMPM_OK) rc = empm_check_cuda(nullptr, cudaDeviceSynchronize(), "empm_batch_create");
+    if (rc != EMPM_OK) {
         empm_ctx_destroy(ctx);
         return rc;
     }
@@ -161,16 +229,17 @@ extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, i
     return EMPM_OK;
 }
 
+extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, int max_steps, EmpmCtx** out) {
+    return empm_batch_create(params, &n_particles, 1, max_steps, out);
+}
+
 extern "C" int empm_ctx_destroy(EmpmCtx* ctx) {
     if (!ctx) return EMPM_OK;
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     for (cudaEvent_t ev : ctx->timing_events) cudaEventDestroy(ev);
     free_sorted(ctx->sb);
-    if (ctx->grid_mom) cudaFree(ctx->grid_mom);
-    if (ctx->grid_vel) cudaFree(ctx->grid_vel);
-    if (ctx->flags) cudaFree(ctx->flags);
-    if (ctx->d_steps) cudaFree(ctx->d_steps);
-    if (ctx->d_status) cudaFree(ctx->d_status);
+    void* ptrs[] = {ctx->d_inst, ctx->grid_mom, ctx->grid_vel, ctx->flags, ctx->d_steps, ctx->d_status};
+    for (void* q : ptrs) if (q) cudaFree(q);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
     if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
@@ -191,7 +260,7 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
             break;
         case EMPM_OPT_G2P_TILE: ctx->g2p_tile = value != 0; break;
         case EMPM_OPT_TILE_CAP:
-            if (value < 27 || value > 4096) return empm_set_error(ctx, EMPM_ERR_INVALID, "tile_cap %d out of [27, 4096]", value);
+            if (value < 27 || value > 3072) return empm_set_error(ctx, EMPM_ERR_INVALID, "tile_cap %d out of [27, 3072]", value);
             ctx->tile_cap = value;
             break;
         default: return empm_set_error(ctx, EMPM_ERR_INVALID, "unknown option %d", option);
@@ -200,15 +269,22 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
     return EMPM_OK;
 }
 
-extern "C" int empm_ctx_set_params(EmpmCtx* ctx, const EmpmModelParams* params) {
+extern "C" int empm_batch_set_params(EmpmCtx* ctx, int instance, const EmpmModelParams* params) {
     if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    if (instance < 0 || instance >= ctx->n_inst)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "instance %d out of [0, %d)", instance, ctx->n_inst);
     int rc = validate_params(ctx, params);
     if (rc) return rc;
-    if (params->n_grid != ctx->params.n_grid)
-        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_grid cannot change (%d -> %d)", ctx->params.n_grid, params->n_grid);
-    if (memcmp(&ctx->params, params, sizeof(EmpmModelParams)) != 0) ctx->graph_valid = false;
-    ctx->params = *params;
-    return EMPM_OK;
+    if (params->n_grid != ctx->params[instance].n_grid)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_grid cannot change (%d -> %d)", ctx->params[instance].n_grid,
+                              params->n_grid);
+    if (memcmp(&ctx->params[instance], params, sizeof(EmpmModelParams)) == 0) return EMPM_OK;
+    ctx->params[instance] = *params;
+    return upload_instances(ctx);
+}
+
+extern "C" int empm_ctx_set_params(EmpmCtx* ctx, const EmpmModelParams* params) {
+    return empm_batch_set_params(ctx, 0, params);
 }
 
 extern "C" int empm_prepare(EmpmCtx* ctx, const float* E, const float* nu, float* mu, float* lam,
@@ -269,25 +345,16 @@ static void timing_mark(EmpmCtx* ctx, int kernel, int which, cudaStream_t stream
     if (which == 1) ctx->timing_count[kernel] = idx + 1;
 }
 
-static StepConsts step_consts(EmpmCtx* ctx, const EmpmStep* d_step) {
-    const EmpmModelParams& P = ctx->params;
-    StepConsts c;
-    c.n = ctx->n_particles;
-    c.G = P.n_grid;
-    c.NB = ctx->NB;
-    c.dx = P.grid_lim / (float)P.n_grid;
-    c.inv_dx = (float)P.n_grid / P.grid_lim;
-    c.grid_lim = P.grid_lim;
-    c.rpic = P.rpic_damping;
-    c.ms.material = P.material;
-    c.ms.softening = P.softening;
-    c.ms.hardening = P.hardening;
-    c.ms.xi = P.xi;
-    c.ms.plastic_viscosity = P.plastic_viscosity;
-    c.ms.alpha = P.alpha;
-    c.step = d_step;
-    c.status = ctx->d_status;
-    return c;
+static Launch make_launch(EmpmCtx* ctx, int table) {
+    Launch L;
+    L.inst = ctx->d_inst;
+    L.n_inst = ctx->n_inst;
+    L.n_total = ctx->n_particles;
+    L.nblocks = (int)ctx->nblocks;
+    L.steps = ctx->d_steps;
+    L.table = table;
+    L.status = ctx->d_status;
+    return L;
 }
 
 static ParticleArrays particle_arrays(const EmpmParticles* p, int n) {
@@ -313,23 +380,16 @@ static ParticleArrays particle_arrays(float* base, int n) {
     return a;
 }
 
-static int launch_grid_update(EmpmCtx* ctx, const EmpmStep* d_step, cudaStream_t stream) {
-    const EmpmModelParams& P = ctx->params;
+static int launch_grid_update(EmpmCtx* ctx, int table, cudaStream_t stream) {
     GridUpdateArgs g;
     g.mom = ctx->grid_mom;
     g.vel = ctx->grid_vel;
     g.flags = ctx->flags;
-    g.G = P.n_grid;
-    g.NB = ctx->NB;
-    g.dx = P.grid_lim / (float)P.n_grid;
-    g.g = v3(P.gravity[0], P.gravity[1], P.gravity[2]);
-    g.damping = P.grid_v_damping_scale;
-    g.step = d_step;
-    const long long nblocks = (long long)ctx->NB * ctx->NB * ctx->NB;
-    int nb = blocks_for(nblocks, 4);
+    g.L = make_launch(ctx, table);
+    long long nb = (ctx->nblocks + 3) / 4;
     if (nb > ctx->sm_count * 8) nb = ctx->sm_count * 8;
     timing_mark(ctx, 1, 0, stream);
-    k_grid_update_sparse<<<nb, 256, 0, stream>>>(g);
+    k_grid_update_sparse<<<(int)nb, 256, 0, stream>>>(g);
     timing_mark(ctx, 1, 1, stream);
     CK(cudaGetLastError(), "k_grid_update_sparse");
     return EMPM_OK;
@@ -337,9 +397,9 @@ static int launch_grid_update(EmpmCtx* ctx, const EmpmStep* d_step, cudaStream_t
 
 // Direct path: particles in the caller's order, one particle per thread.
 static int launch_substep_direct(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out, const EmpmMaterial* mat,
-                                 const EmpmStep* d_step, cudaStream_t stream) {
+                                 int table, cudaStream_t stream) {
     const int n = ctx->n_particles;
-    const StepConsts c = step_consts(ctx, d_step);
+    const Launch L = make_launch(ctx, table);
     const ParticleArrays Pin = particle_arrays(in, n);
     const ParticleArrays Pout = particle_arrays(out, n);
     MaterialArrays M;
@@ -352,15 +412,15 @@ static int launch_substep_direct(EmpmCtx* ctx, const EmpmParticles* in, EmpmPart
     const F9Planes Fe = f9_planes(mat->F_elastic, n);
     if (n > 0) {
         timing_mark(ctx, 0, 0, stream);
-        k_p2g_direct<<<blocks_for(n, 128), 128, 0, stream>>>(Pin, M, Fe, c, ctx->grid_mom, ctx->flags);
+        k_p2g_direct<<<blocks_for(n, 128), 128, 0, stream>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags);
         timing_mark(ctx, 0, 1, stream);
         CK(cudaGetLastError(), "k_p2g_direct");
     }
-    int rc = launch_grid_update(ctx, d_step, stream);
+    int rc = launch_grid_update(ctx, table, stream);
     if (rc) return rc;
     if (n > 0) {
         timing_mark(ctx, 2, 0, stream);
-        k_g2p_direct<<<blocks_for(n, 128), 128, 0, stream>>>(Pin, Fe, M, Pout, c, ctx->grid_vel);
+        k_g2p_direct<<<blocks_for(n, 128), 128, 0, stream>>>(Pin, Fe, M, Pout, L, ctx->grid_vel);
         timing_mark(ctx, 2, 1, stream);
         CK(cudaGetLastError(), "k_g2p_direct");
     }
@@ -372,7 +432,7 @@ static int ensure_sorted_buffers(EmpmCtx* ctx) {
     const int n = ctx->n_particles;
     if (sb.allocated && sb.n == n) return EMPM_OK;
     free_sorted(sb);
-    const size_t nblocks = (size_t)ctx->NB * ctx->NB * ctx->NB;
+    const size_t nblocks = (size_t)ctx->nblocks;
     sb.max_chunks = (int)((size_t)n / TILE_THREADS + nblocks + 1);
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
@@ -383,15 +443,25 @@ static int ensure_sorted_buffers(EmpmCtx* ctx) {
     if (e == cudaSuccess) e = cudaMalloc(&sb.fe, sizeof(float) * 9 * (size_t)n + 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.keys, sizeof(int) * (size_t)n + 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.ranks, sizeof(int) * (size_t)n + 64);
-    if (e == cudaSuccess) e = cudaMalloc(&sb.counts, sizeof(int) * nblocks);
-    if (e == cudaSuccess) e = cudaMalloc(&sb.offsets, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.block_counts, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.block_offsets, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.chunk_counts, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&sb.chunk_offsets, sizeof(int) * nblocks);
     if (e == cudaSuccess) e = cudaMalloc(&sb.cell_counts, sizeof(int) * nblocks * 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.cell_offsets, sizeof(int) * nblocks * 64);
-    if (e == cudaSuccess) e = cudaMemset(sb.cell_counts, 0, sizeof(int) * nblocks * 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.chunks, sizeof(int2) * (size_t)sb.max_chunks);
     if (e == cudaSuccess) e = cudaMalloc(&sb.nchunks, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(sb.counts, 0, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMemset(sb.block_counts, 0, sizeof(int) * nblocks);
+    if (e == cudaSuccess) e = cudaMemset(sb.cell_counts, 0, sizeof(int) * nblocks * 64);
     if (e == cudaSuccess) e = cudaMemset(sb.nchunks, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        size_t bytes = 0;
+        e = cub::DeviceScan::ExclusiveSum(nullptr, bytes, sb.block_counts, sb.block_offsets, (int)nblocks);
+        if (e == cudaSuccess) {
+            sb.scan_tmp_bytes = bytes;
+            e = cudaMalloc(&sb.scan_tmp, bytes + 16);
+        }
+    }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         free_sorted(sb);
@@ -421,15 +491,14 @@ static MaterialArrays sorted_material(EmpmCtx* ctx, int mc) {
     return M;
 }
 
-// sort `src` (caller order when src_mat is given, else the current sorted
-// state) into the other sorted buffers
+// Sort `src` (the caller's arrays when user_src is given, else the current
+// sorted state) into the other sorted buffers: cell keys and ranks, block
+// scan (CUB), per-block cell scan and chunk list, scatter.
 static int launch_sort(EmpmCtx* ctx, SortedState& ss, const ParticleArrays* user_src, const EmpmMaterial* user_mat,
                        cudaStream_t stream) {
     SortedBuffers& sb = ctx->sb;
     const int n = ctx->n_particles;
-    const int G = ctx->params.n_grid;
-    const float inv_dx = (float)G / ctx->params.grid_lim;
-    const int nblocks = ctx->NB * ctx->NB * ctx->NB;
+    const int nblocks = (int)ctx->nblocks;
     PermuteArgs a;
     if (user_src) {
         a.src = *user_src;
@@ -454,13 +523,19 @@ static int launch_sort(EmpmCtx* ctx, SortedState& ss, const ParticleArrays* user
     a.ranks = sb.ranks;
     a.offsets = sb.cell_offsets;
     a.n = n;
-    k_sort_keys<<<blocks_for(n, 256), 256, 0, stream>>>(reinterpret_cast<const float4*>(a.src.x), n, inv_dx, G,
-                                                        ctx->NB, sb.keys, sb.ranks, sb.cell_counts, sb.counts);
+    const Launch L = make_launch(ctx, 0);
+    k_sort_keys<<<blocks_for(n, 256), 256, 0, stream>>>(reinterpret_cast<const float4*>(a.src.x), L, sb.keys, sb.ranks,
+                                                        sb.cell_counts, sb.block_counts);
     CK(cudaGetLastError(), "k_sort_keys");
-    k_sort_scan<<<1, 1024, 0, stream>>>(sb.counts, sb.offsets, nblocks, TILE_THREADS, sb.chunks, sb.nchunks);
-    CK(cudaGetLastError(), "k_sort_scan");
-    k_cell_scan<<<blocks_for((long long)nblocks * 32, 256), 256, 0, stream>>>(sb.cell_counts, sb.offsets,
-                                                                              sb.cell_offsets, nblocks);
+    k_chunk_counts<<<blocks_for(nblocks, 256), 256, 0, stream>>>(sb.block_counts, sb.chunk_counts, nblocks, TILE_THREADS);
+    CK(cudaGetLastError(), "k_chunk_counts");
+    size_t bytes = sb.scan_tmp_bytes;
+    CK(cub::DeviceScan::ExclusiveSum(sb.scan_tmp, bytes, sb.block_counts, sb.block_offsets, nblocks, stream), "block scan");
+    bytes = sb.scan_tmp_bytes;
+    CK(cub::DeviceScan::ExclusiveSum(sb.scan_tmp, bytes, sb.chunk_counts, sb.chunk_offsets, nblocks, stream), "chunk scan");
+    k_cell_scan<<<blocks_for((long long)nblocks * 32, 256), 256, 0, stream>>>(
+        sb.cell_counts, sb.block_counts, sb.block_offsets, sb.chunk_offsets, sb.chunk_counts, sb.cell_offsets,
+        sb.chunks, sb.nchunks, nblocks, TILE_THREADS);
     CK(cudaGetLastError(), "k_cell_scan");
     k_sort_scatter<<<blocks_for(n, 256), 256, 0, stream>>>(a);
     CK(cudaGetLastError(), "k_sort_scatter");
@@ -469,14 +544,14 @@ static int launch_sort(EmpmCtx* ctx, SortedState& ss, const ParticleArrays* user
     return EMPM_OK;
 }
 
-static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, const EmpmStep* d_step, cudaStream_t stream) {
+static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaStream_t stream) {
     SortedBuffers& sb = ctx->sb;
     const int n = ctx->n_particles;
     TiledArgs t;
     t.P = particle_arrays(sb.part[ss.pc], n);
     t.M = sorted_material(ctx, ss.mc);
     t.Fe = f9_planes(sb.fe, n);
-    t.c = step_consts(ctx, d_step);
+    t.L = make_launch(ctx, table);
     t.cl.chunks = sb.chunks;
     t.cl.nchunks = sb.nchunks;
     t.grid = ctx->grid_mom;
@@ -487,13 +562,13 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, const EmpmStep* 
     const size_t smem = sizeof(float4) * (size_t)ctx->tile_cap;
     timing_mark(ctx, 0, 0, stream);
     if (ctx->p2g_mode == 2) {
-        k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, stream>>>(t.P, t.M, t.Fe, t.c, ctx->grid_mom, ctx->flags);
+        k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, stream>>>(t.P, t.M, t.Fe, t.L, ctx->grid_mom, ctx->flags);
     } else {
         k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
     }
     timing_mark(ctx, 0, 1, stream);
     CK(cudaGetLastError(), "k_p2g_sorted");
-    int rc = launch_grid_update(ctx, d_step, stream);
+    int rc = launch_grid_update(ctx, table, stream);
     if (rc) return rc;
     t.grid = ctx->grid_vel;
     t.tile_cap = ctx->g2p_tile ? ctx->tile_cap : 0;
@@ -501,7 +576,7 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, const EmpmStep* 
     if (ctx->g2p_tile) {
         k_g2p_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
     } else {
-        k_g2p_direct<<<blocks_for(n, 128), 128, 0, stream>>>(t.P, t.Fe, t.M, t.out, t.c, ctx->grid_vel);
+        k_g2p_direct<<<blocks_for(n, 128), 128, 0, stream>>>(t.P, t.Fe, t.M, t.out, t.L, ctx->grid_vel);
     }
     timing_mark(ctx, 2, 1, stream);
     CK(cudaGetLastError(), "k_g2p_sorted");
@@ -510,19 +585,18 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, const EmpmStep* 
 }
 
 static bool use_sorted(EmpmCtx* ctx) {
-    const long long nblocks = (long long)ctx->NB * ctx->NB * ctx->NB;
-    return ctx->sort_every > 0 && ctx->n_particles > 0 && nblocks <= (1 << 20);
+    return ctx->sort_every > 0 && ctx->n_particles > 0;
 }
 
 // The whole launch sequence of a rollout (also what a graph captures).
-static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat, int n_steps,
-                          cudaStream_t stream) {
+static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat, int n_tables,
+                          int n_steps, cudaStream_t stream) {
     int rc = EMPM_OK;
     if (!use_sorted(ctx)) {
         for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
             const EmpmParticles* in = (i & 1) ? b : a;
             EmpmParticles* out = (i & 1) ? a : b;
-            rc = launch_substep_direct(ctx, in, out, mat, ctx->d_steps + i, stream);
+            rc = launch_substep_direct(ctx, in, out, mat, n_tables == 1 ? 0 : i, stream);
         }
         return rc;
     }
@@ -532,7 +606,7 @@ static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, cons
     rc = launch_sort(ctx, ss, &ua, mat, stream);
     for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
         if (i > 0 && i % ctx->sort_every == 0) rc = launch_sort(ctx, ss, nullptr, nullptr, stream);
-        if (rc == EMPM_OK) rc = launch_substep_sorted(ctx, ss, ctx->d_steps + i, stream);
+        if (rc == EMPM_OK) rc = launch_substep_sorted(ctx, ss, n_tables == 1 ? 0 : i, stream);
     }
     if (rc) return rc;
     UnsortArgs u;
@@ -551,17 +625,19 @@ static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, cons
     return EMPM_OK;
 }
 
-static int upload_steps(EmpmCtx* ctx, const EmpmStep* steps, int n_steps, cudaStream_t stream) {
+static int upload_steps(EmpmCtx* ctx, const EmpmStep* steps, int n_tables, cudaStream_t stream) {
     if (!steps) return empm_set_error(ctx, EMPM_ERR_INVALID, "steps is NULL");
-    if (n_steps < 1 || n_steps > ctx->max_steps)
-        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, %d]", n_steps, ctx->max_steps);
-    for (int s = 0; s < n_steps; ++s) {
+    if (n_tables < 1 || n_tables > 100000) return empm_set_error(ctx, EMPM_ERR_INVALID, "n_tables %d out of [1, 100000]", n_tables);
+    const size_t total = (size_t)n_tables * ctx->n_inst;
+    for (size_t s = 0; s < total; ++s) {
         if (steps[s].n_colliders < 0 || steps[s].n_colliders > EMPM_MAX_COLLIDERS ||
             steps[s].n_modifiers < 0 || steps[s].n_modifiers > EMPM_MAX_MODIFIERS)
-            return empm_set_error(ctx, EMPM_ERR_INVALID, "step %d: collider/modifier count out of range", s);
+            return empm_set_error(ctx, EMPM_ERR_INVALID, "step entry %zu: collider/modifier count out of range", s);
     }
+    int rc = ensure_step_capacity(ctx, n_tables);
+    if (rc) return rc;
     // pageable source: the runtime stages it before returning, so the caller may reuse it
-    CK(cudaMemcpyAsync(ctx->d_steps, steps, sizeof(EmpmStep) * (size_t)n_steps, cudaMemcpyHostToDevice, stream),
+    CK(cudaMemcpyAsync(ctx->d_steps, steps, sizeof(EmpmStep) * total, cudaMemcpyHostToDevice, stream),
        "upload step table");
     return EMPM_OK;
 }
@@ -577,25 +653,28 @@ extern "C" int empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles
     cudaStream_t s = (cudaStream_t)stream;
     rc = upload_steps(ctx, step, 1, s);
     if (rc) return rc;
-    return launch_substep_direct(ctx, in, out, mat, ctx->d_steps, s);
+    return launch_substep_direct(ctx, in, out, mat, 0, s);
 }
 
 extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
-                            const EmpmStep* steps, int n_steps, int use_graph, void* stream) {
+                            const EmpmStep* steps, int n_tables, int n_steps, int use_graph, void* stream) {
     if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
     int rc = check_particles(ctx, a, "a");
     if (!rc) rc = check_particles(ctx, b, "b");
     if (!rc) rc = check_material(ctx, mat);
     if (rc) return rc;
     if (a->x == b->x) return empm_set_error(ctx, EMPM_ERR_INVALID, "a and b must be distinct buffers");
+    if (n_steps < 1 || n_steps > 100000) return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
+    if (n_tables != 1 && n_tables != n_steps)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_tables must be 1 or n_steps (%d, %d)", n_tables, n_steps);
     cudaStream_t s = (cudaStream_t)stream;
-    rc = upload_steps(ctx, steps, n_steps, s);
+    rc = upload_steps(ctx, steps, n_tables, s);
     if (rc) return rc;
     if (use_sorted(ctx)) {
         rc = ensure_sorted_buffers(ctx);
         if (rc) return rc;
     }
-    if (!use_graph) return launch_rollout(ctx, a, b, mat, n_steps, s);
+    if (!use_graph) return launch_rollout(ctx, a, b, mat, n_tables, n_steps, s);
     // CUDA graph path: capture on the context's own stream (legacy stream 0
     // cannot be captured), joined to the caller's stream by events.
     GraphKey key;
@@ -604,10 +683,12 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
     key.b = *b;
     key.mat = *mat;
     key.n_steps = n_steps;
+    key.n_tables = n_tables;
     key.sort_every = ctx->sort_every;
     key.p2g_mode = ctx->p2g_mode;
     key.g2p_tile = ctx->g2p_tile;
     key.tile_cap = ctx->tile_cap;
+    key.params_version = ctx->params_version;
     if (!ctx->graph_valid || memcmp(&key, &ctx->graph_key, sizeof(key)) != 0) {
         if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
         ctx->graph_valid = false;
@@ -615,7 +696,7 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
         ctx->timing = false;
         cudaError_t cap = cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal);
         if (cap != cudaSuccess) { ctx->timing = timing_was; CK(cap, "begin capture"); }
-        rc = launch_rollout(ctx, a, b, mat, n_steps, ctx->own_stream);
+        rc = launch_rollout(ctx, a, b, mat, n_tables, n_steps, ctx->own_stream);
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
         ctx->timing = timing_was;
@@ -677,6 +758,16 @@ extern "C" int empm_ctx_grid(EmpmCtx* ctx, float** momentum, float** velocity) {
     if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
     if (momentum) *momentum = reinterpret_cast<float*>(ctx->grid_mom);
     if (velocity) *velocity = reinterpret_cast<float*>(ctx->grid_vel);
+    return EMPM_OK;
+}
+
+extern "C" int empm_batch_info(EmpmCtx* ctx, int* n_instances, int* particle_offsets, int* block_offsets) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    if (n_instances) *n_instances = ctx->n_inst;
+    for (int i = 0; i < ctx->n_inst; ++i) {
+        if (particle_offsets) particle_offsets[i] = ctx->poff[i];
+        if (block_offsets) block_offsets[i] = ctx->boff[i];
+    }
     return EMPM_OK;
 }
 

@@ -218,6 +218,58 @@ EMPM_HD float4 p2g_node(const P2GParticle& q, int i, int j, int k, float dx, flo
     return make_float4(add.x, add.y, add.z, wm);
 }
 
+// Per-particle terms of the 27 P2G contributions, arranged so that each node
+// costs ~20 flops:
+//   (weight*mass)*(v + C dpos) + dt*(-vol*stress*dweight)
+// with dpos = ((i,j,k) - fx)*dx becomes  wm*(a + i B0 + j B1 + k B2) + S (f0, f1, f2)
+// where a = v - dx*C*fx, B = dx*C, S = dt*inv_dx*(-vol*stress) and
+// (f0, f1, f2) = (dwx wy wz, wx dwy wz, wx wy dwz).
+struct P2GPre {
+    Stencil st;
+    float   m;
+    V3      a;
+    M3      B;
+    M3      S;
+};
+
+EMPM_HD P2GPre p2g_pre(const P2GParticle& q, float dx, float inv_dx, float dt) {
+    P2GPre p;
+    p.st = q.st;
+    p.m = q.wm_scale;
+    p.B = dx * q.Cd;
+    const V3 fx = v3(q.st.fx[0], q.st.fx[1], q.st.fx[2]);
+    p.a = q.v - p.B * fx;
+    p.S = (dt * inv_dx) * q.Sv;
+    return p;
+}
+
+// Calls emit(i, j, k, contribution) for the 27 stencil nodes in (i, j, k) order.
+template <typename Emit>
+__device__ __forceinline__ void p2g_emit(const P2GPre& p, Emit emit) {
+    const Stencil& st = p.st;
+    const V3 B0 = col(p.B, 0), B1 = col(p.B, 1), B2 = col(p.B, 2);
+    const V3 S0 = col(p.S, 0), S1 = col(p.S, 1), S2 = col(p.S, 2);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const V3 ai = p.a + (float)i * B0;
+        const float wx = st.w[0][i], dwx = st.dw[0][i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const V3 aij = ai + (float)j * B1;
+            const float wxy = wx * st.w[1][j], dxy = dwx * st.w[1][j], xdy = wx * st.dw[1][j];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const V3 aijk = aij + (float)k * B2;
+                const float wz = st.w[2][k];
+                const float wm = (wxy * wz) * p.m;
+                const float f0 = dxy * wz, f1 = xdy * wz, f2 = wxy * st.dw[2][k];
+                const V3 c = wm * aijk + f0 * S0 + f1 * S1 + f2 * S2;
+                emit(i, j, k, make_float4(c.x, c.y, c.z, wm));
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ M3 damp_affine(const M3& C, float rpic) {
     if (rpic < -0.001f) return m3_zero();
     return (1.f - rpic) * C + (rpic / 2.f) * (C - transpose(C));
@@ -234,28 +286,48 @@ struct G2POut {
     M3 gradv;
 };
 
+// G2P gather (mpm_utils.py:528-550), rearranged so that each node costs ~25
+// flops: with o = (i,j,k) and wg = weight * grid_v,
+//   v = sum wg,   C = 4 inv_dx (sum wg (x) o - v (x) fx),
+//   grad v = inv_dx sum grid_v (x) (dwx wy wz, wx dwy wz, wx wy dwz).
 template <typename Fetch>
 __device__ __forceinline__ G2POut g2p_gather(const Stencil& st, float inv_dx, Fetch fetch) {
-    G2POut o;
-    o.v = v3(0.f, 0.f, 0.f);
-    o.C = m3_zero();
-    o.gradv = m3_zero();
+    V3 vs = v3(0.f, 0.f, 0.f);
+    V3 m0 = vs, m1 = vs, m2 = vs;      // sum wg * i, sum wg * j, sum wg * k
+    V3 g0 = vs, g1 = vs, g2 = vs;      // columns of sum grid_v (x) dweight / inv_dx
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 3; ++i) {
+        const float wx = st.w[0][i], dwx = st.dw[0][i];
 #pragma unroll
-        for (int j = 0; j < 3; ++j)
+        for (int j = 0; j < 3; ++j) {
+            const float wxy = wx * st.w[1][j], dxy = dwx * st.w[1][j], xdy = wx * st.dw[1][j];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const V3 dpos = v3((float)i - st.fx[0], (float)j - st.fx[1], (float)k - st.fx[2]);
-                const float weight = st.w[0][i] * st.w[1][j] * st.w[2][k];
-                const V3 gv = fetch(i, j, k);
-                o.v = o.v + gv * weight;
-                o.C = o.C + (weight * inv_dx * 4.f) * outer(gv, dpos);
-                const V3 dweight = v3(st.dw[0][i] * st.w[1][j] * st.w[2][k],
-                                      st.w[0][i] * st.dw[1][j] * st.w[2][k],
-                                      st.w[0][i] * st.w[1][j] * st.dw[2][k]) * inv_dx;
-                o.gradv = o.gradv + outer(gv, dweight);
+                const V3 g = fetch(i, j, k);
+                const float wz = st.w[2][k];
+                const V3 wg = (wxy * wz) * g;
+                vs = vs + wg;
+                if (i) m0 = m0 + (float)i * wg;
+                if (j) m1 = m1 + (float)j * wg;
+                if (k) m2 = m2 + (float)k * wg;
+                g0 = g0 + (dxy * wz) * g;
+                g1 = g1 + (xdy * wz) * g;
+                g2 = g2 + (wxy * st.dw[2][k]) * g;
             }
+        }
+    }
+    G2POut o;
+    o.v = vs;
+    const float c4 = 4.f * inv_dx;
+    const V3 mc[3] = {m0 - st.fx[0] * vs, m1 - st.fx[1] * vs, m2 - st.fx[2] * vs};
+    const V3 gc[3] = {g0, g1, g2};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            o.C.m[3 * r + c] = c4 * comp(mc[c], r);
+            o.gradv.m[3 * r + c] = inv_dx * comp(gc[c], r);
+        }
     return o;
 }
 

@@ -22,20 +22,29 @@ namespace empm {
 
 // Rotate the column pair (p, q) of the 3x3 column arrays b and v so that
 // b_p and b_q become orthogonal. Returns false when they already are.
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ float fast_rcp(float x) { return __fdividef(1.f, x); }
+#else
+inline float fast_rcp(float x) { return 1.f / x; }
+inline float rsqrtf(float x) { return 1.f / sqrtf(x); }
+#endif
+
 EMPM_HD bool jacobi_pair(float b[3][3], float v[3][3], int p, int q) {
     const float alpha = b[p][0] * b[p][0] + b[p][1] * b[p][1] + b[p][2] * b[p][2];
     const float beta  = b[q][0] * b[q][0] + b[q][1] * b[q][1] + b[q][2] * b[q][2];
     const float gamma = b[p][0] * b[q][0] + b[p][1] * b[q][1] + b[p][2] * b[q][2];
-    // relative orthogonality test; also true when a column is zero
-    if (fabsf(gamma) <= 4e-7f * sqrtf(alpha * beta)) return false;
-    const float zeta = (beta - alpha) / (2.f * gamma);
+    // relative orthogonality |gamma| <= tol * sqrt(alpha * beta), squared; also true for a zero column
+    if (gamma * gamma <= (1.6e-13f * alpha) * beta) return false;
+    const float zeta = (beta - alpha) * fast_rcp(2.f * gamma);
     float t;
-    if (fabsf(zeta) > 1e15f) {
-        t = 0.5f / zeta;
+    const float az = fabsf(zeta);
+    if (az > 1e15f) {
+        t = fast_rcp(2.f * zeta);
     } else {
-        t = (zeta >= 0.f ? 1.f : -1.f) / (fabsf(zeta) + sqrtf(1.f + zeta * zeta));
+        const float h = 1.f + zeta * zeta;
+        t = copysignf(fast_rcp(az + h * rsqrtf(h)), zeta);   // sign(zeta) / (|zeta| + sqrt(1 + zeta^2))
     }
-    const float c = 1.f / sqrtf(1.f + t * t);
+    const float c = rsqrtf(1.f + t * t);
     const float s = c * t;
     for (int r = 0; r < 3; ++r) {
         const float bp = b[p][r], bq = b[q][r];
@@ -57,9 +66,10 @@ EMPM_HD void swap_cols(float a[3][3], int i, int j) {
 // columns of u (u accumulates G^T, so that m_original = u * m).
 EMPM_HD void givens_rows(float m[3][3], float u[3][3], int p, int q, int c) {
     const float a = m[p][c], b = m[q][c];
-    const float r = sqrtf(a * a + b * b);
-    if (r == 0.f) return;
-    const float cs = a / r, sn = b / r;
+    const float r2 = a * a + b * b;
+    if (r2 == 0.f) return;
+    const float inv = rsqrtf(r2);
+    const float cs = a * inv, sn = b * inv;
     for (int k = 0; k < 3; ++k) {
         const float mp = m[p][k], mq = m[q][k];
         m[p][k] = cs * mp + sn * mq;

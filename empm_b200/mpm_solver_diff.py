@@ -86,7 +86,7 @@ class MPMWARPDiff(object):
         # launch options of the library (see EMPM_OPT_* in include/empm_b200.h)
         self.sort_every = 16
         self.p2g_mode = 2          # 0 direct, 1 shared-memory tile, 2 warp-aggregated
-        self.g2p_tile = True
+        self.g2p_tile = False
         self.tile_cap = 1024
 
     def initialize(self, n_particles, n_grid=100, grid_lim=1.0, device="cuda:0"):
@@ -302,7 +302,7 @@ class MPMWARPDiff(object):
         mat = self._material(mpm_model, state_a)
         a, b = state_a._particles(), state_b._particles()
         with torch.cuda.device(state_a.device):
-            N.check(ctx.L.empm_rollout(ctx.ptr, a, b, mat, table, n_steps, int(self.use_graph),
+            N.check(ctx.L.empm_rollout(ctx.ptr, a, b, mat, table, n_steps, n_steps, int(self.use_graph),
                                        _stream_ptr(state_a.device)), ctx.ptr)
         self.time = t_end
         return state_a if n_steps % 2 == 0 else state_b

@@ -151,3 +151,30 @@ def cuboid_callback(w: Workload, solver):
         solver.collider_params[k].velocity = w.velocity_schedule(step)
 
     return cb
+
+
+def c4(seed: int = 4, n_inst: int = 32, T: int = 300, n_lo: int = 20_000, n_hi: int = 300_000):
+    """Batched CMA-ES population: n_inst plasticine instances, particle counts
+    log-uniform in [n_lo, n_hi], grids from {48, 64, 96, 128}^3, each body a
+    random sub-box; per-instance log E ~ N(log 2e4, 0.3^2), log yield ~
+    N(log 2e3, 0.3^2), nu ~ N(0.3, 0.05) clipped to [0.2, 0.45];
+    dt = 2e-4 x T substeps; sticky floor at y = 3 dx and slip walls."""
+    from .batch import InstanceSpec
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_inst):
+        n = int(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))
+        G = int(rng.choice([48, 64, 96, 128]))
+        side = float(np.clip((n / (8.0 * G ** 3)) ** (1.0 / 3.0), 0.15, 0.6))
+        lo = rng.uniform(0.1, 0.9 - side, 3)
+        x = (lo + side * rng.uniform(0.0, 1.0, (n, 3))).astype(np.float32)
+        E = np.float32(np.exp(rng.normal(np.log(2e4), 0.3)))
+        ys = np.float32(np.exp(rng.normal(np.log(2e3), 0.3)))
+        nu = np.float32(np.clip(rng.normal(0.3, 0.05), 0.2, 0.45))
+        specs.append(InstanceSpec(
+            x=x, v=np.zeros((n, 3), np.float32), vol=np.full(n, np.float32(side ** 3 / n), np.float32),
+            rho=np.full(n, np.float32(1e3), np.float32), E=np.full(n, E, np.float32), nu=np.full(n, nu, np.float32),
+            yield_stress=np.full(n, ys, np.float32), n_grid=G, material="plasticine", gravity=(0.0, -9.8, 0.0),
+            colliders=_floor_walls(G)))
+    return specs, 2e-4, T

@@ -175,12 +175,27 @@ typedef struct EmpmCtx EmpmCtx;
 
 int  empm_version(void);
 
-/* Create a context for one simulation instance of n_particles on a G^3 grid.
- * Allocates the two grid buffers (2 * 16 * G^3 bytes), a step table of
- * max_steps entries and the status word on the current device. */
+/* Create a context for one simulation instance of n_particles on a G^3 grid
+ * (a batch of one, see empm_batch_create). Allocates the two grid buffers
+ * (2 * 16 * 64 * ceil(G/4)^3 bytes), room for max_steps step tables and the
+ * status word on the current device. */
 int  empm_ctx_create(const EmpmModelParams* params, int n_particles, int max_steps, EmpmCtx** out);
 int  empm_ctx_destroy(EmpmCtx* ctx);
 int  empm_ctx_set_params(EmpmCtx* ctx, const EmpmModelParams* params);
+
+/* A batch of n_instances independent simulations advanced by the same
+ * launches (the population of a CMA-ES generation, or the requests of a
+ * serving slot set). Instance i has its own parameters, particle count and
+ * grid; its particles occupy [poff_i, poff_i + n_particles[i]) of every
+ * particle and material array passed to empm_substep / empm_rollout
+ * (poff_i = sum of the previous counts), and its grid follows the previous
+ * instances' grids in the grid buffers. No counterpart in the reference,
+ * which evaluates a population serially (trainer_warp_mpm.py:598-661). */
+int  empm_batch_create(const EmpmModelParams* params, const int* n_particles, int n_instances, int max_steps,
+                       EmpmCtx** out);
+int  empm_batch_set_params(EmpmCtx* ctx, int instance, const EmpmModelParams* params);
+/* n_instances and, when non-NULL, the first particle and first grid block of each instance. */
+int  empm_batch_info(EmpmCtx* ctx, int* n_instances, int* particle_offsets, int* block_offsets);
 
 /* mu = E / (2 (1 + nu)), lam = E nu / ((1 + nu)(1 - 2 nu)); mass = density * vol,
  * written into x[4p+3]. Any of E/nu (mu/lam) or density (x) may be NULL to skip. */
@@ -195,20 +210,24 @@ int  empm_pack_particles(const float* x3, const float* v3, const float* C9, cons
 int  empm_unpack_particles(const EmpmParticles* src, float* x3, float* v3, float* C9, float* F9,
                            int n, void* stream);
 
-/* One MLS-MPM substep: in -> out (distinct buffers). step is a host pointer;
- * the schedule is copied to the device on the given stream. */
+/* One MLS-MPM substep: in -> out (distinct buffers). step is a host array of
+ * one schedule per instance (n_instances entries), copied to the device on
+ * the given stream. */
 int  empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out,
                   const EmpmMaterial* mat, const EmpmStep* step, void* stream);
 
 /* n_steps substeps, ping-ponging between a and b (the result is in a when
- * n_steps is even, else in b). With sorting enabled the particles are copied
- * into cell-block order inside the library at the start, re-sorted every
- * EMPM_OPT_SORT_EVERY substeps and written back in the caller's order at the
- * end, together with mu, lam, yield_stress and F_elastic. steps is a host array of n_steps schedules
- * (n_steps <= max_steps of the context). When use_graph != 0 the launch
- * sequence is captured once into a CUDA graph per (a, b, n_steps) and replayed. */
+ * n_steps is even, else in b). steps is a host array of n_tables schedule
+ * tables of n_instances entries each: n_tables == 1 reuses one table for
+ * every substep (static boundary conditions), n_tables == n_steps gives each
+ * substep its own. With sorting enabled the particles are copied into cell
+ * order inside the library at the start, re-sorted every EMPM_OPT_SORT_EVERY
+ * substeps and written back in the caller's order at the end, together with
+ * mu, lam, yield_stress and F_elastic. When use_graph != 0 the launch
+ * sequence is captured once into a CUDA graph per (a, b, n_steps, options)
+ * and replayed. */
 int  empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
-                  const EmpmStep* steps, int n_steps, int use_graph, void* stream);
+                  const EmpmStep* steps, int n_tables, int n_steps, int use_graph, void* stream);
 
 /* Launch options of a context (empm_ctx_set_option). */
 #define EMPM_OPT_SORT_EVERY  1   /* rollouts re-sort particles by 4^3 cell block every N substeps; 0 = no sorting (default 16) */

@@ -47,6 +47,20 @@ def test_null_context_is_rejected():
     L = N.lib()
     st = N.EmpmStep()
     assert L.empm_substep(None, None, None, None, st, None) == -1
-    assert L.empm_rollout(None, None, None, None, None, 1, 0, None) == -1
+    assert L.empm_rollout(None, None, None, None, None, 1, 1, 0, None) == -1
     with pytest.raises(N.EmpmError):
         N.check(L.empm_ctx_destroy(None) - 1)
+
+
+def test_batch_create_rejects_bad_arguments_without_gpu():
+    L = N.lib()
+    out = ctypes.c_void_p()
+    p = (N.EmpmModelParams * 2)()
+    for q in p:
+        q.n_grid, q.grid_lim = 32, 1.0
+    counts = (ctypes.c_int * 2)(100, -5)
+    assert L.empm_batch_create(p, counts, 2, 4, ctypes.byref(out)) == -1        # negative count
+    counts[1] = 10
+    assert L.empm_batch_create(p, counts, 0, 4, ctypes.byref(out)) == -1        # no instances
+    p[1].n_grid = 3
+    assert L.empm_batch_create(p, counts, 2, 4, ctypes.byref(out)) == -1        # bad grid in instance 1
