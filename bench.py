@@ -360,14 +360,250 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# c4: batched CMA-ES population (32 instances in one launch sequence)
+# ---------------------------------------------------------------------------
+def c4_instance_workload(spec, dt, T, name="c4 instance 0"):
+    """The first population member as a single Workload (CPU baseline sample)."""
+    from empm_b200.workloads import Workload
+
+    return Workload(name=name, n=spec.n, G=spec.n_grid, dt=dt, T=T, material=spec.material, x=spec.x, v=spec.v,
+                    vol=spec.vol, rho=spec.rho, E=spec.E, nu=spec.nu, ys=spec.yield_stress, gravity=tuple(spec.gravity),
+                    colliders=spec.colliders, description=name)
+
+
+def run_reference_c4(args):
+    from oracle import oracle as O
+    from oracle import specs as OS
+    from empm_b200 import workloads as W
+
+    specs, dt, T = W.c4(T=args.substeps or 300)
+    w = c4_instance_workload(specs[0], dt, T)
+    sim = OS.sim_from_workload(w, precision="fp32_omp")
+    per_step = args.ref_substeps
+
+    def one_step():
+        for _ in range(per_step):
+            sim.substep(dt)
+
+    for _ in range(args.warmup):
+        one_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_step()
+    el = time.perf_counter() - t0
+    value = w.n * per_step * args.steps / el
+    cores = int(O.lib("fp32_omp").lib.or_num_threads())
+    sample = (f"population member 0 ({w.n} particles, {w.G}^3) x {per_step} substeps per step (FP32 OpenMP CPU "
+              "oracle; the reference's Warp CPU device cannot be installed offline)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": C4_DESCRIPTION, "sample_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+C4_DESCRIPTION = ("batched CMA-ES population: 32 plasticine instances, particles log-U[20k,300k] (3.17M total), "
+                  "grids {48,64,96,128}^3, per-instance lognormal E and yield, dt=2e-4 x 300 substeps, "
+                  "CUDA graph per 50-substep block")
+
+
+def run_ours_c4(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from empm_b200 import workloads as W
+    from empm_b200.batch import BatchedMPM
+
+    specs, dt, T = W.c4(T=args.substeps or 300)
+    total = sum(s.n for s in specs)
+    batch = BatchedMPM(specs, device=dev)
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap"):
+        val = getattr(args, opt)
+        if val is not None:
+            setattr(batch, opt, val)
+    init = [t.clone() for t in (batch._x4[0], batch._v4[0], batch._C[0], batch._F[0], batch.mu, batch.lam,
+                                batch.yield_stress)]
+
+    def reset():
+        batch.cur = 0
+        batch.time = 0.0
+        for dst, src in zip((batch._x4[0], batch._v4[0], batch._C[0], batch._F[0], batch.mu, batch.lam,
+                             batch.yield_stress), init):
+            dst.copy_(src)
+
+    def step():
+        reset()
+        batch.rollout(dt, T, block=50)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    status = batch.read_status()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * total * T * args.steps / (ms / 1e3)
+
+    # per-kernel durations: one rollout on the stream path with CUDA events
+    batch.use_graph = False
+    batch.kernel_timing(True, max_launches=T + 8)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    step()
+    p1.record()
+    torch.cuda.synchronize()
+    kt = batch.kernel_times()
+    stream_ms = p0.elapsed_time(p1)
+    batch.kernel_timing(False)
+    batch.use_graph = True
+    peak, peak_kind = load_peaks()
+    bp = bytes_per_particle("plasticine")
+    kms = {k: v[0] / max(v[1], 1) for k, v in kt.items()}
+    dom = "stress_p2g"
+    achieved = total * bp[dom] / (kms[dom] / 1e3) / 1e9
+    substep_ms = ms / args.steps / T
+
+    # plain: the same population one instance at a time on the single-instance path
+    plain_ms = None
+    if not args.no_plain:
+        alone = []
+        for s in specs:
+            b1 = BatchedMPM([s], device=dev)
+            b1.rollout(dt, T, block=T)         # warm-up and graph capture
+            alone.append(b1)
+        torch.cuda.synchronize()
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record()
+        for b1 in alone:
+            b1.cur = 0
+            b1.time = 0.0
+            b1.rollout(dt, T, block=T)
+        q1.record()
+        torch.cuda.synchronize()
+        plain_ms = q0.elapsed_time(q1)
+        del alone
+
+    # end to end through the batch API with host buffers (one CMA-ES generation per step)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    hx = pin(np.concatenate([s.x for s in specs]))
+    hv = pin(np.concatenate([s.v for s in specs]))
+    hE = pin(np.concatenate([s.E for s in specs]))
+    hnu = pin(np.concatenate([s.nu for s in specs]))
+    hys = pin(np.concatenate([s.yield_stress for s in specs]))
+    hout = torch.empty((total, 3), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        batch.cur = 0
+        batch.time = 0.0
+        batch._x4[0][:, :3].copy_(hx, non_blocking=True)
+        batch._v4[0][:, :3].copy_(hv, non_blocking=True)
+        batch.E.copy_(hE, non_blocking=True)
+        batch.nu.copy_(hnu, non_blocking=True)
+        batch.yield_stress.copy_(hys, non_blocking=True)
+        batch._C[0].zero_()
+        batch._F[0].copy_(init[3])
+        batch.prepare()
+        batch.rollout(dt, T, block=50)
+        hout.copy_(batch.positions(), non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    r1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(r0.elapsed_time(r1))
+    e2e_value = world * total * T * args.steps / (e2e_ms / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(c4_instance_workload(specs[0], dt, T), budget_s=12.0, max_substeps=60)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    plain_value = total * T / (plain_ms / 1e3) if plain_ms else None
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": C4_DESCRIPTION, "instances": len(specs), "particles": total,
+                   "grids": sorted(set(s.n_grid for s in specs)), "substeps_per_step": T, "dt": dt,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (working set ~1 GB > 126 MB), no flush",
+                   "launch": "one CUDA graph per 50-substep block for the whole population",
+                   "options": {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode,
+                               "g2p_tile": batch.g2p_tile},
+                   "substep_us": substep_ms * 1e3,
+                   "substep_hbm_frac": (total * bp["substep"] / (substep_ms / 1e3) / 1e9) / peak,
+                   "plain_value": plain_value,
+                   "batched_vs_plain": (value / world) / plain_value if plain_value else None,
+                   "plain": "the same 32 instances one at a time on the single-instance path "
+                            "(one CUDA graph per 300-substep rollout)",
+                   "status_word": status},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_particle": bp[dom], "launch_ms": kms[dom],
+                     "kernel_ms": {k: round(v, 5) for k, v in kms.items()},
+                     "timing": "CUDA events around each kernel on its launch stream, stream path of one "
+                               f"population rollout in this run ({stream_ms:.2f} ms vs {ms / args.steps:.2f} ms graph)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": total * 36, "d2h_bytes_per_step": total * 12},
+        "gpu_launches": 3 * T * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2"])
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="c4: skip the one-instance-at-a-time comparison")
     ap.add_argument("--ref-substeps", type=int, default=2, help="substeps per step of the reference arm")
     ap.add_argument("--particles", type=int, default=None, help="override the workload's particle count")
     ap.add_argument("--grid", type=int, default=None, help="override the workload's grid resolution")
@@ -378,8 +614,8 @@ def main():
     ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
     args = ap.parse_args()
     if args.impl == "reference":
-        return run_reference(args)
-    return run_ours(args)
+        return run_reference_c4(args) if args.workload == "c4" else run_reference(args)
+    return run_ours_c4(args) if args.workload == "c4" else run_ours(args)
 
 
 if __name__ == "__main__":
