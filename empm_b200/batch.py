@@ -287,3 +287,35 @@ class BatchedMPM:
                 self.ptr = None
         except Exception:
             pass
+
+
+def single_instance(spec: InstanceSpec, device="cuda:0"):
+    """(solver, model, state) of the reference-facing single-instance API for
+    one instance spec: what a caller of MPMWARPDiff builds for one simulation."""
+    from .mpm_data_structure import MPMModelStruct, MPMStateStruct
+
+    dev = torch.device(device)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)  # noqa: E731
+    n = spec.n
+    st = MPMStateStruct()
+    st.init(n, device=dev)
+    st.from_torch(t(spec.x), t(spec.vol), None, t(spec.v) if spec.v is not None else None, n_grid=spec.n_grid,
+                  grid_lim=spec.grid_lim, device=dev)
+    st.reset_density(t(spec.rho), update_mass=True)
+    md = MPMModelStruct()
+    md.init(n, device=dev)
+    md.init_other_params(n_grid=spec.n_grid, grid_lim=spec.grid_lim)
+    md.gravitational_accelaration = tuple(spec.gravity)
+    sv = MPMWARPDiff()
+    sv.initialize(n, n_grid=spec.n_grid, grid_lim=spec.grid_lim, device=dev)
+    sv.set_parameters_dict(md, st, {"material": spec.material, "softening": spec.softening,
+                                    "plastic_viscosity": spec.plastic_viscosity,
+                                    "friction_angle": spec.friction_angle, "rpic_damping": spec.rpic_damping,
+                                    "grid_v_damping_scale": spec.grid_v_damping_scale})
+    md.E.copy_(t(spec.E))
+    md.nu.copy_(t(spec.nu))
+    md.finalize_mu_lam(n)
+    if spec.yield_stress is not None:
+        md.yield_stress.copy_(t(spec.yield_stress))
+    register_colliders(sv, spec.colliders)
+    return sv, md, st
