@@ -4,6 +4,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <stdarg.h>
+#include <mutex>
 #include "../../include/empm_b200.h"
 #include <cub/device/device_scan.cuh>
 #include "kernels.cuh"
@@ -801,6 +802,139 @@ extern "C" int empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launch
         }
         total_ms3[k] = total;
         launches3[k] = ctx->timing_count[k];
+    }
+    return EMPM_OK;
+}
+
+// ===========================================================================
+// Allocation-free substep
+// ===========================================================================
+// For callers that cannot allocate device memory when they step the
+// simulation. One example is a host application that reserves all of its
+// device memory at start-up and then runs the simulator inside a
+// fixed-budget control or rendering loop, where a cudaMalloc could stall the
+// loop or fail. Another is code that runs while a memory pool owned by
+// another framework must not grow. These callers still pass every input and
+// output buffer. The grid scratch that a context would allocate comes from
+// file-scope device arrays sized for grids up to
+// EMPM_NOALLOC_MAX_GRID^3 nodes. Every GPU that loads the library holds
+// them (8 MiB of grid plus a few KiB) until the process exits.
+
+namespace {
+constexpr int kNoallocNB = (EMPM_NOALLOC_MAX_GRID + 3) / 4;
+constexpr long long kNoallocBlocks = (long long)kNoallocNB * kNoallocNB * kNoallocNB;
+constexpr int kNoallocMaxDevices = 64;
+
+__device__ __align__(256) float4 g_noalloc_grid[2 * kNoallocBlocks * 64];   // accumulator | velocities
+__device__ __align__(256) unsigned char g_noalloc_flags[kNoallocBlocks];
+__device__ __align__(256) InstanceConsts g_noalloc_inst[1];
+__device__ __align__(256) EmpmStep g_noalloc_step[1];
+__device__ __align__(256) unsigned g_noalloc_status[1];
+
+// Device addresses of the arrays above. In host code their names are host-side
+// stand-ins, not device addresses, so the addresses are looked up once per
+// device with cudaGetSymbolAddress while that device is current.
+struct NoallocPtrs {
+    bool           ready = false;
+    float4*        grid = nullptr;
+    unsigned char* flags = nullptr;
+    InstanceConsts* inst = nullptr;
+    EmpmStep*      step = nullptr;
+    unsigned*      status = nullptr;
+};
+NoallocPtrs g_noalloc_ptrs[kNoallocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+int noalloc_setup(int device, NoallocPtrs** out) {
+    EmpmCtx* ctx = nullptr;
+    if (device < 0 || device >= kNoallocMaxDevices)
+        return empm_set_error(nullptr, EMPM_ERR_UNSUPPORTED, "device %d beyond the %d supported", device,
+                              kNoallocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoallocPtrs& p = g_noalloc_ptrs[device];
+    if (!p.ready) {
+        CK(cudaGetSymbolAddress((void**)&p.grid, g_noalloc_grid), "cudaGetSymbolAddress(grid)");
+        CK(cudaGetSymbolAddress((void**)&p.flags, g_noalloc_flags), "cudaGetSymbolAddress(flags)");
+        CK(cudaGetSymbolAddress((void**)&p.inst, g_noalloc_inst), "cudaGetSymbolAddress(instance)");
+        CK(cudaGetSymbolAddress((void**)&p.step, g_noalloc_step), "cudaGetSymbolAddress(step)");
+        CK(cudaGetSymbolAddress((void**)&p.status, g_noalloc_status), "cudaGetSymbolAddress(status)");
+        p.ready = true;
+    }
+    *out = &p;
+    return EMPM_OK;
+}
+}  // namespace
+
+extern "C" int empm_substep_noalloc(const EmpmModelParams* params, const EmpmParticles* in, EmpmParticles* out,
+                                    const EmpmMaterial* mat, const EmpmStep* step, int n_particles, void* stream) {
+    EmpmCtx* ctx = nullptr;
+    int rc = validate_params(nullptr, params);
+    if (rc) return rc;
+    if (params->n_grid > EMPM_NOALLOC_MAX_GRID)
+        return empm_set_error(nullptr, EMPM_ERR_INVALID,
+                              "n_grid %d exceeds the allocation-free maximum of %d (use a context for larger grids)",
+                              params->n_grid, EMPM_NOALLOC_MAX_GRID);
+    if (n_particles < 0) return empm_set_error(nullptr, EMPM_ERR_INVALID, "n_particles < 0");
+    if (!step || step->n_colliders < 0 || step->n_colliders > EMPM_MAX_COLLIDERS || step->n_modifiers < 0 ||
+        step->n_modifiers > EMPM_MAX_MODIFIERS)
+        return empm_set_error(nullptr, EMPM_ERR_INVALID, "bad step schedule");
+    rc = check_particles(nullptr, in, "in");
+    if (!rc) rc = check_particles(nullptr, out, "out");
+    if (!rc) rc = check_material(nullptr, mat);
+    if (rc) return rc;
+    if (in->x == out->x) return empm_set_error(nullptr, EMPM_ERR_INVALID, "in and out must be distinct buffers");
+    int device = 0;
+    CK(cudaGetDevice(&device), "cudaGetDevice");
+    NoallocPtrs* P = nullptr;
+    rc = noalloc_setup(device, &P);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int NB = grid_nb(params->n_grid);
+    const long long nblocks = (long long)NB * NB * NB;
+    const InstanceConsts ic = instance_consts(*params, n_particles, 0, 0);
+    // the arrays keep the previous call's contents: reset what must start at zero
+    CK(cudaMemsetAsync(P->grid, 0, sizeof(float4) * (size_t)nblocks * 64, s), "clear grid scratch");
+    CK(cudaMemsetAsync(P->flags, 0, (size_t)nblocks, s), "clear block flags");
+    CK(cudaMemsetAsync(P->status, 0, sizeof(unsigned), s), "clear status");
+    // pageable sources: the runtime stages them before returning
+    CK(cudaMemcpyAsync(P->inst, &ic, sizeof(InstanceConsts), cudaMemcpyHostToDevice, s), "upload instance");
+    CK(cudaMemcpyAsync(P->step, step, sizeof(EmpmStep), cudaMemcpyHostToDevice, s), "upload step");
+    Launch L;
+    L.inst = P->inst;
+    L.n_inst = 1;
+    L.n_total = n_particles;
+    L.nblocks = (int)nblocks;
+    L.steps = P->step;
+    L.table = 0;
+    L.status = P->status;
+    const ParticleArrays Pin = particle_arrays(in, n_particles);
+    const ParticleArrays Pout = particle_arrays(out, n_particles);
+    MaterialArrays M;
+    M.vol = mat->vol;
+    M.mu = mat->mu;
+    M.lam = mat->lam;
+    M.ys = mat->yield_stress;
+    M.sel = mat->selection;
+    M.pid = nullptr;
+    const F9Planes Fe = f9_planes(mat->F_elastic, n_particles);
+    float4* mom = P->grid;
+    float4* vel = P->grid + nblocks * 64;
+    if (n_particles > 0) {
+        k_p2g_direct<<<blocks_for(n_particles, 128), 128, 0, s>>>(Pin, M, Fe, L, mom, P->flags);
+        CK(cudaGetLastError(), "k_p2g_direct (allocation-free)");
+    }
+    GridUpdateArgs g;
+    g.mom = mom;
+    g.vel = vel;
+    g.flags = P->flags;
+    g.L = L;
+    long long nb = (nblocks + 3) / 4;
+    if (nb > 148 * 8) nb = 148 * 8;
+    k_grid_update_sparse<<<(int)nb, 256, 0, s>>>(g);
+    CK(cudaGetLastError(), "k_grid_update_sparse (allocation-free)");
+    if (n_particles > 0) {
+        k_g2p_direct<<<blocks_for(n_particles, 128), 128, 0, s>>>(Pin, Fe, M, Pout, L, vel);
+        CK(cudaGetLastError(), "k_g2p_direct (allocation-free)");
     }
     return EMPM_OK;
 }

@@ -245,6 +245,26 @@ int  empm_read_status(EmpmCtx* ctx, uint32_t* status, void* stream);
 /* Last error message of the context (or of the library when ctx is NULL). */
 int  empm_last_error(EmpmCtx* ctx, char* buf, int len);
 
+/* One substep that allocates nothing. No counterpart in the reference.
+ * For callers that cannot allocate device memory when they step the
+ * simulation: for example an application that reserves all of its device
+ * memory at start-up and steps the simulator inside a fixed-budget control or
+ * rendering loop, where a cudaMalloc could stall or fail, or code running
+ * while another framework's memory pool must not grow. The caller passes the
+ * inputs and outputs as for empm_substep (particles in the caller's order,
+ * one schedule for the single instance described by params). The grid scratch
+ * lives in file-scope device arrays sized for grids of at most
+ * EMPM_NOALLOC_MAX_GRID^3 nodes (8 MiB, held by every GPU that loads the
+ * library until the process exits); larger n_grid is rejected with
+ * EMPM_ERR_INVALID. The first call on a device looks the arrays' device
+ * addresses up (cudaGetSymbolAddress), so make it before any stream capture.
+ * Every call shares the arrays and clears them at its start: calls that
+ * overlap on the GPU (different streams, threads or processes sharing the
+ * library on one device) race and must be serialised by the caller. */
+#define EMPM_NOALLOC_MAX_GRID 64
+int  empm_substep_noalloc(const EmpmModelParams* params, const EmpmParticles* in, EmpmParticles* out,
+                          const EmpmMaterial* mat, const EmpmStep* step, int n_particles, void* stream);
+
 /* ---- diagnostics (used by the parity tests) ------------------------------ */
 
 /* Return map + Kirchhoff stress of the material switch for n particles, on
