@@ -68,6 +68,11 @@ class EmpmMaterial(ctypes.Structure):
     ]
 
 
+class EmpmMaterialGrad(ctypes.Structure):
+    _fields_ = [("mu", ctypes.c_void_p), ("lam", ctypes.c_void_p), ("yield_stress", ctypes.c_void_p),
+                ("mass", ctypes.c_void_p)]
+
+
 class EmpmError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"empm error {code}: {message}")
@@ -110,6 +115,11 @@ def lib():
         "empm_read_status": ([P, ctypes.POINTER(ctypes.c_uint32), P], I),
         "empm_last_error": ([P, ctypes.c_char_p, I], I),
         "empm_debug_stress": ([ctypes.POINTER(EmpmModelParams), P, P, P, P, ctypes.c_float, P, P, I, P], I),
+        "empm_adjoint_segment": ([P, ctypes.POINTER(EmpmParticles), P, P, P, ctypes.POINTER(EmpmMaterial), P, I,
+                                  ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterialGrad), P], I),
+        "empm_prepare_adjoint": ([P, P, P, P, P, P, P, P, P, I, P], I),
+        "empm_debug_stress_adjoint": ([ctypes.POINTER(EmpmModelParams), P, P, P, P, ctypes.c_float, P, P, P, P, P,
+                                       P, I, P], I),
         "empm_ctx_grid": ([P, ctypes.POINTER(P), ctypes.POINTER(P)], I),
         "empm_ctx_timing": ([P, I, I], I),
         "empm_ctx_set_option": ([P, I, I], I),

@@ -1,0 +1,318 @@
+// adjoint.cuh — reverse-mode kernels of one MLS-MPM substep (direct path:
+// particles in the caller's order, one particle or node per thread).
+//
+// The reference obtains gradients by replaying Warp's generated adjoints of
+// every launched kernel (tape.backward, interface.py:197,418,720,935). Here
+// the adjoint of one substep is three hand-written kernels that run after the
+// substep's forward grid has been recomputed (k_p2g_direct, then
+// k_grid_update_keep):
+//
+//   k_adj_g2p   per particle: adjoint of x', v', C', F' -> scatter of the node
+//               velocity adjoint, and the particle's x and F_elastic adjoints
+//               from the G2P gather;
+//   k_adj_grid  per touched node: the boundary conditions replayed forwards
+//               and transposed backwards, then normalisation -> adjoint of
+//               the accumulated momentum and mass;
+//   k_adj_p2g   per particle: gather of the momentum/mass adjoint -> adjoint
+//               of v, C, mass, the stress, and x; then the constitutive
+//               adjoint (spectral.cuh) -> F_trial, mu, lam and yield adjoints,
+//               and the velocity modifiers' adjoint.
+//
+// The state of substep k is (x, v, C, F_trial, mu, lam, yield); mass is
+// constant. Particles whose selection flag is set produce constant outputs,
+// so their adjoints are zero. The quadratic B-spline weights are C1, so the
+// x adjoint includes the weights' first and second derivatives.
+#pragma once
+#include "kernels.cuh"
+#include "spectral.cuh"
+
+namespace empm {
+
+// second derivative of the quadratic B-spline weight at stencil offset o
+EMPM_HD float bspline_d2(int o) { return o == 1 ? -2.f : 1.f; }
+
+// Hessian (grid units) of w = wx wy wz at node (i, j, k) of the stencil, times b
+EMPM_HD V3 weight_hessian_times(const Stencil& st, int i, int j, int k, V3 b) {
+    const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
+    const float dx = st.dw[0][i], dy = st.dw[1][j], dz = st.dw[2][k];
+    const float hxx = bspline_d2(i) * wy * wz, hyy = wx * bspline_d2(j) * wz, hzz = wx * wy * bspline_d2(k);
+    const float hxy = dx * dy * wz, hxz = dx * wy * dz, hyz = wx * dy * dz;
+    return v3(hxx * b.x + hxy * b.y + hxz * b.z, hxy * b.x + hyy * b.y + hyz * b.z, hxz * b.x + hyz * b.y + hzz * b.z);
+}
+
+__global__ void __launch_bounds__(256) k_grid_update_keep(const GridUpdateArgs a) { grid_update_blocks<true>(a); }
+
+// ---------------------------------------------------------------------------
+// G2P adjoint
+// ---------------------------------------------------------------------------
+struct AdjG2PArgs {
+    ParticleArrays P;      // state of substep k (x)
+    F9Planes       Fe;     // elastic F of substep k
+    MaterialArrays M;      // selection
+    ParticleArrays Gn;     // adjoint of the state after substep k
+    Launch         L;
+    const float4*  vel;    // node velocities of substep k
+    float4*        gacc;   // node velocity adjoint (accumulated here)
+    float4*        gx;     // out: x adjoint through G2P
+    F9Planes       gFe;    // out: F_elastic adjoint
+};
+
+__global__ void __launch_bounds__(128) k_adj_g2p(const AdjG2PArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.L.n_total) return;
+    if (a.M.sel && __ldg(a.M.sel + p) != 0) {
+        a.gx[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        f9_store(a.gFe, p, m3_zero());
+        return;
+    }
+    const StepConsts c = consts_of(a.L, find_instance_particle(a.L, p));
+    const float dt = c.step->dt;
+    const float4 xm = __ldg(a.P.x + p);
+    const V3 x = v3(xm.x, xm.y, xm.z);
+    const Stencil st = make_stencil(x, c.inv_dx);
+    const bool in_grid = stencil_in_grid(st, c.G);
+    const GlobalFetch fetch{a.vel, &c};
+    const G2POut o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+
+    // x' = clamp(x + dt v'): the clamp passes the adjoint only strictly inside the band
+    const float dx = 1.f / c.inv_dx;
+    const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
+    const V3 y = x + dt * o.v;
+    const float4 gx4 = __ldg(a.Gn.x + p), gv4 = __ldg(a.Gn.v + p);
+    const V3 gxu = v3(y.x > lo && y.x < hi ? gx4.x : 0.f, y.y > lo && y.y < hi ? gx4.y : 0.f,
+                      y.z > lo && y.z < hi ? gx4.z : 0.f);
+    const V3 gvt = v3(gv4.x, gv4.y, gv4.z) + dt * gxu;
+    const M3 gC = f9_load(a.Gn.C, p), gF = f9_load(a.Gn.F, p);
+    // F' = (I + dt grad v) F_e
+    const M3 Fe = f9_load(a.Fe, p);
+    const M3 gGv = dt * (gF * transpose(Fe));
+    const M3 gFe = transpose(m3_identity() + dt * o.gradv) * gF;
+
+    // per node: q = gvt + 4 inv_dx gC (o - fx); node velocity adjoint w q + gGv dweight
+    const float c4 = 4.f * c.inv_dx;
+    const float idx2 = c.inv_dx * c.inv_dx;
+    const V3 fx = v3(st.fx[0], st.fx[1], st.fx[2]);
+    const V3 q0 = gvt - c4 * (gC * fx);
+    const V3 Q0 = c4 * col(gC, 0), Q1 = c4 * col(gC, 1), Q2 = c4 * col(gC, 2);
+    V3 gxa = gxu - (c4 * c.inv_dx) * (transpose(gC) * o.v);
+    const M3 gGvT = transpose(gGv);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
+                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= c.G || iy >= c.G || iz >= c.G)) continue;
+                const long long addr = gaddr(c, ix, iy, iz);
+                const float4 g4 = __ldg(a.vel + addr);
+                const V3 vg = v3(g4.x, g4.y, g4.z);
+                const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
+                const float w = wx * wy * wz;
+                const V3 dw = c.inv_dx * v3(st.dw[0][i] * wy * wz, wx * st.dw[1][j] * wz, wx * wy * st.dw[2][k]);
+                const V3 q = q0 + (float)i * Q0 + (float)j * Q1 + (float)k * Q2;
+                const V3 gvg = w * q + gGv * dw;
+                red_add_v4(a.gacc + addr, make_float4(gvg.x, gvg.y, gvg.z, 0.f));
+                gxa = gxa + dot(vg, q) * dw + idx2 * weight_hessian_times(st, i, j, k, gGvT * vg);
+            }
+    a.gx[p] = make_float4(gxa.x, gxa.y, gxa.z, 0.f);
+    f9_store(a.gFe, p, gFe);
+}
+
+// ---------------------------------------------------------------------------
+// grid adjoint over the touched blocks
+// ---------------------------------------------------------------------------
+struct AdjGridArgs {
+    float4*        mom;     // accumulation of substep k; zeroed here
+    float4*        gacc;    // node velocity adjoint; zeroed here
+    float4*        gmom;    // out: adjoint of the accumulation (momentum xyz, mass w)
+    unsigned char* flags;   // touched blocks of substep k; cleared here
+    Launch         L;
+};
+
+__global__ void __launch_bounds__(256) k_adj_grid(const AdjGridArgs a) {
+    const int nblocks = a.L.nblocks;
+    const int group = threadIdx.x >> 6;
+    const int lane = threadIdx.x & 63;
+    for (int base = blockIdx.x * 4; base < nblocks; base += gridDim.x * 4) {
+        const int b = base + group;
+        const bool active = b < nblocks && a.flags[b] != 0;
+        __syncthreads();   // every group has read its flag before any is cleared
+        if (!active) continue;
+        const int inst = find_instance_block(a.L, b);
+        const InstanceConsts* I = a.L.inst + inst;
+        const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
+        const float damping = __ldg(&I->damping);
+        const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
+        const long long node = ((long long)b << 6) | lane;
+        const float4 m = a.mom[node];
+        const float4 g4 = a.gacc[node];
+        a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+        a.gacc[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+        // replay the forward update to learn which projections applied
+        V3 v = grid_velocity(m, st.dt, v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2])), damping);
+        unsigned long long codes = 0;
+        if (st.n_colliders > 0) {
+            int i, j, k;
+            node_coords(((long long)(b - boff) << 6) | lane, NB, i, j, k);
+            if (i < G && j < G && k < G) {
+                const long long dense = ((long long)i * G + j) * G + k;
+                apply_colliders_rec(st, i, j, k, G, __ldg(&I->dx), dense, v,
+                                    [&](int cidx, unsigned code) { codes |= (unsigned long long)code << (4 * cidx); });
+            }
+        }
+        V3 g = v3(g4.x, g4.y, g4.z);
+        for (int cidx = st.n_colliders - 1; codes != 0 && cidx >= 0; --cidx) {
+            const unsigned code = (unsigned)(codes >> (4 * cidx)) & 15u;
+            if (code & 1u) g.x = 0.f;
+            if (code & 2u) g.y = 0.f;
+            if (code & 4u) g.z = 0.f;
+            if (code & 8u) g = g * 0.3f;
+        }
+        if (damping < 1.f) g = g - (1.f - damping) * g;
+        float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (m.w > 1e-15f) {
+            const float inv = 1.f / m.w;
+            out = make_float4(g.x * inv, g.y * inv, g.z * inv, -(g.x * m.x + g.y * m.y + g.z * m.z) * inv * inv);
+        }
+        a.gmom[node] = out;
+        if (lane == 0) a.flags[b] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// P2G + constitutive adjoint
+// ---------------------------------------------------------------------------
+struct AdjP2GArgs {
+    ParticleArrays P;      // state of substep k (v after the velocity modifiers)
+    MaterialArrays M;      // mu, lam, yield at the start of substep k; vol; selection; caller index
+    Launch         L;      // step table with the modifiers
+    const float4*  gmom;   // adjoint of the accumulation
+    const float4*  gx;     // x adjoint through G2P
+    F9Planes       gFe;    // F_elastic adjoint
+    ParticleArrays G;      // out: adjoint of the state of substep k
+    float*         g_mu;   // in: adjoint after substep k; out: before it
+    float*         g_lam;
+    float*         g_ys;
+    float*         g_mass; // accumulated over substeps
+};
+
+__global__ void __launch_bounds__(128) k_adj_p2g(const AdjP2GArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.L.n_total) return;
+    if (a.M.sel && __ldg(a.M.sel + p) != 0) {
+        a.G.x[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        a.G.v[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        f9_store(a.G.C, p, m3_zero());
+        f9_store(a.G.F, p, m3_zero());
+        return;   // material scalars are untouched by the substep: their adjoints carry over
+    }
+    const StepConsts c = consts_of(a.L, find_instance_particle(a.L, p));
+    const EmpmStep& step = *c.step;
+    const float dt = step.dt;
+    const float4 xm = __ldg(a.P.x + p);
+    const V3 x = v3(xm.x, xm.y, xm.z);
+    const float mass = xm.w;
+    const float4 vv = __ldg(a.P.v + p);
+    const V3 v = v3(vv.x, vv.y, vv.z);
+    const float vol = __ldg(a.M.vol + p);
+
+    SpectralEval e;
+    spectral_eval(f9_load(a.P.F, p), __ldg(a.M.mu + p), __ldg(a.M.lam + p), __ldg(a.M.ys + p), dt, c.ms, e);
+    const M3 Sv = (-vol) * spectral_tau(e);
+    const M3 Cd = damp_affine(f9_load(a.P.C, p), c.rpic);
+
+    const Stencil st = make_stencil(x, c.inv_dx);
+    const bool in_grid = stencil_in_grid(st, c.G);
+    const float dx = c.dx;
+    const float idx2 = c.inv_dx * c.inv_dx;
+    const M3 SvT = transpose(Sv);
+    V3 Wg = v3(0.f, 0.f, 0.f);      // sum w gmv
+    M3 gCd = m3_zero();             // sum w gmv (x) dpos
+    M3 gSv = m3_zero();             // sum gmv (x) dweight
+    float gmass = 0.f;
+    V3 gxa = v3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
+                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= c.G || iy >= c.G || iz >= c.G)) continue;
+                const float4 g4 = __ldg(a.gmom + gaddr(c, ix, iy, iz));
+                const V3 gmv = v3(g4.x, g4.y, g4.z);
+                const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
+                const float w = wx * wy * wz;
+                const V3 dw = c.inv_dx * v3(st.dw[0][i] * wy * wz, wx * st.dw[1][j] * wz, wx * wy * st.dw[2][k]);
+                const V3 dpos = v3(((float)i - st.fx[0]) * dx, ((float)j - st.fx[1]) * dx, ((float)k - st.fx[2]) * dx);
+                const float s = g4.w + dot(gmv, v + Cd * dpos);
+                gmass += w * s;
+                Wg = Wg + w * gmv;
+                gCd = gCd + outer(w * gmv, dpos);
+                gSv = gSv + outer(gmv, dw);
+                gxa = gxa + (mass * s) * dw + (dt * idx2) * weight_hessian_times(st, i, j, k, SvT * gmv);
+            }
+    gxa = gxa - mass * (transpose(Cd) * Wg);
+    V3 gv = mass * Wg;
+    gCd = mass * gCd;
+    const M3 g_tau = (-vol * dt) * gSv;
+    M3 gC = m3_zero();
+    if (!(c.rpic < -0.001f)) gC = (1.f - c.rpic) * gCd + (c.rpic / 2.f) * (gCd - transpose(gCd));
+
+    const SpectralGrad sg = spectral_adjoint(e, f9_load(a.gFe, p), g_tau, a.g_mu[p], a.g_lam[p], a.g_ys[p]);
+
+    // velocity modifiers, in reverse order (mpm_solver_diff.py:977-991, 1022-1036,
+    // 1098-1142, 1198-1212, 1332-1348, 1391-1410). A modifier that overwrites v
+    // cuts the adjoint; the rotation modifier's dependence on x is not
+    // differentiated.
+    if (step.n_modifiers > 0) {
+        const int mi = a.M.pid ? __ldg(a.M.pid + p) : p;
+        for (int m = step.n_modifiers - 1; m >= 0; --m) {
+            const EmpmModifier& md = step.modifiers[m];
+            if (md.gate != EMPM_GATE_APPLY) continue;
+            const int mk = md.mask ? __ldg(md.mask + mi) : 0;
+            switch (md.kind) {
+                case EMPM_MOD_IMPULSE:
+                    if (mk == 1) gmass -= dot(gv, v3(md.vec[0], md.vec[1], md.vec[2])) * dt / (mass * mass);
+                    break;
+                case EMPM_MOD_SET_VELOCITY:
+                case EMPM_MOD_ROTATION:
+                    if (mk == 1) gv = v3(0.f, 0.f, 0.f);
+                    break;
+                case EMPM_MOD_MOVER:
+                    if (mk == 1) gxa = gxa + md.scale[0] * cross(gv, v3(md.normal[0], md.normal[1], md.normal[2]));
+                    break;
+                default: break;
+            }
+        }
+    }
+    const float4 gxg = __ldg(a.gx + p);
+    a.G.x[p] = make_float4(gxa.x + gxg.x, gxa.y + gxg.y, gxa.z + gxg.z, 0.f);
+    a.G.v[p] = make_float4(gv.x, gv.y, gv.z, 0.f);
+    f9_store(a.G.C, p, gC);
+    f9_store(a.G.F, p, sg.gFt);
+    a.g_mu[p] = sg.g_mu;
+    a.g_lam[p] = sg.g_lam;
+    a.g_ys[p] = sg.g_ys;
+    a.g_mass[p] += gmass;
+}
+
+// dL/dE, dL/dnu from dL/dmu, dL/dlam (compute_mu_lam_from_E_nu, mpm_utils.py:277-283),
+// and dL/ddensity from dL/dmass with mass = density * vol (mpm_data_structure.py:719-726)
+__global__ void k_prepare_adjoint(const float* E, const float* nu, const float* g_mu, const float* g_lam, float* g_E,
+                                  float* g_nu, const float* vol, const float* g_mass, float* g_density, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (g_E && g_nu) {
+        const float e = E[p], q = nu[p];
+        const float a = 1.f + q, b = 1.f - 2.f * q;
+        const float dmu_dE = 1.f / (2.f * a), dlam_dE = q / (a * b);
+        const float dmu_dnu = -e / (2.f * a * a), dlam_dnu = e * (1.f + 2.f * q * q) / (a * a * b * b);
+        g_E[p] = g_mu[p] * dmu_dE + g_lam[p] * dlam_dE;
+        g_nu[p] = g_mu[p] * dmu_dnu + g_lam[p] * dlam_dnu;
+    }
+    if (g_density) g_density[p] = g_mass[p] * vol[p];
+}
+
+}  // namespace empm

@@ -43,6 +43,20 @@ struct SortedBuffers {
     size_t scan_tmp_bytes = 0;
 };
 
+// Buffers of the reverse-mode path (empm_adjoint_segment), allocated on first use.
+struct AdjointBuffers {
+    int     capacity = 0;      // substeps per segment the buffers hold
+    float*  states = nullptr;  // capacity + 1 packed particle states (x4 | v4 | C f9 | F f9)
+    float*  mats = nullptr;    // capacity snapshots of mu | lam | yield
+    float*  work = nullptr;    // mu | lam | yield updated by the recomputed substeps
+    float*  fe = nullptr;      // elastic F of the substep being differentiated (f9)
+    float*  gfe = nullptr;     // its adjoint (f9)
+    float4* gx = nullptr;      // x adjoint through G2P
+    float4* gacc = nullptr;    // node velocity adjoint (blocked grid), zero between substeps
+    float4* gmom = nullptr;    // adjoint of the P2G accumulation (blocked grid)
+    std::vector<EmpmStep> tables;   // host staging of the step tables
+};
+
 struct EmpmCtx {
     // instances
     int          n_inst = 0;
@@ -75,6 +89,7 @@ struct EmpmCtx {
     int          g2p_tile = 0;
     int          tile_cap = 1024;          // nodes per shared-memory tile (16 B each)
     SortedBuffers sb;
+    AdjointBuffers adj;
     // per-kernel event timing (stream path only)
     bool         timing = false;
     int          timing_capacity = 0;

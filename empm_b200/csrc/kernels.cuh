@@ -190,7 +190,10 @@ struct GridUpdateArgs {
     Launch         L;
 };
 
-__global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs a) {
+// kKeep: leave the accumulation and the block flags in place (the adjoint
+// replays the boundary conditions from the accumulated momentum afterwards).
+template <bool kKeep>
+__device__ __forceinline__ void grid_update_blocks(const GridUpdateArgs& a) {
     const int nblocks = a.L.nblocks;
     const int group = threadIdx.x >> 6;   // 4 node blocks per iteration
     const int lane = threadIdx.x & 63;
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs
             const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
             const long long node = ((long long)b << 6) | lane;
             const float4 m = a.mom[node];
-            a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (!kKeep) a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
             V3 v = grid_velocity(m, st.dt, v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2])), __ldg(&I->damping));
             if (st.n_colliders > 0) {
                 int i, j, k;
@@ -216,10 +219,12 @@ __global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs
                 }
             }
             a.vel[node] = make_float4(v.x, v.y, v.z, m.w);
-            if (lane == 0) a.flags[b] = 0;
+            if (!kKeep && lane == 0) a.flags[b] = 0;
         }
     }
 }
+
+__global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs a) { grid_update_blocks<false>(a); }
 
 // -------------------------------------------------------------------------
 // G2P (shared by both paths through the fetch functor)

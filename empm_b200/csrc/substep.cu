@@ -8,6 +8,7 @@
 #include "../../include/empm_b200.h"
 #include <cub/device/device_scan.cuh>
 #include "kernels.cuh"
+#include "adjoint.cuh"
 #include "ctx.hpp"
 
 using namespace empm;
@@ -121,6 +122,12 @@ static void free_sorted(SortedBuffers& sb) {
                     sb.cell_counts, sb.cell_offsets, sb.chunks, sb.nchunks, sb.scan_tmp};
     for (void* q : ptrs) if (q) cudaFree(q);
     sb = SortedBuffers();
+}
+
+static void free_adjoint(AdjointBuffers& ab) {
+    void* ptrs[] = {ab.states, ab.mats, ab.work, ab.fe, ab.gfe, ab.gx, ab.gacc, ab.gmom};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    ab = AdjointBuffers();
 }
 
 static InstanceConsts instance_consts(const EmpmModelParams& P, int n, int poff, int boff) {
@@ -239,6 +246,7 @@ extern "C" int empm_ctx_destroy(EmpmCtx* ctx) {
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     for (cudaEvent_t ev : ctx->timing_events) cudaEventDestroy(ev);
     free_sorted(ctx->sb);
+    free_adjoint(ctx->adj);
     void* ptrs[] = {ctx->d_inst, ctx->grid_mom, ctx->grid_vel, ctx->flags, ctx->d_steps, ctx->d_status};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -803,6 +811,239 @@ extern "C" int empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launch
         total_ms3[k] = total;
         launches3[k] = ctx->timing_count[k];
     }
+    return EMPM_OK;
+}
+
+// ===========================================================================
+// Reverse mode
+// ===========================================================================
+namespace {
+
+__global__ void k_debug_stress_adjoint(const float* Ft9, const float* mu, const float* lam, const float* ys,
+                                       float dt, MaterialScalars ms, const float* gF9, const float* gS9,
+                                       float* g_mu, float* g_lam, float* g_ys, float* gFt9, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    M3 Ft, gF, gS;
+    for (int i = 0; i < 9; ++i) { Ft.m[i] = Ft9[9 * p + i]; gF.m[i] = gF9[9 * p + i]; gS.m[i] = gS9[9 * p + i]; }
+    SpectralEval e;
+    spectral_eval(Ft, mu[p], lam[p], ys[p], dt, ms, e);
+    const SpectralGrad g = spectral_adjoint(e, gF, gS, g_mu[p], g_lam[p], g_ys[p]);
+    for (int i = 0; i < 9; ++i) gFt9[9 * p + i] = g.gFt.m[i];
+    g_mu[p] = g.g_mu;
+    g_lam[p] = g.g_lam;
+    g_ys[p] = g.g_ys;
+}
+
+}  // namespace
+
+// packed x4 | v4 | C | F state at base (the layout of particle_arrays(float*, n))
+static EmpmParticles packed_particles(float* base, int n) {
+    const size_t np = padded4(n);
+    EmpmParticles p;
+    p.x = base;
+    p.v = base + 4 * np;
+    p.C = base + 8 * np;
+    p.F = base + 17 * np;
+    return p;
+}
+
+static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
+    AdjointBuffers& ab = ctx->adj;
+    const size_t np = padded4(ctx->n_particles);
+    if (!ab.gacc) {
+        const size_t grid_bytes = (size_t)ctx->nblocks * 64 * sizeof(float4);
+        CK(cudaMalloc(&ab.gacc, grid_bytes), "adjoint grid");
+        CK(cudaMalloc(&ab.gmom, grid_bytes), "adjoint grid");
+        CK(cudaMemset(ab.gacc, 0, grid_bytes), "adjoint grid");
+        CK(cudaMalloc(&ab.work, 3 * np * sizeof(float)), "adjoint material");
+        CK(cudaMalloc(&ab.fe, 9 * np * sizeof(float)), "adjoint elastic F");
+        CK(cudaMalloc(&ab.gfe, 9 * np * sizeof(float)), "adjoint elastic F");
+        CK(cudaMalloc(&ab.gx, np * sizeof(float4)), "adjoint x");
+    }
+    if (n_steps > ab.capacity) {
+        CK(cudaDeviceSynchronize(), "sync before adjoint buffer growth");
+        if (ab.states) cudaFree(ab.states);
+        if (ab.mats) cudaFree(ab.mats);
+        ab.states = nullptr;
+        ab.mats = nullptr;
+        ab.capacity = 0;
+        CK(cudaMalloc(&ab.states, (size_t)(n_steps + 1) * 26 * np * sizeof(float)), "adjoint segment states");
+        CK(cudaMalloc(&ab.mats, (size_t)n_steps * 3 * np * sizeof(float)), "adjoint segment material");
+        ab.capacity = n_steps;
+    }
+    return EMPM_OK;
+}
+
+extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* ckpt_mu,
+                                    const float* ckpt_lam, const float* ckpt_yield, const EmpmMaterial* mat,
+                                    const EmpmStep* steps, int n_steps, EmpmParticles* grad,
+                                    EmpmMaterialGrad* gmat, void* stream) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    int rc = check_particles(ctx, ckpt, "ckpt");
+    if (!rc) rc = check_particles(ctx, grad, "grad");
+    if (rc) return rc;
+    if (!ckpt_mu || !ckpt_lam || !ckpt_yield)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "checkpoint mu / lam / yield pointer is NULL");
+    if (!mat || !mat->vol) return empm_set_error(ctx, EMPM_ERR_INVALID, "mat or mat->vol is NULL");
+    if (!gmat || !gmat->mu || !gmat->lam || !gmat->yield_stress || !gmat->mass)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "material gradient pointer is NULL");
+    if (n_steps < 1 || n_steps > 100000)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
+    if (!steps) return empm_set_error(ctx, EMPM_ERR_INVALID, "steps is NULL");
+    const int n = ctx->n_particles;
+    cudaStream_t s = (cudaStream_t)stream;
+    // tables [0, n_steps): as given. [n_steps, 2 n_steps): the same without the
+    // velocity modifiers, for recomputing a substep from a stored state whose
+    // velocities already include them.
+    AdjointBuffers& ab = ctx->adj;
+    const size_t per = (size_t)n_steps * ctx->n_inst;
+    ab.tables.assign(steps, steps + per);
+    ab.tables.insert(ab.tables.end(), steps, steps + per);
+    for (size_t t = per; t < 2 * per; ++t) ab.tables[t].n_modifiers = 0;
+    rc = upload_steps(ctx, ab.tables.data(), 2 * n_steps, s);
+    if (rc) return rc;
+    if (n == 0) return EMPM_OK;
+    rc = ensure_adjoint_buffers(ctx, n_steps);
+    if (rc) return rc;
+
+    const size_t np = padded4(n);
+    const size_t state_floats = 26 * np;
+    float* mu_w = ab.work;
+    float* lam_w = ab.work + np;
+    float* ys_w = ab.work + 2 * np;
+    const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
+
+    // 1. forward over the segment from the checkpoint, keeping every state
+    const EmpmParticles s0 = packed_particles(ab.states, n);
+    CK(cudaMemcpyAsync(s0.x, ckpt->x, sizeof(float4) * n, d2d, s), "copy checkpoint");
+    CK(cudaMemcpyAsync(s0.v, ckpt->v, sizeof(float4) * n, d2d, s), "copy checkpoint");
+    CK(cudaMemcpyAsync(s0.C, ckpt->C, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
+    CK(cudaMemcpyAsync(s0.F, ckpt->F, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
+    CK(cudaMemcpyAsync(mu_w, ckpt_mu, sizeof(float) * n, d2d, s), "copy checkpoint");
+    CK(cudaMemcpyAsync(lam_w, ckpt_lam, sizeof(float) * n, d2d, s), "copy checkpoint");
+    CK(cudaMemcpyAsync(ys_w, ckpt_yield, sizeof(float) * n, d2d, s), "copy checkpoint");
+    EmpmMaterial wm = *mat;
+    wm.mu = mu_w;
+    wm.lam = lam_w;
+    wm.yield_stress = ys_w;
+    wm.F_elastic = ab.fe;
+    for (int k = 0; k < n_steps; ++k) {
+        CK(cudaMemcpyAsync(ab.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), d2d, s), "snapshot");
+        const EmpmParticles in = packed_particles(ab.states + (size_t)k * state_floats, n);
+        EmpmParticles out = packed_particles(ab.states + (size_t)(k + 1) * state_floats, n);
+        rc = launch_substep_direct(ctx, &in, &out, &wm, k, s);
+        if (rc) return rc;
+    }
+
+    // 2. substeps in reverse: recompute the grid, then the three adjoint kernels
+    const ParticleArrays Gp = particle_arrays(grad, n);
+    const F9Planes Fe = f9_planes(ab.fe, n);
+    const F9Planes gFe = f9_planes(ab.gfe, n);
+    long long nb = (ctx->nblocks + 3) / 4;
+    if (nb > ctx->sm_count * 8) nb = ctx->sm_count * 8;
+    for (int k = n_steps - 1; k >= 0; --k) {
+        float* snap = ab.mats + (size_t)k * 3 * np;
+        CK(cudaMemcpyAsync(ab.work, snap, 3 * np * sizeof(float), d2d, s), "restore snapshot");
+        EmpmParticles sk = packed_particles(ab.states + (size_t)k * state_floats, n);
+        const ParticleArrays Pk = particle_arrays(&sk, n);
+        MaterialArrays Mw;
+        Mw.vol = mat->vol;
+        Mw.mu = mu_w;
+        Mw.lam = lam_w;
+        Mw.ys = ys_w;
+        Mw.sel = mat->selection;
+        Mw.pid = nullptr;
+        const Launch Lrec = make_launch(ctx, n_steps + k);
+        const Launch Lk = make_launch(ctx, k);
+        k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
+        CK(cudaGetLastError(), "k_p2g_direct (adjoint recompute)");
+        GridUpdateArgs gu;
+        gu.mom = ctx->grid_mom;
+        gu.vel = ctx->grid_vel;
+        gu.flags = ctx->flags;
+        gu.L = Lrec;
+        k_grid_update_keep<<<(int)nb, 256, 0, s>>>(gu);
+        CK(cudaGetLastError(), "k_grid_update_keep");
+        AdjG2PArgs ag;
+        ag.P = Pk;
+        ag.Fe = Fe;
+        ag.M = Mw;
+        ag.Gn = Gp;
+        ag.L = Lk;
+        ag.vel = ctx->grid_vel;
+        ag.gacc = ab.gacc;
+        ag.gx = ab.gx;
+        ag.gFe = gFe;
+        k_adj_g2p<<<blocks_for(n, 128), 128, 0, s>>>(ag);
+        CK(cudaGetLastError(), "k_adj_g2p");
+        AdjGridArgs gg;
+        gg.mom = ctx->grid_mom;
+        gg.gacc = ab.gacc;
+        gg.gmom = ab.gmom;
+        gg.flags = ctx->flags;
+        gg.L = Lk;
+        k_adj_grid<<<(int)nb, 256, 0, s>>>(gg);
+        CK(cudaGetLastError(), "k_adj_grid");
+        AdjP2GArgs ap;
+        ap.P = Pk;
+        ap.M = Mw;
+        ap.M.mu = snap;
+        ap.M.lam = snap + np;
+        ap.M.ys = snap + 2 * np;
+        ap.L = Lk;
+        ap.gmom = ab.gmom;
+        ap.gx = ab.gx;
+        ap.gFe = gFe;
+        ap.G = Gp;
+        ap.g_mu = gmat->mu;
+        ap.g_lam = gmat->lam;
+        ap.g_ys = gmat->yield_stress;
+        ap.g_mass = gmat->mass;
+        k_adj_p2g<<<blocks_for(n, 128), 128, 0, s>>>(ap);
+        CK(cudaGetLastError(), "k_adj_p2g");
+    }
+    return EMPM_OK;
+}
+
+extern "C" int empm_prepare_adjoint(const float* E, const float* nu, const float* g_mu, const float* g_lam,
+                                    float* g_E, float* g_nu, const float* vol, const float* g_mass,
+                                    float* g_density, int n, void* stream) {
+    EmpmCtx* ctx = nullptr;
+    if (n < 0) return empm_set_error(nullptr, EMPM_ERR_INVALID, "n < 0");
+    const bool en = g_E || g_nu;
+    if (en && !(E && nu && g_mu && g_lam && g_E && g_nu))
+        return empm_set_error(nullptr, EMPM_ERR_INVALID, "E, nu, g_mu, g_lam, g_E, g_nu must all be given");
+    if (g_density && !(vol && g_mass))
+        return empm_set_error(nullptr, EMPM_ERR_INVALID, "vol and g_mass are needed for g_density");
+    if (n == 0) return EMPM_OK;
+    k_prepare_adjoint<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        E, nu, g_mu, g_lam, en ? g_E : nullptr, en ? g_nu : nullptr, vol, g_mass, g_density, n);
+    CK(cudaGetLastError(), "k_prepare_adjoint");
+    return EMPM_OK;
+}
+
+extern "C" int empm_debug_stress_adjoint(const EmpmModelParams* params, const float* F_trial9, const float* mu,
+                                         const float* lam, const float* yield_stress, float dt, const float* g_F9,
+                                         const float* g_stress9, float* g_mu, float* g_lam, float* g_yield,
+                                         float* g_F_trial9, int n, void* stream) {
+    EmpmCtx* ctx = nullptr;
+    int rc = validate_params(nullptr, params);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!F_trial9 || !mu || !lam || !yield_stress || !g_F9 || !g_stress9 || !g_mu || !g_lam ||
+                            !g_yield || !g_F_trial9)))
+        return empm_set_error(nullptr, EMPM_ERR_INVALID, "bad empm_debug_stress_adjoint arguments");
+    if (n == 0) return EMPM_OK;
+    MaterialScalars ms;
+    ms.material = params->material;
+    ms.softening = params->softening;
+    ms.hardening = params->hardening;
+    ms.xi = params->xi;
+    ms.plastic_viscosity = params->plastic_viscosity;
+    ms.alpha = params->alpha;
+    k_debug_stress_adjoint<<<blocks_for(n, 128), 128, 0, (cudaStream_t)stream>>>(
+        F_trial9, mu, lam, yield_stress, dt, ms, g_F9, g_stress9, g_mu, g_lam, g_yield, g_F_trial9, n);
+    CK(cudaGetLastError(), "k_debug_stress_adjoint");
     return EMPM_OK;
 }
 

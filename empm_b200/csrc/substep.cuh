@@ -102,12 +102,24 @@ __device__ __forceinline__ bool apply_modifiers(const EmpmStep& st, int mask_ind
 // Grid boundary conditions for node (i, j, k), applied in registration order
 // (the collide closures of mpm_solver_diff.py:473-528, 612-672, 756-793,
 // 835-858, 878-935, 1275-1286). v is the node velocity after normalisation.
-__device__ __forceinline__ void apply_colliders(const EmpmStep& st, int i, int j, int k, int G, float dx,
-                                                long long node, V3& v) {
+//
+// Each collider acts on v as a diagonal projection (plus a constant). The
+// recorder receives, for every collider that changed v, a code: bit a
+// (a = 0, 1, 2) means component a was overwritten by a constant, and bit 3
+// means the remaining components were scaled by 0.3 (surface type 11). The
+// adjoint replays the sequence and applies the transposed projections in
+// reverse order.
+struct NoColliderRecord {
+    __device__ __forceinline__ void operator()(int, unsigned) const {}
+};
+
+template <typename Rec>
+__device__ __forceinline__ void apply_colliders_rec(const EmpmStep& st, int i, int j, int k, int G, float dx,
+                                                    long long node, V3& v, Rec rec) {
     for (int c = 0; c < st.n_colliders; ++c) {
         const EmpmCollider& cl = st.colliders[c];
         if (cl.gate == EMPM_GATE_OFF) continue;
-        if (cl.gate == EMPM_GATE_ZERO_ALL) { v = v3(0.f, 0.f, 0.f); continue; }
+        if (cl.gate == EMPM_GATE_ZERO_ALL) { v = v3(0.f, 0.f, 0.f); rec(c, 7u); continue; }
         const V3 p = v3(cl.point[0], cl.point[1], cl.point[2]);
         const V3 off = v3((float)i * dx - p.x, (float)j * dx - p.y, (float)k * dx - p.z);
         switch (cl.kind) {
@@ -117,25 +129,29 @@ __device__ __forceinline__ void apply_colliders(const EmpmStep& st, int i, int j
                 int shape = (cl.kind == EMPM_COLL_SURFACE) ? EMPM_SHAPE_HALFSPACE : cl.shape;
                 if (shape == EMPM_SHAPE_CUBE) {
                     inside = fabsf(off.x) < cl.size[0] && fabsf(off.y) < cl.size[1] && fabsf(off.z) < cl.size[2];
-                    if (inside) v = v3(0.f, 0.f, 0.f);
+                    if (inside) { v = v3(0.f, 0.f, 0.f); rec(c, 7u); }
                 } else if (shape == EMPM_SHAPE_SPHERE) {
-                    if (length(off) < cl.radius) v = v3(0.f, 0.f, 0.f);
+                    if (length(off) < cl.radius) { v = v3(0.f, 0.f, 0.f); rec(c, 7u); }
                 } else if (shape == EMPM_SHAPE_CYLINDER) {
                     const V3 ax = v3(cl.normal[0], cl.normal[1], cl.normal[2]);
                     const float proj = dot(off, ax);
                     const V3 radial = off - proj * ax;
-                    if (fabsf(proj) < cl.half_height && length(radial) < cl.radius) v = v3(0.f, 0.f, 0.f);
+                    if (fabsf(proj) < cl.half_height && length(radial) < cl.radius) {
+                        v = v3(0.f, 0.f, 0.f);
+                        rec(c, 7u);
+                    }
                 } else if (shape == EMPM_SHAPE_HALFSPACE) {
                     const V3 n = v3(cl.normal[0], cl.normal[1], cl.normal[2]);
                     if (dot(off, n) < 0.f) {
                         if (cl.surface_type == 11) {
                             const float z = (float)k * dx;
-                            if (z < 0.4f || z > 0.53f) v = v3(0.f, 0.f, 0.f);
-                            else v = v3(v.x, 0.f, v.z) * 0.3f;
+                            if (z < 0.4f || z > 0.53f) { v = v3(0.f, 0.f, 0.f); rec(c, 7u); }
+                            else { v = v3(v.x, 0.f, v.z) * 0.3f; rec(c, 2u | 8u); }
                         } else {
                             // sticky, and (as in the reference) slip / separate as well:
                             // the projected velocity is computed there but zero is written.
                             v = v3(0.f, 0.f, 0.f);
+                            rec(c, 7u);
                         }
                     }
                 }
@@ -156,29 +172,38 @@ __device__ __forceinline__ void apply_colliders(const EmpmStep& st, int i, int j
                 } else if (cl.shape == EMPM_SHAPE_HALFSPACE) {
                     inside = dot(off, v3(cl.normal[0], cl.normal[1], cl.normal[2])) < 0.f;
                 }
-                if (inside) v = vset;
+                if (inside) { v = vset; rec(c, 7u); }
                 break;
             }
             case EMPM_COLL_CUBOID_VELOCITY:
-                if (fabsf(off.x) < cl.size[0] && fabsf(off.y) < cl.size[1] && fabsf(off.z) < cl.size[2])
+                if (fabsf(off.x) < cl.size[0] && fabsf(off.y) < cl.size[1] && fabsf(off.z) < cl.size[2]) {
                     v = v3(cl.velocity[0], cl.velocity[1], cl.velocity[2]);
+                    rec(c, 7u);
+                }
                 break;
             case EMPM_COLL_BOUNDING_BOX: {
                 const int pad = 3;
-                if (i < pad && v.x < 0.f) v.x = 0.f;
-                if (i >= G - pad && v.x > 0.f) v.x = 0.f;
-                if (j < pad && v.y < 0.f) v.y = 0.f;
-                if (j >= G - pad && v.y > 0.f) v.y = 0.f;
-                if (k < pad && v.z < 0.f) v.z = 0.f;
-                if (k >= G - pad && v.z > 0.f) v.z = 0.f;
+                unsigned code = 0;
+                if (i < pad && v.x < 0.f) { v.x = 0.f; code |= 1u; }
+                if (i >= G - pad && v.x > 0.f) { v.x = 0.f; code |= 1u; }
+                if (j < pad && v.y < 0.f) { v.y = 0.f; code |= 2u; }
+                if (j >= G - pad && v.y > 0.f) { v.y = 0.f; code |= 2u; }
+                if (k < pad && v.z < 0.f) { v.z = 0.f; code |= 4u; }
+                if (k >= G - pad && v.z > 0.f) { v.z = 0.f; code |= 4u; }
+                if (code) rec(c, code);
                 break;
             }
             case EMPM_COLL_GRID_MASK:
-                if (cl.mask && __ldg(cl.mask + node) >= 1) v = v3(0.f, 0.f, 0.f);
+                if (cl.mask && __ldg(cl.mask + node) >= 1) { v = v3(0.f, 0.f, 0.f); rec(c, 7u); }
                 break;
             default: break;
         }
     }
+}
+
+__device__ __forceinline__ void apply_colliders(const EmpmStep& st, int i, int j, int k, int G, float dx,
+                                                long long node, V3& v) {
+    apply_colliders_rec(st, i, j, k, G, dx, node, v, NoColliderRecord{});
 }
 
 // Grid normalisation, gravity and damping (mpm_utils.py:426-438, 722-734).

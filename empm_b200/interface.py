@@ -9,8 +9,22 @@ Mirrors the four Functions of phys_sim/diff_simulator/warp_mpm/interface.py
 * MPMDifferentiableSimulationWCheckpoint (:476-774) — (x, v, F, C) of a segment
 * MPMDifferentiableSimulationClean (:777-986) — (x, v, F, C, cov)
 
-The forward passes run the CUDA substep; gradients come from the library's
-adjoint kernels (``empm_b200.adjoint``).
+The forward passes run the CUDA substep. With requires_grad the rollout is
+checkpointed (``empm_b200.adjoint.CheckpointedRollout``), and the backward passes
+run the library's adjoint kernels segment by segment. The gradients returned,
+and their quirks, follow the reference's backward passes:
+
+* a scalar (0-d) E or nu gets the per-particle gradients summed and divided by
+  the particle count (interface.py:210-236). For the Trail function that
+  gradient is taken with respect to the 1e6-scaled value;
+* the Trail backward sums the gradient of all records over time and injects it
+  at the final state (interface.py:178-197);
+* MPMDifferentiableSimulation / Trail return no position gradient, and the
+  density gradient restricted to ``density_change_mask`` (interface.py:238-251);
+* gradients are taken at the start of the taped substeps. With
+  extra_no_grad_steps > 0, Simulation and Trail therefore return zero velocity
+  and density gradients (their inputs are not on the tape), while
+  WCheckpoint / Clean return the gradients at the state after the extra steps.
 """
 from __future__ import annotations
 
@@ -20,7 +34,11 @@ import torch
 import torch.autograd as autograd
 from torch import Tensor
 
+from .adjoint import CheckpointedRollout, prepare_adjoint
 from .mpm_data_structure import MPMModelStruct, MPMStateStruct
+
+#: substeps between checkpoints of a differentiable rollout (MPMWARPDiff.checkpoint_every overrides it)
+CHECKPOINT_EVERY = 20
 
 
 def _set_E_nu(mpm_solver, mpm_model, E: Tensor, nu: Tensor, scale_scalar_E: float = 1.0):
@@ -50,6 +68,23 @@ def _run(mpm_solver, mpm_model, state, n_steps, dt, record_every=None, step_call
     return cur, recorded
 
 
+def _taped_run(mpm_solver, mpm_model, state, n_steps, dt, step_callback=None):
+    tape = CheckpointedRollout(mpm_solver, mpm_model, state, dt, n_steps,
+                               checkpoint_every=int(getattr(mpm_solver, "checkpoint_every", CHECKPOINT_EVERY)),
+                               step_callback=step_callback)
+    return tape, tape.forward()
+
+
+def _param_grads(ctx, res):
+    """(E_grad, nu_grad, density_grad) from the tape's mu / lam / mass adjoints."""
+    model, state = ctx.mpm_model, ctx.tape_state
+    n = state.n_particles
+    g_E, g_nu, g_rho = prepare_adjoint(model.E, model.nu, res["mu"], res["lam"], state.particle_vol, res["mass"])
+    E_grad = g_E.sum() / n if ctx.aggregating_E else g_E
+    nu_grad = g_nu.sum() / n if ctx.aggregating_nu else g_nu
+    return E_grad, nu_grad, g_rho
+
+
 def _fast_run(mpm_solver, mpm_model, state, n_steps, dt):
     if n_steps <= 0:
         return state
@@ -60,6 +95,10 @@ def _fast_run(mpm_solver, mpm_model, state, n_steps, dt):
     work._C.copy_(state._C)
     work._F_trial.copy_(state._F_trial)
     return mpm_solver.rollout(mpm_model, work, other, dt, n_steps)
+
+
+def _masked_density(g_rho: Tensor, mask: Optional[Tensor]) -> Tensor:
+    return g_rho if mask is None else g_rho[mask.to(g_rho.device).bool()]
 
 
 class MPMDifferentiableSimulationTrail(autograd.Function):
@@ -84,14 +123,32 @@ class MPMDifferentiableSimulationTrail(autograd.Function):
             prev, _ = _run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
         prev.update_mass()
         mpm_solver.prepare_mu_lam(mpm_model, prev, device=device)
-        final, recorded = _run(mpm_solver, mpm_model, prev, num_substeps, substep_size, record_every=substep,
-                               step_callback=mpm_solver.step_callback)
-        ctx.final_state = final
-        return torch.stack(recorded, dim=0)
+        ctx.requires_grad = requires_grad
+        if not requires_grad:
+            final, recorded = _run(mpm_solver, mpm_model, prev, num_substeps, substep_size, record_every=substep,
+                                   step_callback=mpm_solver.step_callback)
+            ctx.final_state = final
+            return torch.stack(recorded, dim=0)
+        tape = CheckpointedRollout(mpm_solver, mpm_model, prev, substep_size, num_substeps,
+                                   checkpoint_every=int(getattr(mpm_solver, "checkpoint_every", CHECKPOINT_EVERY)),
+                                   record_every=substep, step_callback=mpm_solver.step_callback)
+        ctx.final_state = tape.forward()
+        ctx.tape, ctx.tape_state, ctx.mpm_model = tape, prev, mpm_model
+        ctx.on_tape = extra_no_grad_steps == 0
+        ctx.save_for_backward(density_change_mask)
+        return torch.stack(tape.records, dim=0)
 
     @staticmethod
     def backward(ctx, out_pos_grad):
-        raise NotImplementedError("adjoint of MPMDifferentiableSimulationTrail is not available in this build")
+        # interface.py:178-197: the record gradients are summed over time and
+        # injected at the final state
+        res = ctx.tape.backward(g_x=out_pos_grad.sum(dim=0))
+        E_grad, nu_grad, density_grad = _param_grads(ctx, res)
+        velo_grad = res["v"] if ctx.on_tape else torch.zeros_like(res["v"])
+        density_grad = _masked_density(density_grad if ctx.on_tape else torch.zeros_like(density_grad),
+                                       ctx.saved_tensors[0])
+        return (None, None, None, None, None, None, None, velo_grad, E_grad, nu_grad, density_grad, None, None,
+                None, None, None)
 
 
 class MPMDifferentiableSimulation(autograd.Function):
@@ -116,12 +173,23 @@ class MPMDifferentiableSimulation(autograd.Function):
             prev = _fast_run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
         prev.update_mass()
         mpm_solver.prepare_mu_lam(mpm_model, prev, device=device)
-        final = _fast_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        if not requires_grad:
+            return _fast_run(mpm_solver, mpm_model, prev, num_substeps, substep_size).particle_x.clone()
+        ctx.tape, final = _taped_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        ctx.tape_state, ctx.mpm_model = prev, mpm_model
+        ctx.on_tape = extra_no_grad_steps == 0
+        ctx.save_for_backward(density_change_mask)
         return final.particle_x.clone()
 
     @staticmethod
     def backward(ctx, out_pos_grad):
-        raise NotImplementedError("adjoint of MPMDifferentiableSimulation is not available in this build")
+        res = ctx.tape.backward(g_x=out_pos_grad)
+        E_grad, nu_grad, density_grad = _param_grads(ctx, res)
+        velo_grad = res["v"] if ctx.on_tape else torch.zeros_like(res["v"])
+        density_grad = _masked_density(density_grad if ctx.on_tape else torch.zeros_like(density_grad),
+                                       ctx.saved_tensors[0])
+        return (None, None, None, None, None, None, None, velo_grad, E_grad, nu_grad, density_grad, None, None,
+                None, None, None)
 
 
 class MPMDifferentiableSimulationWCheckpoint(autograd.Function):
@@ -140,14 +208,18 @@ class MPMDifferentiableSimulationWCheckpoint(autograd.Function):
         prev = mpm_state
         if extra_no_grad_steps > 0:
             prev = _fast_run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
-        final = _fast_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        ctx.tape, final = _taped_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        ctx.tape_state, ctx.mpm_model = prev, mpm_model
         n = final.n_particles
         return (final.particle_x.clone(), final.particle_v.clone(), final.particle_F_trial.reshape(n, 3, 3).clone(),
                 final.particle_C.reshape(n, 3, 3).clone())
 
     @staticmethod
-    def backward(ctx, *grads):
-        raise NotImplementedError("adjoint of MPMDifferentiableSimulationWCheckpoint is not available in this build")
+    def backward(ctx, out_pos_grad, out_velo_grad, out_F_grad, out_C_grad):
+        res = ctx.tape.backward(g_x=out_pos_grad, g_v=out_velo_grad, g_C=out_C_grad, g_F=out_F_grad)
+        E_grad, nu_grad, density_grad = _param_grads(ctx, res)
+        return (None, None, None, None, None, res["x"], res["v"], res["F"], res["C"], E_grad, nu_grad, density_grad,
+                None, None, None, None)
 
 
 class MPMDifferentiableSimulationClean(autograd.Function):
@@ -168,11 +240,17 @@ class MPMDifferentiableSimulationClean(autograd.Function):
             prev = _fast_run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
         prev.update_mass()
         mpm_solver.prepare_mu_lam(mpm_model, prev, device=device)
-        final = _fast_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        ctx.tape, final = _taped_run(mpm_solver, mpm_model, prev, num_substeps, substep_size)
+        ctx.tape_state, ctx.mpm_model = prev, mpm_model
         n = final.n_particles
         return (final.particle_x.clone(), final.particle_v.clone(), final.particle_F_trial.reshape(n, 3, 3).clone(),
                 final.particle_C.reshape(n, 3, 3).clone(), final.particle_cov.view(-1, 6).clone())
 
     @staticmethod
-    def backward(ctx, *grads):
-        raise NotImplementedError("adjoint of MPMDifferentiableSimulationClean is not available in this build")
+    def backward(ctx, out_pos_grad, out_velo_grad, out_F_grad, out_C_grad, out_cov_grad):
+        # the covariance output is a pass-through (its update is disabled in the
+        # reference, mpm_utils.py:578), so its gradient does not reach the inputs
+        res = ctx.tape.backward(g_x=out_pos_grad, g_v=out_velo_grad, g_C=out_C_grad, g_F=out_F_grad)
+        E_grad, nu_grad, density_grad = _param_grads(ctx, res)
+        return (None, None, None, None, None, res["x"], res["v"], res["F"], res["C"], E_grad, nu_grad, density_grad,
+                None, None, None, None)

@@ -265,7 +265,61 @@ int  empm_last_error(EmpmCtx* ctx, char* buf, int len);
 int  empm_substep_noalloc(const EmpmModelParams* params, const EmpmParticles* in, EmpmParticles* out,
                           const EmpmMaterial* mat, const EmpmStep* step, int n_particles, void* stream);
 
+/* ---- reverse mode ----------------------------------------------------------- */
+
+/* Adjoints of the per-particle material scalars and of the mass (device
+ * arrays of n_particles floats). */
+typedef struct {
+    float* mu;             /* in: dL/dmu after the segment; out: dL/dmu at its start */
+    float* lam;            /* same for lam */
+    float* yield_stress;   /* same for the yield stress */
+    float* mass;           /* dL/dmass of the segment is ADDED here */
+} EmpmMaterialGrad;
+
+/* Reverse-mode differentiation of n_steps substeps starting from a
+ * checkpoint. Replaces the replay of Warp's generated adjoints
+ * (tape.backward, interface.py:197,418,720,935; the checkpointed replay of
+ * MPMDifferentiableSimulationWCheckpoint.backward, interface.py:579-774)
+ * through p2g2p_differentiable (mpm_solver_diff.py:165-291).
+ *   ckpt            state at the segment start (library layout, as the input of
+ *                   empm_substep; not modified);
+ *   ckpt_mu/lam/yield  material scalars at the segment start (device, n floats);
+ *   mat             vol and selection are used; mu, lam, yield_stress and
+ *                   F_elastic are ignored;
+ *   steps           n_steps tables of n_instances schedules, as given to
+ *                   empm_rollout with n_tables = n_steps;
+ *   grad            in: dL/d(state after the segment) in the library layout
+ *                   (x and v planes as float4 with w ignored, C and F_trial as
+ *                   f9 planes); out: dL/d(state at the segment start);
+ *   gmat            see EmpmMaterialGrad.
+ * The segment is recomputed from the checkpoint and the state of every
+ * substep is kept in context-owned memory: about 120 bytes per particle and
+ * substep, allocated on first use and grown as needed (so call it outside
+ * stream capture). The adjoint of each substep then recomputes that substep's
+ * grid and runs the three adjoint kernels. The result is the gradient of the
+ * FP32 forward map, up to FP32 rounding. The velocity written by a rotation
+ * modifier is treated as independent of x. */
+int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* ckpt_mu, const float* ckpt_lam,
+                          const float* ckpt_yield, const EmpmMaterial* mat, const EmpmStep* steps, int n_steps,
+                          EmpmParticles* grad, EmpmMaterialGrad* gmat, void* stream);
+
+/* Chain rule through empm_prepare: dL/dE and dL/dnu from dL/dmu and dL/dlam
+ * (compute_mu_lam_from_E_nu, mpm_utils.py:277-283), and dL/ddensity =
+ * dL/dmass * vol (get_float_array_product, mpm_data_structure.py:719-726).
+ * Either group of pointers may be NULL. */
+int  empm_prepare_adjoint(const float* E, const float* nu, const float* g_mu, const float* g_lam, float* g_E,
+                          float* g_nu, const float* vol, const float* g_mass, float* g_density, int n, void* stream);
+
 /* ---- diagnostics (used by the parity tests) ------------------------------ */
+
+/* Adjoint of empm_debug_stress for n particles (row-major [N,3,3] like it):
+ * given dL/dF_elastic, dL/dstress and dL/d(mu, lam, yield after the update),
+ * returns dL/dF_trial and overwrites g_mu, g_lam, g_yield with dL/d(mu, lam,
+ * yield before the update). mu, lam, yield_stress are inputs only. */
+int  empm_debug_stress_adjoint(const EmpmModelParams* params, const float* F_trial9, const float* mu,
+                               const float* lam, const float* yield_stress, float dt, const float* g_F9,
+                               const float* g_stress9, float* g_mu, float* g_lam, float* g_yield,
+                               float* g_F_trial9, int n, void* stream);
 
 /* Return map + Kirchhoff stress of the material switch for n particles, on
  * the device, in the reference's [N,3,3] row-major layout: the body of

@@ -120,6 +120,28 @@ def svd3(A: np.ndarray, precision: str = "fp64"):
     return U, s, V
 
 
+def stress(material: int, F_trial: np.ndarray, mu: np.ndarray, lam: np.ndarray, ys: np.ndarray, dt: float,
+           softening: float = 0.1, hardening: float = 0.0, xi: float = 0.0, plastic_viscosity: float = 0.0,
+           alpha: float = 0.0, precision: str = "fp64"):
+    """Return map + Kirchhoff stress of n particles (compute_stress_from_F_trial,
+    mpm_utils.py:602-665). Returns (F_elastic [n,9], stress [n,9], mu', lam', ys')."""
+    L = lib(precision)
+    R = L.np_real
+    n = F_trial.shape[0]
+    Ft = np.ascontiguousarray(F_trial, dtype=R).reshape(n, 9)
+    mu = np.array(mu, dtype=R).reshape(n)
+    lam = np.array(lam, dtype=R).reshape(n)
+    ys = np.array(ys, dtype=R).reshape(n)
+    Fe = np.zeros((n, 9), R)
+    S = np.zeros((n, 9), R)
+    m = L.OrModel()
+    m.material = int(material)
+    m.softening, m.hardening, m.xi = softening, hardening, xi
+    m.plastic_viscosity, m.alpha = plastic_viscosity, alpha
+    L.lib.or_stress(ctypes.byref(m), n, None, _ptr(Ft), _ptr(mu), _ptr(lam), _ptr(ys), R(dt), _ptr(Fe), _ptr(S))
+    return Fe, S, mu, lam, ys
+
+
 @dataclass
 class OrColliderSpec:
     """One collider in registration order (fields as in Dirichlet_collider)."""

@@ -64,3 +64,25 @@ def test_batch_create_rejects_bad_arguments_without_gpu():
     assert L.empm_batch_create(p, counts, 0, 4, ctypes.byref(out)) == -1        # no instances
     p[1].n_grid = 3
     assert L.empm_batch_create(p, counts, 2, 4, ctypes.byref(out)) == -1        # bad grid in instance 1
+
+
+def test_adjoint_entry_points_reject_bad_arguments_without_gpu():
+    L = N.lib()
+    g = N.EmpmParticles()
+    gm = N.EmpmMaterialGrad()
+    mat = N.EmpmMaterial()
+    st = (N.EmpmStep * 1)()
+    assert L.empm_adjoint_segment(None, g, None, None, None, mat, st, 1, g, gm, None) == -1
+    assert "ctx" in N.last_error()
+    assert L.empm_prepare_adjoint(None, None, None, None, None, None, None, None, None, -1, None) == -1
+    # g_E without E / nu / g_mu / g_lam
+    buf = (ctypes.c_float * 4)()
+    assert L.empm_prepare_adjoint(None, None, None, None, buf, buf, None, None, None, 4, None) == -1
+    # g_density without vol / g_mass
+    assert L.empm_prepare_adjoint(None, None, None, None, None, None, None, None, buf, 4, None) == -1
+    # nothing to do: accepted without touching the device
+    assert L.empm_prepare_adjoint(None, None, None, None, None, None, None, None, None, 0, None) == 0
+    p = N.EmpmModelParams()
+    p.n_grid, p.grid_lim = 16, 1.0
+    assert L.empm_debug_stress_adjoint(p, None, None, None, None, 0.0, None, None, None, None, None, None, 3,
+                                       None) == -1
