@@ -150,7 +150,7 @@ def get_workload(name, particles=None, grid=None, substeps=None):
         kw["G"] = grid
     if substeps:
         kw["T"] = substeps
-    return {"c1": W.c1, "c2": W.c2}[name](**kw)
+    return {"c1": W.c1, "c2": W.c2, "c3": W.c3}[name](**kw)
 
 
 def cpu_baseline(w, budget_s=12.0, max_substeps=40):
@@ -633,12 +633,213 @@ def run_ours_c4(args):
     return 0
 
 
+ADJ_P2G_BYTES = 308   # adjoint P2G per particle: state, material, G2P adjoints and carried adjoints in; state adjoint out
+
+
+def run_ours_c3(args):
+    """Gradient of the differentiable rollout: one step = checkpointed forward
+    of T substeps + the adjoint of all of them, for the loss mean |x_T - x_target|^2
+    (x_target: the same initial state rolled out with the target material)."""
+    import torch
+
+    world, rank, local = dist_setup(args)
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from empm_b200 import workloads as W
+    from empm_b200.adjoint import CheckpointedRollout, prepare_adjoint
+    from empm_b200.interface import MPMDifferentiableSimulation
+
+    kw = {k: v for k, v in (("n", args.particles), ("G", args.grid), ("T", args.substeps)) if v}
+    w = W.c3(**kw)
+    target = W.c3(guess=False, **kw)
+    every = args.checkpoint_every
+    solver, md, st, other = W.build_product(target, device=dev)
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap"):
+        val = getattr(args, opt)
+        if val is not None:
+            setattr(solver, opt, val)
+    x_target = solver.rollout(md, st, other, w.dt, w.T).particle_x.clone()
+    # the guess: same initial state, guess material
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)  # noqa: E731
+    md.E.copy_(t(w.E))
+    md.nu.copy_(t(w.nu))
+    init = dict(x=t(np.concatenate([w.x, (w.vol * w.rho)[:, None]], 1).astype(np.float32)),
+                v=t(np.concatenate([w.v, np.zeros((w.n, 1), np.float32)], 1)), ys=t(w.ys))
+    n = w.n
+
+    def reset():
+        st._x4.copy_(init["x"])
+        st._v4.copy_(init["v"])
+        st._C.zero_()
+        st.particle_F_trial = torch.eye(3, device=dev).expand(n, 3, 3)
+        md.finalize_mu_lam(n)
+        md.yield_stress.copy_(init["ys"])
+        solver.time = 0.0
+
+    def grad_step():
+        reset()
+        tape = CheckpointedRollout(solver, md, st, w.dt, w.T, checkpoint_every=every)
+        final = tape.forward()
+        diff = final.particle_x - x_target
+        res = tape.backward(g_x=2.0 * diff / n)
+        g_E, g_nu, _ = prepare_adjoint(md.E, md.nu, res["mu"], res["lam"])
+        return (diff * diff).sum(1).mean(), g_E.sum(), g_nu.sum(), res["yield_stress"].sum()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+
+            tt = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            return float(tt.item())
+        return x
+
+    for _ in range(args.warmup):
+        out = grad_step()
+    torch.cuda.synchronize()
+    loss0 = float(out[0])
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        out = grad_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * n * w.T * args.steps / (ms / 1e3)
+    grads = {"loss": float(out[0]), "dL/dE (sum)": float(out[1]), "dL/dnu (sum)": float(out[2]),
+             "dL/dyield (sum)": float(out[3])}
+
+    # forward-only rollout of the same workload, for the gradient / forward cost ratio
+    def fwd_step():
+        reset()
+        solver.rollout(md, st, other, w.dt, w.T)
+
+    fwd_step()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        fwd_step()
+    f1.record()
+    torch.cuda.synchronize()
+    fwd_ms = f0.elapsed_time(f1) / args.steps
+
+    # per-kernel durations on the stream path (CUDA events around each launch)
+    solver.use_graph = False
+    solver.kernel_timing(True, max_launches=3 * w.T + 8)
+    torch.cuda.synchronize()
+    grad_step()
+    torch.cuda.synchronize()
+    kt = solver.kernel_times()
+    akt = solver.adjoint_kernel_times()
+    solver.kernel_timing(False)
+    solver.use_graph = True
+    kms = {k: v[0] / max(v[1], 1) for k, v in list(kt.items()) + list(akt.items())}
+    peak, peak_kind = load_peaks()
+    bp = bytes_per_particle(w.material)
+    dom = "adj_p2g"
+    achieved = n * ADJ_P2G_BYTES / (kms[dom] / 1e3) / 1e9
+    adj_ms = ms / args.steps - fwd_ms
+    adj_substep_frac = (n * 3 * bp["substep"] / (adj_ms / w.T / 1e3) / 1e9) / peak
+
+    # end to end through the reference's autograd Function with host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    hx, hv, hrho, hys = pin(w.x), pin(w.v), pin(w.rho), pin(w.ys)
+    hgv = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    hgs = torch.empty(3, dtype=torch.float32).pin_memory()
+    mask = torch.ones(n, dtype=torch.int32, device=dev)
+
+    def e2e_step():
+        x0 = hx.to(dev, non_blocking=True)
+        v0 = hv.to(dev, non_blocking=True).requires_grad_(True)
+        rho = hrho.to(dev, non_blocking=True).requires_grad_(True)
+        md.yield_stress.copy_(hys, non_blocking=True)
+        E = torch.tensor(float(w.E[0]), device=dev, requires_grad=True)
+        nu = torch.tensor(float(w.nu[0]), device=dev, requires_grad=True)
+        solver.time = 0.0
+        xo = MPMDifferentiableSimulation.apply(solver, st, md, 1, w.dt, w.T, x0, v0, E, nu, rho, mask, None, dev,
+                                               True, 0)
+        loss = ((xo - x_target) ** 2).sum(1).mean()
+        loss.backward()
+        hgv.copy_(v0.grad, non_blocking=True)
+        hgs.copy_(torch.stack([loss.detach(), E.grad, nu.grad]), non_blocking=True)
+
+    st.set_require_grad(True)
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    q1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1))
+    e2e_value = world * n * w.T * args.steps / (e2e_ms / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w)
+        cpu["sample"] += "; forward substeps only: the CPU oracle has no adjoint"
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "differentiated " + METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.description + f", checkpoint every {every}, loss mean |x_T - x_target|^2",
+                   "particles": n, "grid": w.G, "substeps_per_step": w.T, "dt": w.dt,
+                   "step": "checkpointed forward + adjoint of every substep (gradients in x0, v0, C0, F0, "
+                           "mu, lam, yield, mass; E and nu through the prepare adjoint)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (segment states ~0.5 GB > 126 MB), no flush",
+                   "forward_ms": fwd_ms, "gradient_over_forward": (ms / args.steps) / fwd_ms,
+                   "adjoint_substep_hbm_frac": adj_substep_frac,
+                   "adjoint_bytes_per_particle_substep": 3 * bp["substep"],
+                   "loss_at_first_timed_step": loss0, "gradients": grads},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_particle": ADJ_P2G_BYTES, "launch_ms": kms[dom],
+                     "kernel_ms": {k: round(v, 5) for k, v in kms.items()},
+                     "timing": "CUDA events around each kernel on its launch stream, stream path of one "
+                               "gradient step in this run"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n * (12 + 12 + 4 + 4),
+                "d2h_bytes_per_step": n * 12 + 12,
+                "path": "MPMDifferentiableSimulation.apply + loss.backward() with pinned host inputs"},
+        # forward: 3 kernels per substep (+ sorts); adjoint: 3 forward + 2 recompute + 3 adjoint kernels per substep
+        "gpu_launches": 11 * w.T * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c4"])
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--checkpoint-every", dest="checkpoint_every", type=int, default=20,
+                    help="c3: substeps between checkpoints of the differentiable rollout")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="c4: skip the one-instance-at-a-time comparison")
@@ -653,6 +854,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_c4(args) if args.workload == "c4" else run_reference(args)
+    if args.workload == "c3":
+        return run_ours_c3(args)
     return run_ours_c4(args) if args.workload == "c4" else run_ours(args)
 
 

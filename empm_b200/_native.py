@@ -124,6 +124,7 @@ def lib():
         "empm_ctx_timing": ([P, I, I], I),
         "empm_ctx_set_option": ([P, I, I], I),
         "empm_ctx_kernel_times": ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
+        "empm_ctx_adjoint_kernel_times": ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

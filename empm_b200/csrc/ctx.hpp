@@ -54,6 +54,8 @@ struct AdjointBuffers {
     float4* gx = nullptr;      // x adjoint through G2P
     float4* gacc = nullptr;    // node velocity adjoint (blocked grid), zero between substeps
     float4* gmom = nullptr;    // adjoint of the P2G accumulation (blocked grid)
+    float*  gstate = nullptr;  // state adjoint in cell order (packed like states)
+    float*  gmats = nullptr;   // mu | lam | yield | mass adjoints in cell order
     std::vector<EmpmStep> tables;   // host staging of the step tables
 };
 
@@ -93,8 +95,10 @@ struct EmpmCtx {
     // per-kernel event timing (stream path only)
     bool         timing = false;
     int          timing_capacity = 0;
-    int          timing_count[3] = {0, 0, 0};
-    std::vector<cudaEvent_t> timing_events;   // [3][capacity][2]
+    // timed kernels: 0 stress+P2G, 1 grid update, 2 G2P, 3 adjoint G2P, 4 adjoint grid, 5 adjoint P2G
+    static constexpr int kTimedKernels = 6;
+    int          timing_count[kTimedKernels] = {0, 0, 0, 0, 0, 0};
+    std::vector<cudaEvent_t> timing_events;   // [kTimedKernels][capacity][2]
     char         err[512] = {0};
 };
 

@@ -125,7 +125,7 @@ static void free_sorted(SortedBuffers& sb) {
 }
 
 static void free_adjoint(AdjointBuffers& ab) {
-    void* ptrs[] = {ab.states, ab.mats, ab.work, ab.fe, ab.gfe, ab.gx, ab.gacc, ab.gmom};
+    void* ptrs[] = {ab.states, ab.mats, ab.work, ab.fe, ab.gfe, ab.gx, ab.gacc, ab.gmom, ab.gstate, ab.gmats};
     for (void* q : ptrs) if (q) cudaFree(q);
     ab = AdjointBuffers();
 }
@@ -782,11 +782,11 @@ extern "C" int empm_batch_info(EmpmCtx* ctx, int* n_instances, int* particle_off
 
 extern "C" int empm_ctx_timing(EmpmCtx* ctx, int enable, int max_launches) {
     if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
-    ctx->timing_count[0] = ctx->timing_count[1] = ctx->timing_count[2] = 0;
+    for (int k = 0; k < EmpmCtx::kTimedKernels; ++k) ctx->timing_count[k] = 0;
     if (!enable) { ctx->timing = false; return EMPM_OK; }
     if (max_launches < 1 || max_launches > 1000000)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "max_launches %d out of [1, 1000000]", max_launches);
-    const size_t need = (size_t)3 * max_launches * 2;
+    const size_t need = (size_t)EmpmCtx::kTimedKernels * max_launches * 2;
     while (ctx->timing_events.size() < need) {
         cudaEvent_t ev;
         CK(cudaEventCreate(&ev), "cudaEventCreate");
@@ -797,9 +797,10 @@ extern "C" int empm_ctx_timing(EmpmCtx* ctx, int enable, int max_launches) {
     return EMPM_OK;
 }
 
-extern "C" int empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3) {
+static int kernel_times(EmpmCtx* ctx, int first, float* total_ms3, int* launches3) {
     if (!ctx || !total_ms3 || !launches3) return empm_set_error(ctx, EMPM_ERR_INVALID, "bad arguments");
-    for (int k = 0; k < 3; ++k) {
+    for (int j = 0; j < 3; ++j) {
+        const int k = first + j;
         float total = 0.f;
         for (int i = 0; i < ctx->timing_count[k]; ++i) {
             const size_t base = ((size_t)k * ctx->timing_capacity + i) * 2;
@@ -808,10 +809,18 @@ extern "C" int empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launch
             CK(cudaEventElapsedTime(&ms, ctx->timing_events[base], ctx->timing_events[base + 1]), "cudaEventElapsedTime");
             total += ms;
         }
-        total_ms3[k] = total;
-        launches3[k] = ctx->timing_count[k];
+        total_ms3[j] = total;
+        launches3[j] = ctx->timing_count[k];
     }
     return EMPM_OK;
+}
+
+extern "C" int empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3) {
+    return kernel_times(ctx, 0, total_ms3, launches3);
+}
+
+extern "C" int empm_ctx_adjoint_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3) {
+    return kernel_times(ctx, 3, total_ms3, launches3);
 }
 
 // ===========================================================================
@@ -833,6 +842,33 @@ __global__ void k_debug_stress_adjoint(const float* Ft9, const float* mu, const 
     g_mu[p] = g.g_mu;
     g_lam[p] = g.g_lam;
     g_ys[p] = g.g_ys;
+}
+
+// Adjoint state between the caller's order and cell order: to_sorted gathers
+// dst[i] = src[pid[i]]; otherwise scatters dst[pid[i]] = src[i].
+struct GradPermuteArgs {
+    ParticleArrays src, dst;
+    const float* s_mu; const float* s_lam; const float* s_ys; const float* s_mass;
+    float* d_mu; float* d_lam; float* d_ys; float* d_mass;
+    const int* pid;
+    int n;
+    int to_sorted;
+};
+
+__global__ void k_permute_grad(const GradPermuteArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int u = __ldg(a.pid + i);
+    const int s = a.to_sorted ? u : i;
+    const int d = a.to_sorted ? i : u;
+    a.dst.x[d] = __ldg(a.src.x + s);
+    a.dst.v[d] = __ldg(a.src.v + s);
+    f9_store(a.dst.C, d, f9_load(a.src.C, s));
+    f9_store(a.dst.F, d, f9_load(a.src.F, s));
+    a.d_mu[d] = __ldg(a.s_mu + s);
+    a.d_lam[d] = __ldg(a.s_lam + s);
+    a.d_ys[d] = __ldg(a.s_ys + s);
+    a.d_mass[d] = __ldg(a.s_mass + s);
 }
 
 }  // namespace
@@ -860,6 +896,8 @@ static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
         CK(cudaMalloc(&ab.fe, 9 * np * sizeof(float)), "adjoint elastic F");
         CK(cudaMalloc(&ab.gfe, 9 * np * sizeof(float)), "adjoint elastic F");
         CK(cudaMalloc(&ab.gx, np * sizeof(float4)), "adjoint x");
+        CK(cudaMalloc(&ab.gstate, 26 * np * sizeof(float)), "adjoint state");
+        CK(cudaMalloc(&ab.gmats, 4 * np * sizeof(float)), "adjoint material");
     }
     if (n_steps > ab.capacity) {
         CK(cudaDeviceSynchronize(), "sync before adjoint buffer growth");
@@ -872,6 +910,25 @@ static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
         CK(cudaMalloc(&ab.mats, (size_t)n_steps * 3 * np * sizeof(float)), "adjoint segment material");
         ab.capacity = n_steps;
     }
+    return EMPM_OK;
+}
+
+// One forward substep on explicit particle arrays (the states of a segment).
+static int launch_substep_arrays(EmpmCtx* ctx, const ParticleArrays& Pin, const ParticleArrays& Pout,
+                                 const MaterialArrays& M, F9Planes Fe, int table, bool warpagg, cudaStream_t s) {
+    const int n = ctx->n_particles;
+    const Launch L = make_launch(ctx, table);
+    timing_mark(ctx, 0, 0, s);
+    if (warpagg) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags);
+    else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags);
+    timing_mark(ctx, 0, 1, s);
+    CK(cudaGetLastError(), "adjoint segment P2G");
+    int rc = launch_grid_update(ctx, table, s);
+    if (rc) return rc;
+    timing_mark(ctx, 2, 0, s);
+    k_g2p_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Fe, M, Pout, L, ctx->grid_vel);
+    timing_mark(ctx, 2, 1, s);
+    CK(cudaGetLastError(), "adjoint segment G2P");
     return EMPM_OK;
 }
 
@@ -914,56 +971,105 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
     float* ys_w = ab.work + 2 * np;
     const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
 
-    // 1. forward over the segment from the checkpoint, keeping every state
-    const EmpmParticles s0 = packed_particles(ab.states, n);
-    CK(cudaMemcpyAsync(s0.x, ckpt->x, sizeof(float4) * n, d2d, s), "copy checkpoint");
-    CK(cudaMemcpyAsync(s0.v, ckpt->v, sizeof(float4) * n, d2d, s), "copy checkpoint");
-    CK(cudaMemcpyAsync(s0.C, ckpt->C, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
-    CK(cudaMemcpyAsync(s0.F, ckpt->F, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
-    CK(cudaMemcpyAsync(mu_w, ckpt_mu, sizeof(float) * n, d2d, s), "copy checkpoint");
-    CK(cudaMemcpyAsync(lam_w, ckpt_lam, sizeof(float) * n, d2d, s), "copy checkpoint");
-    CK(cudaMemcpyAsync(ys_w, ckpt_yield, sizeof(float) * n, d2d, s), "copy checkpoint");
-    EmpmMaterial wm = *mat;
-    wm.mu = mu_w;
-    wm.lam = lam_w;
-    wm.yield_stress = ys_w;
-    wm.F_elastic = ab.fe;
+    // 1. the checkpoint as segment state 0: in cell order when the context
+    //    sorts (the whole segment then runs in that order), else as given
+    const bool sorted = ctx->sort_every > 0;
+    MaterialArrays base;
+    base.vol = mat->vol;
+    base.mu = base.lam = base.ys = nullptr;
+    base.sel = mat->selection;
+    base.pid = nullptr;
+    ParticleArrays Gp = particle_arrays(grad, n);
+    float* gm_mu = gmat->mu;
+    float* gm_lam = gmat->lam;
+    float* gm_ys = gmat->yield_stress;
+    float* gm_mass = gmat->mass;
+    GradPermuteArgs perm;
+    if (sorted) {
+        rc = ensure_sorted_buffers(ctx);
+        if (rc) return rc;
+        SortedState ss;
+        const ParticleArrays ua = particle_arrays(ckpt, n);
+        EmpmMaterial um = *mat;
+        um.mu = const_cast<float*>(ckpt_mu);
+        um.lam = const_cast<float*>(ckpt_lam);
+        um.yield_stress = const_cast<float*>(ckpt_yield);
+        rc = launch_sort(ctx, ss, &ua, &um, s);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ab.states, ctx->sb.part[ss.pc], state_floats * sizeof(float), d2d, s), "sorted checkpoint");
+        const MaterialArrays SM = sorted_material(ctx, ss.mc);
+        CK(cudaMemcpyAsync(mu_w, SM.mu, sizeof(float) * n, d2d, s), "sorted checkpoint");
+        CK(cudaMemcpyAsync(lam_w, SM.lam, sizeof(float) * n, d2d, s), "sorted checkpoint");
+        CK(cudaMemcpyAsync(ys_w, SM.ys, sizeof(float) * n, d2d, s), "sorted checkpoint");
+        base.vol = SM.vol;
+        base.sel = SM.sel;
+        base.pid = SM.pid;
+        // incoming adjoint into cell order
+        const EmpmParticles gs = packed_particles(ab.gstate, n);
+        perm.src = Gp;
+        perm.dst = particle_arrays(&gs, n);
+        perm.s_mu = gmat->mu; perm.s_lam = gmat->lam; perm.s_ys = gmat->yield_stress; perm.s_mass = gmat->mass;
+        gm_mu = ab.gmats;
+        gm_lam = ab.gmats + np;
+        gm_ys = ab.gmats + 2 * np;
+        gm_mass = ab.gmats + 3 * np;
+        perm.d_mu = gm_mu; perm.d_lam = gm_lam; perm.d_ys = gm_ys; perm.d_mass = gm_mass;
+        perm.pid = SM.pid;
+        perm.n = n;
+        perm.to_sorted = 1;
+        k_permute_grad<<<blocks_for(n, 256), 256, 0, s>>>(perm);
+        CK(cudaGetLastError(), "k_permute_grad");
+        Gp = perm.dst;
+    } else {
+        const EmpmParticles s0 = packed_particles(ab.states, n);
+        CK(cudaMemcpyAsync(s0.x, ckpt->x, sizeof(float4) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(s0.v, ckpt->v, sizeof(float4) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(s0.C, ckpt->C, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(s0.F, ckpt->F, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(mu_w, ckpt_mu, sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(lam_w, ckpt_lam, sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(ys_w, ckpt_yield, sizeof(float) * n, d2d, s), "copy checkpoint");
+    }
+    MaterialArrays Mw = base;
+    Mw.mu = mu_w;
+    Mw.lam = lam_w;
+    Mw.ys = ys_w;
+    const F9Planes Fe = f9_planes(ab.fe, n);
+    const F9Planes gFe = f9_planes(ab.gfe, n);
+
+    // 2. forward over the segment, keeping the state before every substep
+    //    (the state after the last one is not needed)
     for (int k = 0; k < n_steps; ++k) {
         CK(cudaMemcpyAsync(ab.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), d2d, s), "snapshot");
-        const EmpmParticles in = packed_particles(ab.states + (size_t)k * state_floats, n);
-        EmpmParticles out = packed_particles(ab.states + (size_t)(k + 1) * state_floats, n);
-        rc = launch_substep_direct(ctx, &in, &out, &wm, k, s);
+        if (k == n_steps - 1) break;
+        const ParticleArrays Pin = particle_arrays(ab.states + (size_t)k * state_floats, n);
+        const ParticleArrays Pout = particle_arrays(ab.states + (size_t)(k + 1) * state_floats, n);
+        rc = launch_substep_arrays(ctx, Pin, Pout, Mw, Fe, k, sorted, s);
         if (rc) return rc;
     }
 
-    // 2. substeps in reverse: recompute the grid, then the three adjoint kernels
-    const ParticleArrays Gp = particle_arrays(grad, n);
-    const F9Planes Fe = f9_planes(ab.fe, n);
-    const F9Planes gFe = f9_planes(ab.gfe, n);
+    // 3. substeps in reverse: recompute the grid, then the three adjoint kernels
     long long nb = (ctx->nblocks + 3) / 4;
     if (nb > ctx->sm_count * 8) nb = ctx->sm_count * 8;
     for (int k = n_steps - 1; k >= 0; --k) {
         float* snap = ab.mats + (size_t)k * 3 * np;
         CK(cudaMemcpyAsync(ab.work, snap, 3 * np * sizeof(float), d2d, s), "restore snapshot");
-        EmpmParticles sk = packed_particles(ab.states + (size_t)k * state_floats, n);
-        const ParticleArrays Pk = particle_arrays(&sk, n);
-        MaterialArrays Mw;
-        Mw.vol = mat->vol;
-        Mw.mu = mu_w;
-        Mw.lam = lam_w;
-        Mw.ys = ys_w;
-        Mw.sel = mat->selection;
-        Mw.pid = nullptr;
+        const ParticleArrays Pk = particle_arrays(ab.states + (size_t)k * state_floats, n);
         const Launch Lrec = make_launch(ctx, n_steps + k);
         const Launch Lk = make_launch(ctx, k);
-        k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
-        CK(cudaGetLastError(), "k_p2g_direct (adjoint recompute)");
+        timing_mark(ctx, 0, 0, s);
+        if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
+        else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
+        timing_mark(ctx, 0, 1, s);
+        CK(cudaGetLastError(), "P2G (adjoint recompute)");
         GridUpdateArgs gu;
         gu.mom = ctx->grid_mom;
         gu.vel = ctx->grid_vel;
         gu.flags = ctx->flags;
         gu.L = Lrec;
+        timing_mark(ctx, 1, 0, s);
         k_grid_update_keep<<<(int)nb, 256, 0, s>>>(gu);
+        timing_mark(ctx, 1, 1, s);
         CK(cudaGetLastError(), "k_grid_update_keep");
         AdjG2PArgs ag;
         ag.P = Pk;
@@ -975,7 +1081,9 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         ag.gacc = ab.gacc;
         ag.gx = ab.gx;
         ag.gFe = gFe;
+        timing_mark(ctx, 3, 0, s);
         k_adj_g2p<<<blocks_for(n, 128), 128, 0, s>>>(ag);
+        timing_mark(ctx, 3, 1, s);
         CK(cudaGetLastError(), "k_adj_g2p");
         AdjGridArgs gg;
         gg.mom = ctx->grid_mom;
@@ -983,7 +1091,9 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         gg.gmom = ab.gmom;
         gg.flags = ctx->flags;
         gg.L = Lk;
+        timing_mark(ctx, 4, 0, s);
         k_adj_grid<<<(int)nb, 256, 0, s>>>(gg);
+        timing_mark(ctx, 4, 1, s);
         CK(cudaGetLastError(), "k_adj_grid");
         AdjP2GArgs ap;
         ap.P = Pk;
@@ -996,12 +1106,28 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         ap.gx = ab.gx;
         ap.gFe = gFe;
         ap.G = Gp;
-        ap.g_mu = gmat->mu;
-        ap.g_lam = gmat->lam;
-        ap.g_ys = gmat->yield_stress;
-        ap.g_mass = gmat->mass;
+        ap.g_mu = gm_mu;
+        ap.g_lam = gm_lam;
+        ap.g_ys = gm_ys;
+        ap.g_mass = gm_mass;
+        timing_mark(ctx, 5, 0, s);
         k_adj_p2g<<<blocks_for(n, 128), 128, 0, s>>>(ap);
+        timing_mark(ctx, 5, 1, s);
         CK(cudaGetLastError(), "k_adj_p2g");
+    }
+
+    // 4. outgoing adjoint back to the caller's order
+    if (sorted) {
+        GradPermuteArgs back;
+        back.src = Gp;
+        back.dst = particle_arrays(grad, n);
+        back.s_mu = gm_mu; back.s_lam = gm_lam; back.s_ys = gm_ys; back.s_mass = gm_mass;
+        back.d_mu = gmat->mu; back.d_lam = gmat->lam; back.d_ys = gmat->yield_stress; back.d_mass = gmat->mass;
+        back.pid = perm.pid;
+        back.n = n;
+        back.to_sorted = 0;
+        k_permute_grad<<<blocks_for(n, 256), 256, 0, s>>>(back);
+        CK(cudaGetLastError(), "k_permute_grad");
     }
     return EMPM_OK;
 }

@@ -323,6 +323,13 @@ class MPMWARPDiff(object):
         N.check(self._ctx.L.empm_ctx_kernel_times(self._ctx.ptr, ms, cnt), self._ctx.ptr)
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("stress_p2g", "grid_update", "g2p"))}
 
+    def adjoint_kernel_times(self):
+        """{kernel: (total_ms, launches)} for the adjoint kernels [adj_g2p, adj_grid, adj_p2g]."""
+        ms = (N.ctypes.c_float * 3)()
+        cnt = (N.ctypes.c_int * 3)()
+        N.check(self._ctx.L.empm_ctx_adjoint_kernel_times(self._ctx.ptr, ms, cnt), self._ctx.ptr)
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("adj_g2p", "adj_grid", "adj_p2g"))}
+
     def print_time_profile(self):
         print("MPM Time profile:")
         for key, value in self.time_profile.items():

@@ -33,6 +33,12 @@
  *   empm_pack_particles / empm_unpack_particles
  *                       <- MPMStateStruct.from_torch / continue_from_torch and
  *                          wp.to_torch of particle arrays (mpm_data_structure.py:119-172,257-292)
+ *   empm_adjoint_segment <- the Warp tape replay of the substep kernels' adjoints
+ *                          (MyTape / tape.backward, warp_utils.py:93-142;
+ *                          interface.py:167-251,391-472,579-774,899-986)
+ *   empm_prepare_adjoint <- the adjoints of compute_mu_lam_from_E_nu and of the mass
+ *                          product on the same tape (mpm_utils.py:277-283,
+ *                          mpm_data_structure.py:719-726)
  */
 #ifndef EMPM_B200_H
 #define EMPM_B200_H
@@ -336,6 +342,10 @@ int  empm_debug_stress(const EmpmModelParams* params, const float* F_trial9, flo
  * milliseconds and the number of launches timed. */
 int  empm_ctx_timing(EmpmCtx* ctx, int enable, int max_launches);
 int  empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3);
+/* The same for the three adjoint kernels of empm_adjoint_segment: adjoint
+ * G2P, adjoint grid update, adjoint P2G (the recomputed forward P2G and grid
+ * update of the adjoint are counted with the forward kernels). */
+int  empm_ctx_adjoint_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3);
 
 /* Device pointers of the context's grid buffers: float4 per node in the
  * blocked layout (4x4x4-node blocks of 64 consecutive float4, block (bi,bj,bk)

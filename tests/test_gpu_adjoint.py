@@ -136,6 +136,7 @@ def _gpu(p, dt, T, every, weights):
         st.set_selection(_t(p["sel"], torch.int32))
     sv = MPMWARPDiff()
     sv.initialize(n, n_grid=G, device=DEV)
+    sv.sort_every = p.get("sort_every", 16)
     for m in p.get("modifiers", []):
         if m["kind"] == "impulse":
             sv.add_impulse_on_particles(st, force=m["force"], dt=dt, point=m["point"], size=m["size"],
@@ -227,9 +228,12 @@ def test_single_substep_adjoint_jelly():
     _check_directional(p, 2e-4, 1, 1, seed=11)
 
 
-def test_segment_adjoint_plasticine_yielding():
+@pytest.mark.parametrize("sort_every", [16, 0])
+def test_segment_adjoint_plasticine_yielding(sort_every):
+    """Cell-sorted segments (sort_every > 0) and the caller-order path."""
     # strong initial deformation so that most particles are on the yield surface
     p = _problem(5, n=800, G=16, seed=2, deform=0.25, speed=0.5)
+    p["sort_every"] = sort_every
     tape = _check_directional(p, 2e-4, 6, 4, seed=12)
     assert [c.step for c in tape.ckpts] == [0, 4]
 
