@@ -109,6 +109,8 @@ def lib():
         "empm_batch_create": ([P, P, I, I, ctypes.POINTER(P)], I),
         "empm_batch_set_params": ([P, I, ctypes.POINTER(EmpmModelParams)], I),
         "empm_batch_info": ([P, ctypes.POINTER(I), P, P], I),
+        "empm_batch_reserve": ([P, I, ctypes.c_longlong, I], I),
+        "empm_batch_reconfigure": ([P, P, P, I, P], I),
         "empm_substep_noalloc": ([ctypes.POINTER(EmpmModelParams), ctypes.POINTER(EmpmParticles),
                                   ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterial),
                                   ctypes.POINTER(EmpmStep), I, P], I),

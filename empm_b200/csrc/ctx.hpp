@@ -23,7 +23,8 @@ struct GraphKey {
 // Particle and material buffers of the sorted path (cell order).
 struct SortedBuffers {
     bool   allocated = false;
-    int    n = 0;
+    int    n = 0;                          // particle capacity
+    long long nb = 0;                      // block capacity
     float* part[2] = {nullptr, nullptr};   // x4 | v4 | C f9 | F f9 per buffer (ping-pong per substep)
     float* fe = nullptr;                   // elastic F handed from P2G to G2P (f9)
     float* matf[2] = {nullptr, nullptr};   // vol | mu | lam | ys (ping-pong per sort)
@@ -46,6 +47,8 @@ struct SortedBuffers {
 // Buffers of the reverse-mode path (empm_adjoint_segment), allocated on first use.
 struct AdjointBuffers {
     int     capacity = 0;      // substeps per segment the buffers hold
+    int     cap_n = 0;         // particle capacity of the per-particle buffers
+    long long cap_blocks = 0;  // block capacity of the grid buffers
     float*  states = nullptr;  // capacity + 1 packed particle states (x4 | v4 | C f9 | F f9)
     float*  mats = nullptr;    // capacity snapshots of mu | lam | yield
     float*  work = nullptr;    // mu | lam | yield updated by the recomputed substeps
@@ -68,12 +71,17 @@ struct EmpmCtx {
     std::vector<int> boff;                 // first global 4^3 block of each instance
     int          n_particles = 0;          // total
     long long    nblocks = 0;              // total 4^3 grid blocks
+    // capacities the device buffers are sized for (empm_batch_reserve);
+    // empm_batch_reconfigure re-lays instances within them without allocating
+    int          cap_particles = 0;
+    long long    cap_blocks = 0;
+    int          cap_inst = 0;
     empm::InstanceConsts* d_inst = nullptr;
     unsigned long long params_version = 0;
     // device
     int          device = 0;
     int          sm_count = 148;
-    int          max_tables = 0;           // capacity of the step-table array, in tables of n_inst steps
+    size_t       step_entries = 0;         // capacity of the step-table array, in EmpmStep entries
     float4*      grid_mom = nullptr;       // P2G accumulation (px, py, pz, m), blocked layout; zero between substeps
     float4*      grid_vel = nullptr;       // node velocity after the grid update, blocked layout
     unsigned char* flags = nullptr;        // touched node blocks of the current substep

@@ -164,14 +164,16 @@ static int upload_instances(EmpmCtx* ctx) {
 }
 
 static int ensure_step_capacity(EmpmCtx* ctx, int n_tables) {
-    if (n_tables <= ctx->max_tables) return EMPM_OK;
+    const size_t need = (size_t)n_tables * ctx->n_inst;
+    if (need <= ctx->step_entries) return EMPM_OK;
     if (ctx->d_steps) {
         CK(cudaDeviceSynchronize(), "sync before step-table growth");
         cudaFree(ctx->d_steps);
         ctx->d_steps = nullptr;
+        ctx->step_entries = 0;
     }
-    CK(cudaMalloc(&ctx->d_steps, sizeof(EmpmStep) * (size_t)n_tables * ctx->n_inst), "step table");
-    ctx->max_tables = n_tables;
+    CK(cudaMalloc(&ctx->d_steps, sizeof(EmpmStep) * need), "step table");
+    ctx->step_entries = need;
     ctx->graph_valid = false;
     return EMPM_OK;
 }
@@ -209,6 +211,9 @@ extern "C" int empm_batch_create(const EmpmModelParams* params, const int* n_par
     }
     ctx->n_particles = (int)total;
     ctx->nblocks = blocks;
+    ctx->cap_particles = (int)total;
+    ctx->cap_blocks = blocks;
+    ctx->cap_inst = n_instances;
     const size_t grid_bytes = (size_t)blocks * 64 * sizeof(float4);
     cudaError_t e = cudaGetDevice(&ctx->device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -290,6 +295,105 @@ extern "C" int empm_batch_set_params(EmpmCtx* ctx, int instance, const EmpmModel
     if (memcmp(&ctx->params[instance], params, sizeof(EmpmModelParams)) == 0) return EMPM_OK;
     ctx->params[instance] = *params;
     return upload_instances(ctx);
+}
+
+extern "C" int empm_batch_reserve(EmpmCtx* ctx, int max_particles, long long max_blocks, int max_instances) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    if (max_particles < 0 || max_particles > 0x3fffffff || max_blocks < 0 || max_blocks > (1LL << 25) ||
+        max_instances < 0 || max_instances > 4096)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "reserve sizes out of range (%d particles, %lld blocks, %d instances)",
+                              max_particles, max_blocks, max_instances);
+    const bool grow_p = max_particles > ctx->cap_particles;
+    const bool grow_b = max_blocks > ctx->cap_blocks;
+    const bool grow_i = max_instances > ctx->cap_inst;
+    if (!grow_p && !grow_b && !grow_i) return EMPM_OK;
+    CK(cudaDeviceSynchronize(), "sync before reserve");
+    if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+    ctx->graph_valid = false;
+    if (grow_b) {
+        const size_t grid_bytes = (size_t)max_blocks * 64 * sizeof(float4);
+        cudaFree(ctx->grid_mom);
+        cudaFree(ctx->grid_vel);
+        cudaFree(ctx->flags);
+        ctx->grid_mom = ctx->grid_vel = nullptr;
+        ctx->flags = nullptr;
+        CK(cudaMalloc(&ctx->grid_mom, grid_bytes), "reserve grid");
+        CK(cudaMalloc(&ctx->grid_vel, grid_bytes), "reserve grid");
+        CK(cudaMalloc(&ctx->flags, (size_t)max_blocks), "reserve grid");
+        CK(cudaMemset(ctx->grid_mom, 0, grid_bytes), "reserve grid");
+        CK(cudaMemset(ctx->grid_vel, 0, grid_bytes), "reserve grid");
+        CK(cudaMemset(ctx->flags, 0, (size_t)max_blocks), "reserve grid");
+        ctx->cap_blocks = max_blocks;
+    }
+    if (grow_i) {
+        cudaFree(ctx->d_inst);
+        ctx->d_inst = nullptr;
+        CK(cudaMalloc(&ctx->d_inst, sizeof(InstanceConsts) * (size_t)max_instances), "reserve instance table");
+        ctx->cap_inst = max_instances;
+        int rc = upload_instances(ctx);
+        if (rc) return rc;
+    }
+    if (grow_p) ctx->cap_particles = max_particles;
+    free_sorted(ctx->sb);       // re-allocated at the new capacity on next use
+    free_adjoint(ctx->adj);
+    // step tables for blocks of up to 64 substeps of max_instances instances
+    const size_t entries = (size_t)64 * ctx->cap_inst;
+    if (entries > ctx->step_entries) {
+        cudaFree(ctx->d_steps);
+        ctx->d_steps = nullptr;
+        ctx->step_entries = 0;
+        CK(cudaMalloc(&ctx->d_steps, sizeof(EmpmStep) * entries), "reserve step tables");
+        ctx->step_entries = entries;
+    }
+    CK(cudaDeviceSynchronize(), "reserve");
+    return EMPM_OK;
+}
+
+extern "C" int empm_batch_reconfigure(EmpmCtx* ctx, const EmpmModelParams* params, const int* n_particles,
+                                      int n_instances, void* stream) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    if (!params || !n_particles || n_instances < 1)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "bad reconfigure arguments (n_instances %d)", n_instances);
+    if (n_instances > ctx->cap_inst)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "%d instances exceed the context's capacity of %d", n_instances,
+                              ctx->cap_inst);
+    long long total = 0, blocks = 0;
+    for (int i = 0; i < n_instances; ++i) {
+        int rc = validate_params(ctx, params + i);
+        if (rc) return rc;
+        if (n_particles[i] < 0) return empm_set_error(ctx, EMPM_ERR_INVALID, "instance %d: n_particles < 0", i);
+        total += n_particles[i];
+        const long long nb = grid_nb(params[i].n_grid);
+        blocks += nb * nb * nb;
+    }
+    if (total > ctx->cap_particles || blocks > ctx->cap_blocks)
+        return empm_set_error(ctx, EMPM_ERR_INVALID,
+                              "batch of %lld particles / %lld blocks exceeds the context's capacity (%d / %lld)", total,
+                              blocks, ctx->cap_particles, ctx->cap_blocks);
+    ctx->n_inst = n_instances;
+    ctx->params.assign(params, params + n_instances);
+    ctx->counts.assign(n_particles, n_particles + n_instances);
+    ctx->poff.clear();
+    ctx->boff.clear();
+    int po = 0, bo = 0;
+    for (int i = 0; i < n_instances; ++i) {
+        ctx->poff.push_back(po);
+        ctx->boff.push_back(bo);
+        po += n_particles[i];
+        const int nb = grid_nb(params[i].n_grid);
+        bo += nb * nb * nb;
+    }
+    ctx->n_particles = (int)total;
+    ctx->nblocks = blocks;
+    // stream-ordered upload: kernels of the previous layout still queued on
+    // this stream read the old table
+    std::vector<InstanceConsts> h(n_instances);
+    for (int i = 0; i < n_instances; ++i) h[i] = instance_consts(ctx->params[i], ctx->counts[i], ctx->poff[i], ctx->boff[i]);
+    CK(cudaMemcpyAsync(ctx->d_inst, h.data(), sizeof(InstanceConsts) * h.size(), cudaMemcpyHostToDevice,
+                       (cudaStream_t)stream), "upload instances");
+    ctx->params_version++;
+    ctx->graph_valid = false;
+    return EMPM_OK;
 }
 
 extern "C" int empm_ctx_set_params(EmpmCtx* ctx, const EmpmModelParams* params) {
@@ -438,10 +542,11 @@ static int launch_substep_direct(EmpmCtx* ctx, const EmpmParticles* in, EmpmPart
 
 static int ensure_sorted_buffers(EmpmCtx* ctx) {
     SortedBuffers& sb = ctx->sb;
-    const int n = ctx->n_particles;
-    if (sb.allocated && sb.n == n) return EMPM_OK;
+    if (sb.allocated && sb.n >= ctx->n_particles && sb.nb >= ctx->nblocks) return EMPM_OK;
     free_sorted(sb);
-    const size_t nblocks = (size_t)ctx->nblocks;
+    // sized for the context's capacity, so that re-laid batches reuse them
+    const int n = ctx->cap_particles;
+    const size_t nblocks = (size_t)ctx->cap_blocks;
     sb.max_chunks = (int)((size_t)n / TILE_THREADS + nblocks + 1);
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
@@ -478,6 +583,7 @@ static int ensure_sorted_buffers(EmpmCtx* ctx) {
     }
     sb.allocated = true;
     sb.n = n;
+    sb.nb = (long long)nblocks;
     return EMPM_OK;
 }
 
@@ -886,9 +992,15 @@ static EmpmParticles packed_particles(float* base, int n) {
 
 static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
     AdjointBuffers& ab = ctx->adj;
-    const size_t np = padded4(ctx->n_particles);
+    if (ab.gacc && (ab.cap_n < ctx->n_particles || ab.cap_blocks < ctx->nblocks)) {
+        CK(cudaDeviceSynchronize(), "sync before adjoint buffer growth");
+        free_adjoint(ab);
+    }
+    const size_t np = padded4(ctx->cap_particles);
     if (!ab.gacc) {
-        const size_t grid_bytes = (size_t)ctx->nblocks * 64 * sizeof(float4);
+        const size_t grid_bytes = (size_t)ctx->cap_blocks * 64 * sizeof(float4);
+        ab.cap_n = ctx->cap_particles;
+        ab.cap_blocks = ctx->cap_blocks;
         CK(cudaMalloc(&ab.gacc, grid_bytes), "adjoint grid");
         CK(cudaMalloc(&ab.gmom, grid_bytes), "adjoint grid");
         CK(cudaMemset(ab.gacc, 0, grid_bytes), "adjoint grid");
@@ -900,7 +1012,7 @@ static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
         CK(cudaMalloc(&ab.gmats, 4 * np * sizeof(float)), "adjoint material");
     }
     if (n_steps > ab.capacity) {
-        CK(cudaDeviceSynchronize(), "sync before adjoint buffer growth");
+        if (ab.states) CK(cudaDeviceSynchronize(), "sync before adjoint buffer growth");
         if (ab.states) cudaFree(ab.states);
         if (ab.mats) cudaFree(ab.mats);
         ab.states = nullptr;
@@ -1037,11 +1149,12 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
     const F9Planes Fe = f9_planes(ab.fe, n);
     const F9Planes gFe = f9_planes(ab.gfe, n);
 
-    // 2. forward over the segment, keeping the state before every substep
-    //    (the state after the last one is not needed)
+    // 2. forward over the segment, keeping the state before every substep.
+    //    The last substep runs too, although the state after it is not needed:
+    //    its P2G writes the velocity modifiers into that substep's stored
+    //    velocities, which the recompute below (without modifiers) relies on.
     for (int k = 0; k < n_steps; ++k) {
         CK(cudaMemcpyAsync(ab.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), d2d, s), "snapshot");
-        if (k == n_steps - 1) break;
         const ParticleArrays Pin = particle_arrays(ab.states + (size_t)k * state_floats, n);
         const ParticleArrays Pout = particle_arrays(ab.states + (size_t)(k + 1) * state_floats, n);
         rc = launch_substep_arrays(ctx, Pin, Pout, Mw, Fe, k, sorted, s);

@@ -200,6 +200,25 @@ int  empm_ctx_set_params(EmpmCtx* ctx, const EmpmModelParams* params);
 int  empm_batch_create(const EmpmModelParams* params, const int* n_particles, int n_instances, int max_steps,
                        EmpmCtx** out);
 int  empm_batch_set_params(EmpmCtx* ctx, int instance, const EmpmModelParams* params);
+
+/* Grow the device buffers of a batch context to hold up to max_particles
+ * particles, max_blocks 4^3 grid blocks (sum of ceil(G/4)^3 over the
+ * instances) and max_instances instances. Synchronises the device: call it at
+ * set-up, not while stepping. No counterpart in the reference: it serves the
+ * request loop (empm_b200/serving.py), which keeps one context for a changing
+ * set of requests. */
+int  empm_batch_reserve(EmpmCtx* ctx, int max_particles, long long max_blocks, int max_instances);
+
+/* Re-lay a batch context for a new set of instances within its capacity,
+ * without allocating: instance i takes particles [poff_i, poff_i + n_i) in
+ * order, as in empm_batch_create. The instance table is uploaded on `stream`,
+ * so work of the previous layout already queued there is unaffected; work on
+ * other streams that uses the context must have finished. Particle buffers
+ * are the caller's: it moves the surviving instances' state to the new
+ * offsets. Exceeding the capacity returns EMPM_ERR_INVALID. No counterpart in
+ * the reference (it serves the request loop). */
+int  empm_batch_reconfigure(EmpmCtx* ctx, const EmpmModelParams* params, const int* n_particles,
+                            int n_instances, void* stream);
 /* n_instances and, when non-NULL, the first particle and first grid block of each instance. */
 int  empm_batch_info(EmpmCtx* ctx, int* n_instances, int* particle_offsets, int* block_offsets);
 
