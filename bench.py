@@ -1,18 +1,21 @@
 #!/usr/bin/env python
 """Benchmark of the MLS-MPM substep on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c3|c4|c5] [--impl ours|reference]
 
-Workload (default c2, the large single forward configuration): 500,000
-particles in two seeded boxes, 128^3 grid, plasticine (von Mises + FCR),
-moving box collider, dt=1e-4 x 1000 substeps. One step = one full 1000-substep
-rollout from the initial state (reset by device copies inside the timed region).
-Metric: particle-substeps/s (whole job; replicas on N>1 GPUs, weak scaling).
+Workloads (metric: particle-substeps/s, whole job; replicas on N>1 GPUs, weak scaling):
+  c4 (default)  batched CMA-ES population: 32 plasticine instances, 3.17M
+                particles in total, grids {48,64,96,128}^3, 300 substeps per
+                step in CUDA-graph blocks of 50; reported beside the same 32
+                instances run one at a time through the single-instance path
+  c1, c2        single forward rollouts (20k particles jelly 48^3; 500k
+                particles plasticine 128^3 with a moving box collider)
+  c3            gradient of a 400-substep rollout (checkpointed forward + adjoint)
+  c5            serving stream of mixed rollout / gradient requests
 
 Timed region: W untimed steps, then K steps bracketed by a barrier and
 torch.cuda.synchronize(), CUDA events on the launch stream, max over ranks.
-The working set (two particle states of 60 MB, the 18 MB elastic-F buffer
-and two 34 MB grids) is larger than the 126 MB L2, so no flush is needed.
+Working sets are larger than the 126 MB L2, so no flush is needed.
 
 --impl reference times the reference's algorithm on the host cores instead:
 the reference is Python + NVIDIA Warp, which cannot be installed offline,
@@ -832,12 +835,163 @@ def run_ours_c3(args):
     return 0
 
 
+def run_ours_c5(args):
+    """Serving stream: Poisson arrivals of mixed rollout / gradient requests
+    through the continuous-batching request loop (empm_b200.serving). The
+    value is the forward particle-substeps of the completed requests per
+    second of makespan (first arrival to last result, host monotonic clock,
+    device work drained); latencies are submit -> result on the same clock."""
+    import torch
+
+    world, rank, local = dist_setup(args)
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from empm_b200 import workloads as W
+    from empm_b200.adjoint import CheckpointedRollout
+    from empm_b200.batch import single_instance
+    from empm_b200.serving import MPMServer
+
+    rate, seconds = args.c5_rate, args.c5_seconds
+    arrivals = W.c5_arrivals(seed=5 + rank, rate=rate, seconds=seconds)
+    srv = MPMServer(hbm_budget=int(args.c5_budget_gb * (1 << 30)), device=dev).start()
+    # warm-up: a few small requests of each kind
+    warm = [srv.submit(W.c5_request(g, 20_000, 48, 60, 1000 + i)) for i, g in enumerate([False, True] * args.warmup)]
+    for t in warm:
+        r = t.wait(600)
+        assert r is not None and r.status == "ok", r and r.error
+    srv.stats.update(blocks=0, substeps=0, particle_substeps=0, relayouts=0)
+    clocks = ClockSampler(local)
+    clocks.start()
+    tickets = []
+    h2d = [0]
+
+    def client():
+        t0 = time.monotonic()
+        for (ta, grad, n, G, T, sd) in arrivals:
+            req = W.c5_request(grad, n, G, T, sd)
+            delay = t0 + ta - time.monotonic()
+            if delay > 0:
+                time.sleep(delay)
+            h2d[0] += n * (12 + 12 + 5 * 4) + (n * 12 if grad else 0)
+            tickets.append((srv.submit(req), grad, n, T))
+
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    rows = []
+    for tk, grad, n, T in tickets:
+        r = tk.wait(3600)
+        rows.append((r.status, grad, n, T, r.submitted, r.finished, r.latency_s))
+        tk.req = None
+        tk.result = None
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    stats = dict(srv.stats)
+    srv.stop(timeout=600)
+    ok = [r for r in rows if r[0] == "ok"]
+    t_first = min(r[4] for r in rows)
+    t_last = max(r[5] for r in rows)
+    makespan = t_last - t_first
+    served = sum(r[2] * r[3] for r in ok)
+    value = served / makespan
+    lat = np.array([r[6] for r in ok]) * 1e3
+    lat_f = np.array([r[6] for r in ok if not r[1]]) * 1e3
+    lat_g = np.array([r[6] for r in ok if r[1]]) * 1e3
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None  # noqa: E731
+
+    # plain: a seeded sample of the same requests, one at a time through the
+    # single-instance API (rollout, or checkpointed rollout + adjoint)
+    prng = np.random.default_rng(55)
+    sample = [arrivals[i] for i in prng.choice(len(arrivals), size=min(args.c5_plain, len(arrivals)), replace=False)]
+    plain_ps, plain_ms = 0, 0.0
+    for (_, grad, n, G, T, sd) in sample:
+        req = W.c5_request(grad, n, G, T, sd)
+        solver, md, st = single_instance(req.spec, device=dev)
+        other = st.partial_clone()
+        target = torch.as_tensor(req.target, device=dev) if grad else None
+        init = [a.clone() for a in (st._x4, st._v4, st._C, st._F_trial, md.mu, md.lam, md.yield_stress)]
+        for rep in range(2):   # the first run creates the context, captures graphs and allocates buffers
+            for dst, src in zip((st._x4, st._v4, st._C, st._F_trial, md.mu, md.lam, md.yield_stress), init):
+                dst.copy_(src)
+            solver.time = 0.0
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if grad:
+                tape = CheckpointedRollout(solver, md, st, req.dt, T, checkpoint_every=50)
+                diff = tape.forward().particle_x - target
+                tape.backward(g_x=2.0 * diff / n)
+            else:
+                solver.rollout(md, st, other, req.dt, T)
+            e1.record()
+            torch.cuda.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        plain_ps += n * T
+        del solver, md, st, other, init
+    plain_value = plain_ps / (plain_ms / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(W.c2(n=200_000, T=40), budget_s=10.0, max_substeps=40)
+        cpu["sample"] += " (the serving stream's plasticine material distributions)"
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([makespan, served], dtype=torch.float64, device=dev)
+        mk = t[:1].clone()
+        dist.all_reduce(mk, op=dist.ReduceOp.MAX)
+        sv = t[1:].clone()
+        dist.all_reduce(sv, op=dist.ReduceOp.SUM)
+        value = float(sv.item()) / float(mk.item())
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    n_grad_substeps = sum(r[3] for r in ok if r[1])
+    line = {
+        "metric": "served " + METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": 1,
+        "warmup": args.warmup, "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"serving stream: Poisson {rate:g} req/s x {seconds:g} s, 70% rollouts / 30% rollout "
+                               "+ gradient, particles log-U[10k,1M], grids U{48..160}, substeps U[50,1000], "
+                               "plasticine with per-particle E/nu/yield distributions, dt=1e-4",
+                   "requests": len(rows), "completed": len(ok),
+                   "statuses": {s_: sum(1 for r in rows if r[0] == s_) for s_ in sorted({r[0] for r in rows})},
+                   "gradient_requests": sum(1 for r in ok if r[1]),
+                   "offered_forward_particle_substeps_per_s": sum(a[2] * a[4] for a in arrivals) / seconds,
+                   "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99), "rollout_p50": pct(lat_f, 50),
+                                  "rollout_p99": pct(lat_f, 99), "gradient_p50": pct(lat_g, 50),
+                                  "gradient_p99": pct(lat_g, 99)},
+                   "makespan_s": makespan, "hbm_budget_gb": args.c5_budget_gb,
+                   "engine": {k: stats[k] for k in ("blocks", "substeps", "relayouts")},
+                   "plain_value": plain_value, "served_vs_plain": value / plain_value,
+                   "plain": f"{len(sample)} requests sampled from the stream, one at a time through the "
+                            "single-instance API (rollout with a CUDA graph; gradient: checkpointed rollout + "
+                            "adjoint with 50-substep segments), each timed on its second run (context, graphs "
+                            "and buffers already built), CUDA events, no queueing",
+                   "timing": "host monotonic clock from the first arrival to the last result",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d[0], "d2h_bytes_per_step":
+                sum(r[2] * (24 if not r[1] else 24) for r in ok),
+                "path": "MPMServer.submit with host (numpy) requests -> results on the host"},
+        "gpu_launches": 3 * stats["substeps"] + 8 * n_grad_substeps,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--c5-rate", dest="c5_rate", type=float, default=20.0, help="c5: arrivals per second")
+    ap.add_argument("--c5-seconds", dest="c5_seconds", type=float, default=60.0, help="c5: arrival window")
+    ap.add_argument("--c5-budget-gb", dest="c5_budget_gb", type=float, default=60.0, help="c5: HBM budget")
+    ap.add_argument("--c5-plain", dest="c5_plain", type=int, default=12, help="c5: requests timed one at a time")
     ap.add_argument("--checkpoint-every", dest="checkpoint_every", type=int, default=20,
                     help="c3: substeps between checkpoints of the differentiable rollout")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -856,6 +1010,8 @@ def main():
         return run_reference_c4(args) if args.workload == "c4" else run_reference(args)
     if args.workload == "c3":
         return run_ours_c3(args)
+    if args.workload == "c5":
+        return run_ours_c5(args)
     return run_ours_c4(args) if args.workload == "c4" else run_ours(args)
 
 

@@ -53,6 +53,7 @@ class EmpmModifier(ctypes.Structure):
 class EmpmStep(ctypes.Structure):
     _fields_ = [
         ("time", ctypes.c_float), ("dt", ctypes.c_float), ("n_colliders", ctypes.c_int), ("n_modifiers", ctypes.c_int),
+        ("hold", ctypes.c_int), ("reserved", ctypes.c_int),
         ("colliders", EmpmCollider * EMPM_MAX_COLLIDERS), ("modifiers", EmpmModifier * EMPM_MAX_MODIFIERS),
     ]
 

@@ -123,6 +123,7 @@ __device__ __forceinline__ bool prepare_particle(const ParticleArrays& P, const 
                                                  const StepConsts& c, int p, P2GParticle& q) {
     if (M.sel && __ldg(M.sel + p) != 0) return false;
     const EmpmStep& st = *c.step;
+    if (st.hold) return false;   // held instance: no contribution this substep
     const float4 xm = __ldg(P.x + p);
     const float4 vv = __ldg(P.v + p);
     const V3 x = v3(xm.x, xm.y, xm.z);
@@ -237,6 +238,13 @@ __device__ __forceinline__ void g2p_particle(const ParticleArrays& P, F9Planes F
         __stcs(out.v + p, make_float4(0.f, 0.f, 0.f, 0.f));
         f9_store(out.C, p, m3_zero());
         f9_store(out.F, p, m3_identity());
+        return;
+    }
+    if (c.step->hold) {   // held instance: the state passes through unchanged
+        __stcs(out.x + p, __ldg(P.x + p));
+        __stcs(out.v + p, __ldg(P.v + p));
+        f9_store(out.C, p, f9_load(P.C, p));
+        f9_store(out.F, p, f9_load(P.F, p));
         return;
     }
     const float dt = c.step->dt;

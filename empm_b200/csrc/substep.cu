@@ -70,7 +70,7 @@ inline int blocks_for(long long n, int threads) { return (int)((n + threads - 1)
 
 static_assert(sizeof(EmpmCollider) == 104, "EmpmCollider layout changed: update empm_b200/_native.py");
 static_assert(sizeof(EmpmModifier) == 88, "EmpmModifier layout changed: update empm_b200/_native.py");
-static_assert(sizeof(EmpmStep) == 2384, "EmpmStep layout changed: update empm_b200/_native.py");
+static_assert(sizeof(EmpmStep) == 2392, "EmpmStep layout changed: update empm_b200/_native.py");
 
 }  // namespace
 
@@ -336,8 +336,8 @@ extern "C" int empm_batch_reserve(EmpmCtx* ctx, int max_particles, long long max
     if (grow_p) ctx->cap_particles = max_particles;
     free_sorted(ctx->sb);       // re-allocated at the new capacity on next use
     free_adjoint(ctx->adj);
-    // step tables for blocks of up to 64 substeps of max_instances instances
-    const size_t entries = (size_t)64 * ctx->cap_inst;
+    // step tables for blocks of up to 128 substeps of max_instances instances
+    const size_t entries = (size_t)128 * ctx->cap_inst;
     if (entries > ctx->step_entries) {
         cudaFree(ctx->d_steps);
         ctx->d_steps = nullptr;
@@ -1060,6 +1060,8 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
     if (n_steps < 1 || n_steps > 100000)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
     if (!steps) return empm_set_error(ctx, EMPM_ERR_INVALID, "steps is NULL");
+    for (size_t e = 0; e < (size_t)n_steps * ctx->n_inst; ++e)
+        if (steps[e].hold) return empm_set_error(ctx, EMPM_ERR_UNSUPPORTED, "held substeps cannot be differentiated");
     const int n = ctx->n_particles;
     cudaStream_t s = (cudaStream_t)stream;
     // tables [0, n_steps): as given. [n_steps, 2 n_steps): the same without the

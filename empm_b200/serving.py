@@ -8,17 +8,20 @@ independent simulations at once, with continuous batching:
 * Every admitted request keeps its particle state resident on the device, in
   one arena shared by all requests in their forward phase. Instance i occupies
   particles ``[poff_i, poff_i + n_i)``.
-* Work proceeds in blocks of up to ``block`` substeps. Each block is one
-  batched launch sequence (``empm_rollout`` on a batch context) over every
-  active request, each request on its own grid, dt and boundary conditions.
+* Work proceeds in blocks of ``block`` substeps (fewer when every active
+  request finishes sooner). Each block is one batched launch sequence
+  (``empm_rollout`` on a batch context) over every active request, each
+  request on its own grid, dt and boundary conditions. A request that
+  finishes inside a block is held for the rest of it (the step tables'
+  ``hold`` flag: no P2G contribution, state copied through).
 * At block boundaries, finished requests leave and waiting requests are
   admitted as instance slots, arena particles, grid blocks and HBM budget
   free up. The arena is then re-laid out: surviving state is gathered to the
   new offsets, and the context is reconfigured without allocating
   (``empm_batch_reconfigure``).
-* A block ends early when a request finishes, or when a gradient request
-  reaches a checkpoint boundary (every ``checkpoint_every`` substeps). There its
-  state, mu, lam and yield are copied to its own checkpoint storage.
+* At every block boundary a gradient request's state, mu, lam and yield are
+  copied to its own checkpoint storage, so its adjoint segments are the
+  blocks it took part in (at most ``block`` substeps each).
 * A gradient request whose forward is done moves to the adjoint engine. That
   engine runs ``empm_adjoint_segment`` over the request's checkpoints on a
   second CUDA stream, so its work overlaps the forward blocks of the others.
@@ -163,13 +166,14 @@ class Ticket:
         self._done.set()
 
 
-def checkpoint_bytes(req: Request, every: int) -> int:
-    """Device bytes a gradient request holds outside the arena: its
-    checkpoints (one per `every` substeps plus the initial state) and its
-    final state."""
+def checkpoint_bytes(req: Request, block: int) -> int:
+    """Device bytes a gradient request holds outside the arena: one
+    checkpoint per block boundary it passes (at most T // block + 1, since
+    only its last block can be short), the initial state and its final
+    state."""
     if not req.grad:
         return 0
-    n_ckpt = req.n_substeps // every + 2
+    n_ckpt = req.n_substeps // block + 3
     return n_ckpt * req.spec.n * STATE_BYTES_PER_PARTICLE
 
 
@@ -185,10 +189,10 @@ class Capacity:
 
 def capacity_for_budget(hbm_budget: int, max_instances: int = 64, grid_share: float = 0.25,
                         ckpt_share: float = 0.35, adjoint_particles: int = 1_000_000,
-                        adjoint_grid: int = 160, every: int = 20) -> Capacity:
+                        adjoint_grid: int = 160, every: int = 50) -> Capacity:
     """Split an HBM budget (bytes) between the forward arena, the grids, the
-    checkpoint pool and the adjoint engine (segment states, its own grids and
-    sorted buffers)."""
+    checkpoint pool and the adjoint engine (segment states of up to `every`
+    substeps, its own grids and sorted buffers)."""
     adj_blocks = grid_blocks(adjoint_grid)
     adjoint = adjoint_particles * ((every + 1) * 104 + every * 12 + 2 * 104 + 3 * 36 + 64 +
                                    SORTED_BYTES_PER_PARTICLE) + adj_blocks * 4 * 64 * 16
@@ -216,10 +220,9 @@ class Plan:
 class Scheduler:
     """Admission and block planning (host only)."""
 
-    def __init__(self, cap: Capacity, block: int = 50, checkpoint_every: int = 20):
+    def __init__(self, cap: Capacity, block: int = 50):
         self.cap = cap
         self.block = int(block)
-        self.every = int(checkpoint_every)
         self.pending: Deque[Ticket] = deque()
         self.forward: List[Ticket] = []
         self.backward: List[Ticket] = []      # gradient requests in (or waiting for) the adjoint engine
@@ -232,7 +235,7 @@ class Scheduler:
         if t.blocks > c.blocks:
             return f"grid {t.req.spec.n_grid}^3 exceeds the grid capacity"
         if t.req.grad:
-            if checkpoint_bytes(t.req, self.every) > c.ckpt_bytes:
+            if checkpoint_bytes(t.req, self.block) > c.ckpt_bytes:
                 return "checkpoints exceed the HBM budget"
             if t.n > c.adjoint_particles or t.blocks > c.adjoint_blocks:
                 return "request exceeds the adjoint engine's capacity"
@@ -251,14 +254,9 @@ class Scheduler:
         t.ckpt_bytes = 0
 
     def block_length(self, active: List[Ticket]) -> int:
-        """Substeps of the next block: at most `block`, ending when a request
-        finishes or a gradient request reaches a checkpoint boundary."""
-        L = self.block
-        for t in active:
-            L = min(L, t.req.n_substeps - t.progress)
-            if t.req.grad:
-                L = min(L, self.every - t.progress % self.every)
-        return max(int(L), 1)
+        """Substeps of the next block: `block`, or fewer when every active
+        request finishes sooner. Requests that finish inside it are held."""
+        return max(1, min(self.block, max(t.req.n_substeps - t.progress for t in active)))
 
     def plan(self, now: float) -> Plan:
         p = Plan()
@@ -284,7 +282,7 @@ class Scheduler:
         used_b = sum(t.blocks for t in keep)
         while self.pending:
             t = self.pending[0]
-            cb = checkpoint_bytes(t.req, self.every)
+            cb = checkpoint_bytes(t.req, self.block)
             if (len(keep) + 1 > self.cap.instances or used_p + t.n > self.cap.particles or
                     used_b + t.blocks > self.cap.blocks or self.ckpt_in_use + cb > self.cap.ckpt_bytes):
                 break
@@ -306,7 +304,7 @@ class Scheduler:
 
     def advance(self, p: Plan) -> None:
         for t in p.active:
-            t.progress += p.block
+            t.progress = min(t.progress + p.block, t.req.n_substeps)
 
     def idle(self) -> bool:
         return not self.pending and not self.forward and not self.backward
@@ -319,7 +317,7 @@ class GpuExecutor:
     """Device state of the server: the batch context and its particle arena,
     the per-request checkpoints and the adjoint engine."""
 
-    def __init__(self, cap: Capacity, device="cuda:0", every: int = 20, sort_every: int = 16):
+    def __init__(self, cap: Capacity, device="cuda:0", sort_every: int = 16):
         import torch
 
         from . import _native as N
@@ -327,7 +325,6 @@ class GpuExecutor:
 
         self.torch, self.N, self.DTYPE = torch, N, DTYPE
         self.cap = cap
-        self.every = every
         self.device = torch.device(device)
         dev = self.device
         self.L = N.lib()
@@ -523,14 +520,18 @@ class GpuExecutor:
         N = self.N
         n_inst = len(active)
         sz = ctypes.sizeof(N.EmpmStep)
-        all_static = all(self.tables[t.id][1] for t in active)
-        n_tables = 1 if all_static else L
+        uniform = all(self.tables[t.id][1] and t.req.n_substeps - t.progress >= L for t in active)
+        n_tables = 1 if uniform else L
         table = (N.EmpmStep * (n_tables * n_inst))()
         for i, t in enumerate(active):
             src, static = self.tables[t.id]
+            remaining = t.req.n_substeps - t.progress
             for s in range(n_tables):
-                ctypes.memmove(ctypes.addressof(table) + (s * n_inst + i) * sz,
-                               ctypes.addressof(src) + (0 if static else t.progress + s) * sz, sz)
+                e = s * n_inst + i
+                k = min(t.progress + s, t.req.n_substeps - 1)
+                ctypes.memmove(ctypes.addressof(table) + e * sz, ctypes.addressof(src) + (0 if static else k) * sz, sz)
+                if s >= remaining:
+                    table[e].hold = 1
         a = self.arenas[self.ai]
         c = self.cur
         views = [N.EmpmParticles(a["x4"][k].data_ptr(), a["v4"][k].data_ptr(), a["C"][k].data_ptr(),
@@ -548,7 +549,7 @@ class GpuExecutor:
         already advanced)."""
         a = self.arenas[self.ai]
         for t in active:
-            if t.req.grad and t.progress < t.req.n_substeps and t.progress % self.every == 0:
+            if t.req.grad and t.progress < t.req.n_substeps:
                 self._checkpoint(t, a, self.cur, self.ai, self.offsets[t.id], self.n_total)
 
     # -- results ------------------------------------------------------------------------
@@ -647,12 +648,11 @@ class GpuExecutor:
 class MPMServer:
     """Continuous-batching request loop on one GPU (see the module docstring)."""
 
-    def __init__(self, hbm_budget: int = 40 << 30, device="cuda:0", block: int = 50, checkpoint_every: int = 20,
-                 max_instances: int = 64, capacity: Optional[Capacity] = None, sort_every: int = 16,
-                 max_blocks_in_flight: int = 2):
-        self.cap = capacity or capacity_for_budget(hbm_budget, max_instances=max_instances, every=checkpoint_every)
-        self.sched = Scheduler(self.cap, block=block, checkpoint_every=checkpoint_every)
-        self.exec = GpuExecutor(self.cap, device=device, every=checkpoint_every, sort_every=sort_every)
+    def __init__(self, hbm_budget: int = 40 << 30, device="cuda:0", block: int = 50, max_instances: int = 64,
+                 capacity: Optional[Capacity] = None, sort_every: int = 16, max_blocks_in_flight: int = 2):
+        self.cap = capacity or capacity_for_budget(hbm_budget, max_instances=max_instances, every=block)
+        self.sched = Scheduler(self.cap, block=block)
+        self.exec = GpuExecutor(self.cap, device=device, sort_every=sort_every)
         self.max_in_flight = max_blocks_in_flight
         self._lock = threading.Lock()
         self._wake = threading.Event()
@@ -790,12 +790,13 @@ class MPMServer:
             ev = ex.torch.cuda.Event()
             ev.record(ex.fwd_stream)
             self._inflight.append(ev)
+            advanced = sum(min(plan.block, t.req.n_substeps - t.progress) * t.n for t in plan.active)
             with self._lock:
                 self.sched.advance(plan)
             ex.after_block(plan.active)
             self.stats["blocks"] += 1
             self.stats["substeps"] += plan.block
-            self.stats["particle_substeps"] += plan.block * sum(t.n for t in plan.active)
+            self.stats["particle_substeps"] += advanced          # held substeps excluded
             worked = True
         return worked
 

@@ -178,3 +178,44 @@ def c4(seed: int = 4, n_inst: int = 32, T: int = 300, n_lo: int = 20_000, n_hi: 
             yield_stress=np.full(n, ys, np.float32), n_grid=G, material="plasticine", gravity=(0.0, -9.8, 0.0),
             colliders=_floor_walls(G)))
     return specs, 2e-4, T
+
+
+def c5_arrivals(seed: int = 5, rate: float = 20.0, seconds: float = 60.0):
+    """Arrival schedule of the serving stream: Poisson arrivals at `rate`
+    requests/s for `seconds`; 70 % rollouts, 30 % rollout + gradient;
+    particles log-uniform in [10k, 1M], grids uniform in 48..160, substeps
+    uniform in [50, 1000]. Returns [(t_arrival_s, grad, n, G, T, seed)]."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > seconds:
+            return out
+        grad = bool(rng.uniform() < 0.3)
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
+        G = int(rng.integers(48, 161))
+        T = int(rng.integers(50, 1001))
+        out.append((t, grad, n, G, T, int(rng.integers(1 << 31))))
+
+
+def c5_request(grad: bool, n: int, G: int, T: int, seed: int, dt: float = 1e-4):
+    """One serving request: a plasticine body in a random sub-box (about 8
+    particles per cell, side clipped to [0.15, 0.6]) with the large single
+    rollout's material distributions (E log-U[1e3,1e5], nu U[0.2,0.45], yield
+    U[5e2,5e3] per particle), sticky floor and slip walls. A gradient
+    request's loss is the mean squared distance of the final positions from
+    the initial ones."""
+    from .batch import InstanceSpec
+    from .serving import Request
+
+    rng = np.random.default_rng(seed)
+    side = float(np.clip((n / (8.0 * G ** 3)) ** (1.0 / 3.0), 0.15, 0.6))
+    lo = rng.uniform(0.1, 0.9 - side, 3)
+    x = (lo + side * rng.uniform(0.0, 1.0, (n, 3))).astype(np.float32)
+    spec = InstanceSpec(
+        x=x, v=np.zeros((n, 3), np.float32), vol=np.full(n, np.float32(side ** 3 / n), np.float32),
+        rho=np.full(n, np.float32(1e3), np.float32),
+        E=np.exp(rng.uniform(np.log(1e3), np.log(1e5), n)).astype(np.float32),
+        nu=rng.uniform(0.2, 0.45, n).astype(np.float32), yield_stress=rng.uniform(5e2, 5e3, n).astype(np.float32),
+        n_grid=G, material="plasticine", gravity=(0.0, -9.8, 0.0), colliders=_floor_walls(G))
+    return Request(spec=spec, n_substeps=T, dt=dt, grad=grad, target=x.copy() if grad else None)

@@ -155,6 +155,10 @@ typedef struct {
     float dt;
     int   n_colliders;
     int   n_modifiers;
+    int   hold;            /* 1: this instance does not advance in this substep; its particles
+                              are copied unchanged (a batch member that has finished while the
+                              others continue). Not supported by empm_adjoint_segment. */
+    int   reserved;        /* 0 */
     EmpmCollider colliders[EMPM_MAX_COLLIDERS];
     EmpmModifier modifiers[EMPM_MAX_MODIFIERS];
 } EmpmStep;

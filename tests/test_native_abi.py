@@ -24,7 +24,7 @@ def test_struct_sizes_match_header():
     # the library static_asserts the same numbers
     assert ctypes.sizeof(N.EmpmCollider) == 104
     assert ctypes.sizeof(N.EmpmModifier) == 88
-    assert ctypes.sizeof(N.EmpmStep) == 2384
+    assert ctypes.sizeof(N.EmpmStep) == 2392
 
 
 def test_ctx_create_rejects_bad_params_without_gpu():

@@ -52,8 +52,8 @@ def test_no_overtaking_and_instance_slots():
     assert list(s.pending) == [c]
 
 
-def test_block_ends_at_completion_and_checkpoints():
-    s = Scheduler(_cap(), block=50, checkpoint_every=20)
+def test_blocks_run_full_length_and_finished_requests_are_held():
+    s = Scheduler(_cap(), block=50)
     a, _ = _submit(s, _req(T=30))
     b, _ = _submit(s, _req(T=200, grad=True))
     lens = []
@@ -61,19 +61,28 @@ def test_block_ends_at_completion_and_checkpoints():
         p = s.plan(float(step))
         if not p.active:
             break
-        lens.append((p.block, [t.progress for t in p.active]))
+        lens.append((p.block, [t.id for t in p.active]))
         s.advance(p)
-    # the gradient request forces blocks to end at multiples of 20; a finishes at 30
-    assert lens[0][0] == 20
-    assert lens[1][0] == 10 and lens[1][1] == [20, 20]
-    assert all(L <= 20 for L, _ in lens)
-    # no block crosses a checkpoint boundary of the gradient request
-    prog = 0
-    for L, _ in lens:
-        assert prog // 20 == (prog + L - 1) // 20
-        prog += L
-    assert prog == 200
+    # a finishes inside the first block (held for its last 20 substeps) and
+    # leaves at its end; b runs four full blocks, one checkpoint per boundary
+    assert lens[0] == (50, [a.id, b.id])
+    assert [L for L, _ in lens] == [50, 50, 50, 50]
+    assert all(ids == [b.id] for _, ids in lens[1:])
+    assert a.progress == 30 and b.progress == 200
     assert b in s.backward      # finished forward -> adjoint queue
+
+
+def test_short_block_only_when_every_request_finishes_in_it():
+    s = Scheduler(_cap(), block=50)
+    a, _ = _submit(s, _req(T=70))
+    b, _ = _submit(s, _req(T=80))
+    p = s.plan(0.0)
+    assert p.block == 50
+    s.advance(p)
+    p = s.plan(1.0)
+    assert p.block == 30          # max remaining: 20 and 30
+    s.advance(p)
+    assert (a.progress, b.progress) == (70, 80)
 
 
 def test_finished_and_cancelled_requests_leave_with_relayout():
@@ -101,9 +110,9 @@ def test_deadline_expiry():
 
 def test_checkpoint_budget_blocks_admission_and_is_released():
     req = _req(n=1000, T=100, grad=True)
-    need = checkpoint_bytes(req, 20)
-    assert need == (100 // 20 + 2) * 1000 * (104 + 12)
-    s = Scheduler(_cap(ckpt=int(need * 1.5)), block=50, checkpoint_every=20)
+    need = checkpoint_bytes(req, 50)
+    assert need == (100 // 50 + 3) * 1000 * (104 + 12)
+    s = Scheduler(_cap(ckpt=int(need * 1.5)), block=50)
     a, _ = _submit(s, req)
     b, _ = _submit(s, _req(n=1000, T=100, grad=True, seed=1))
     p = s.plan(0.0)
