@@ -4,8 +4,8 @@
 // The reference obtains gradients by replaying Warp's generated adjoints of
 // every launched kernel (tape.backward, interface.py:197,418,720,935). Here
 // the adjoint of one substep is three hand-written kernels that run after the
-// substep's forward grid has been recomputed (k_p2g_direct, then
-// k_grid_update_keep):
+// substep's forward grid has been recomputed (P2G, then the grid update in
+// its variant that keeps the momentum and the block flags):
 //
 //   k_adj_g2p   per particle: adjoint of x', v', C', F' -> scatter of the node
 //               velocity adjoint, and the particle's x and F_elastic adjoints
@@ -40,7 +40,6 @@ EMPM_HD V3 weight_hessian_times(const Stencil& st, int i, int j, int k, V3 b) {
     return v3(hxx * b.x + hxy * b.y + hxz * b.z, hxy * b.x + hyy * b.y + hyz * b.z, hxz * b.x + hyz * b.y + hzz * b.z);
 }
 
-__global__ void __launch_bounds__(256) k_grid_update_keep(const GridUpdateArgs a) { grid_update_blocks<true>(a); }
 
 // ---------------------------------------------------------------------------
 // G2P adjoint

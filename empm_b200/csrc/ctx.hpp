@@ -85,6 +85,7 @@ struct EmpmCtx {
     float4*      grid_mom = nullptr;       // P2G accumulation (px, py, pz, m), blocked layout; zero between substeps
     float4*      grid_vel = nullptr;       // node velocity after the grid update, blocked layout
     unsigned char* flags = nullptr;        // touched node blocks of the current substep
+    int*         active = nullptr;         // [1 + blocks]: number of touched blocks, then their ids
     EmpmStep*    d_steps = nullptr;        // device copy of the step schedules
     unsigned*    d_status = nullptr;       // EMPM_STATUS_* bits
     cudaStream_t own_stream = nullptr;     // capture stream for the graph path

@@ -23,6 +23,15 @@
 #include "grid.cuh"
 #include "substep.cuh"
 
+// Minimum resident CTAs per SM asked of the compiler for the two particle
+// kernels of the sorted path (register caps: 65536 / (threads x CTAs)).
+#ifndef EMPM_P2G_MIN_CTAS
+#define EMPM_P2G_MIN_CTAS 4
+#endif
+#ifndef EMPM_G2P_MIN_CTAS
+#define EMPM_G2P_MIN_CTAS 8
+#endif
+
 namespace empm {
 
 // -------------------------------------------------------------------------
@@ -191,41 +200,107 @@ struct GridUpdateArgs {
     Launch         L;
 };
 
-// kKeep: leave the accumulation and the block flags in place (the adjoint
-// replays the boundary conditions from the accumulated momentum afterwards).
+// One touched 4^3 block (64 nodes, two per lane of the calling warp):
+// normalisation, gravity, damping and boundary conditions.
+template <bool kKeep>
+__device__ __forceinline__ void grid_update_block(const GridUpdateArgs& a, int b, int lane) {
+    const int inst = find_instance_block(a.L, b);
+    const InstanceConsts* I = a.L.inst + inst;
+    const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
+    const float dx = __ldg(&I->dx), damping = __ldg(&I->damping);
+    const V3 g = v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2]));
+    const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int in_block = lane + 32 * h;
+        const long long node = ((long long)b << 6) | in_block;
+        const float4 m = a.mom[node];
+        if (!kKeep) a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+        V3 v = grid_velocity(m, st.dt, g, damping);
+        if (st.n_colliders > 0) {
+            int i, j, k;
+            node_coords(((long long)(b - boff) << 6) | in_block, NB, i, j, k);
+            if (i < G && j < G && k < G) {
+                const long long dense = ((long long)i * G + j) * G + k;
+                apply_colliders(st, i, j, k, G, dx, dense, v);
+            }
+        }
+        a.vel[node] = make_float4(v.x, v.y, v.z, m.w);
+    }
+}
+
+// Grid update over the touched blocks. Each warp reads 32 block flags at a
+// time (coalesced), takes the set ones from a ballot and updates those
+// blocks; each lane clears its own flag afterwards, so no block-wide barrier
+// is needed. kKeep leaves the accumulation and the flags in place (the
+// adjoint replays the boundary conditions from the accumulated momentum).
 template <bool kKeep>
 __device__ __forceinline__ void grid_update_blocks(const GridUpdateArgs& a) {
     const int nblocks = a.L.nblocks;
-    const int group = threadIdx.x >> 6;   // 4 node blocks per iteration
-    const int lane = threadIdx.x & 63;
-    for (int base = blockIdx.x * 4; base < nblocks; base += gridDim.x * 4) {
-        const int b = base + group;
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = warp * 32; base < nblocks; base += nwarps * 32) {
+        const long long b = base + lane;
         const bool active = b < nblocks && a.flags[b] != 0;
-        __syncthreads();   // every group has read its flag before any is cleared
-        if (active) {
-            const int inst = find_instance_block(a.L, b);
-            const InstanceConsts* I = a.L.inst + inst;
-            const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
-            const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
-            const long long node = ((long long)b << 6) | lane;
-            const float4 m = a.mom[node];
-            if (!kKeep) a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
-            V3 v = grid_velocity(m, st.dt, v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2])), __ldg(&I->damping));
-            if (st.n_colliders > 0) {
-                int i, j, k;
-                node_coords(((long long)(b - boff) << 6) | lane, NB, i, j, k);
-                if (i < G && j < G && k < G) {
-                    const long long dense = ((long long)i * G + j) * G + k;
-                    apply_colliders(st, i, j, k, G, __ldg(&I->dx), dense, v);
-                }
-            }
-            a.vel[node] = make_float4(v.x, v.y, v.z, m.w);
-            if (!kKeep && lane == 0) a.flags[b] = 0;
+        unsigned mask = __ballot_sync(0xffffffffu, active);
+        while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1;
+            grid_update_block<kKeep>(a, (int)(base + j), lane);
         }
+        if (!kKeep && active) a.flags[b] = 0;
     }
 }
 
 __global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs a) { grid_update_blocks<false>(a); }
+
+// Touched blocks -> list: active[0] counts them, active[1 + i] are their ids
+// (in no particular order). Clears the flags unless kKeep.
+template <bool kKeep>
+__global__ void __launch_bounds__(256) k_collect_blocks(unsigned char* flags, int nblocks, int* active) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool on = b < nblocks && flags[b] != 0;
+    const unsigned m = __ballot_sync(0xffffffffu, on);
+    if (m == 0u) return;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(active, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (on) {
+        active[1 + base + __popc(m & ((1u << lane) - 1u))] = b;
+        if (!kKeep) flags[b] = 0;
+    }
+}
+
+// Grid update over the listed blocks, one thread per node (grid-stride).
+template <bool kKeep>
+__global__ void __launch_bounds__(256) k_grid_update_list(const GridUpdateArgs a, const int* active) {
+    const long long total = (long long)__ldg(active) * 64;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int b = __ldg(active + 1 + (idx >> 6));
+        const int in_block = (int)(idx & 63);
+        const int inst = find_instance_block(a.L, b);
+        const InstanceConsts* I = a.L.inst + inst;
+        const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
+        const long long node = ((long long)b << 6) | in_block;
+        const float4 m = a.mom[node];
+        if (!kKeep) a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+        V3 v = grid_velocity(m, st.dt, v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2])), __ldg(&I->damping));
+        if (st.n_colliders > 0) {
+            const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
+            int i, j, k;
+            node_coords(((long long)(b - boff) << 6) | in_block, NB, i, j, k);
+            if (i < G && j < G && k < G) {
+                const long long dense = ((long long)i * G + j) * G + k;
+                apply_colliders(st, i, j, k, G, __ldg(&I->dx), dense, v);
+            }
+        }
+        a.vel[node] = make_float4(v.x, v.y, v.z, m.w);
+    }
+}
 
 // -------------------------------------------------------------------------
 // G2P (shared by both paths through the fetch functor)
@@ -281,7 +356,7 @@ struct GlobalFetch {
     }
 };
 
-__global__ void __launch_bounds__(128) k_g2p_direct(ParticleArrays P, F9Planes Fe, MaterialArrays M,
+__global__ void __launch_bounds__(128, EMPM_G2P_MIN_CTAS) k_g2p_direct(ParticleArrays P, F9Planes Fe, MaterialArrays M,
                                                     ParticleArrays out, Launch L, const float4* vel) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= L.n_total) return;
@@ -419,7 +494,7 @@ __global__ void k_unsort(const UnsortArgs a) {
 // segment of the warp (cell-sorted order); for each of the 27 stencil nodes
 // the segment's contributions are summed with shuffles and only the segment
 // head issues the 16-byte reduction to the grid.
-__global__ void __launch_bounds__(256) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
+__global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
                                                      float4* grid, unsigned char* flags) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;

@@ -221,6 +221,7 @@ extern "C" int empm_batch_create(const EmpmModelParams* params, const int* n_par
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_mom, grid_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_vel, grid_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->flags, (size_t)blocks);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->active, sizeof(int) * ((size_t)blocks + 1));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_mom, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_vel, 0, grid_bytes);
@@ -252,7 +253,7 @@ extern "C" int empm_ctx_destroy(EmpmCtx* ctx) {
     for (cudaEvent_t ev : ctx->timing_events) cudaEventDestroy(ev);
     free_sorted(ctx->sb);
     free_adjoint(ctx->adj);
-    void* ptrs[] = {ctx->d_inst, ctx->grid_mom, ctx->grid_vel, ctx->flags, ctx->d_steps, ctx->d_status};
+    void* ptrs[] = {ctx->d_inst, ctx->grid_mom, ctx->grid_vel, ctx->flags, ctx->active, ctx->d_steps, ctx->d_status};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
@@ -315,11 +316,14 @@ extern "C" int empm_batch_reserve(EmpmCtx* ctx, int max_particles, long long max
         cudaFree(ctx->grid_mom);
         cudaFree(ctx->grid_vel);
         cudaFree(ctx->flags);
+        cudaFree(ctx->active);
         ctx->grid_mom = ctx->grid_vel = nullptr;
         ctx->flags = nullptr;
+        ctx->active = nullptr;
         CK(cudaMalloc(&ctx->grid_mom, grid_bytes), "reserve grid");
         CK(cudaMalloc(&ctx->grid_vel, grid_bytes), "reserve grid");
         CK(cudaMalloc(&ctx->flags, (size_t)max_blocks), "reserve grid");
+        CK(cudaMalloc(&ctx->active, sizeof(int) * ((size_t)max_blocks + 1)), "reserve grid");
         CK(cudaMemset(ctx->grid_mom, 0, grid_bytes), "reserve grid");
         CK(cudaMemset(ctx->grid_vel, 0, grid_bytes), "reserve grid");
         CK(cudaMemset(ctx->flags, 0, (size_t)max_blocks), "reserve grid");
@@ -493,19 +497,30 @@ static ParticleArrays particle_arrays(float* base, int n) {
     return a;
 }
 
-static int launch_grid_update(EmpmCtx* ctx, int table, cudaStream_t stream) {
+// Grid update of one substep: the touched blocks are collected into a list
+// (the count is reset first), then every node of the listed blocks is
+// updated by its own thread. kKeep leaves the momentum and the flags in place.
+template <bool kKeep>
+static int launch_grid_update_list(EmpmCtx* ctx, const Launch& L, cudaStream_t stream) {
     GridUpdateArgs g;
     g.mom = ctx->grid_mom;
     g.vel = ctx->grid_vel;
     g.flags = ctx->flags;
-    g.L = make_launch(ctx, table);
-    long long nb = (ctx->nblocks + 3) / 4;
-    if (nb > ctx->sm_count * 8) nb = ctx->sm_count * 8;
-    timing_mark(ctx, 1, 0, stream);
-    k_grid_update_sparse<<<(int)nb, 256, 0, stream>>>(g);
-    timing_mark(ctx, 1, 1, stream);
-    CK(cudaGetLastError(), "k_grid_update_sparse");
+    g.L = L;
+    CK(cudaMemsetAsync(ctx->active, 0, sizeof(int), stream), "reset touched-block count");
+    k_collect_blocks<kKeep><<<blocks_for(ctx->nblocks, 256), 256, 0, stream>>>(ctx->flags, (int)ctx->nblocks,
+                                                                               ctx->active);
+    CK(cudaGetLastError(), "k_collect_blocks");
+    k_grid_update_list<kKeep><<<ctx->sm_count * 8, 256, 0, stream>>>(g, ctx->active);
+    CK(cudaGetLastError(), "k_grid_update_list");
     return EMPM_OK;
+}
+
+static int launch_grid_update(EmpmCtx* ctx, int table, cudaStream_t stream) {
+    timing_mark(ctx, 1, 0, stream);
+    const int rc = launch_grid_update_list<false>(ctx, make_launch(ctx, table), stream);
+    timing_mark(ctx, 1, 1, stream);
+    return rc;
 }
 
 // Direct path: particles in the caller's order, one particle per thread.
@@ -1177,15 +1192,10 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
         timing_mark(ctx, 0, 1, s);
         CK(cudaGetLastError(), "P2G (adjoint recompute)");
-        GridUpdateArgs gu;
-        gu.mom = ctx->grid_mom;
-        gu.vel = ctx->grid_vel;
-        gu.flags = ctx->flags;
-        gu.L = Lrec;
         timing_mark(ctx, 1, 0, s);
-        k_grid_update_keep<<<(int)nb, 256, 0, s>>>(gu);
+        rc = launch_grid_update_list<true>(ctx, Lrec, s);
         timing_mark(ctx, 1, 1, s);
-        CK(cudaGetLastError(), "k_grid_update_keep");
+        if (rc) return rc;
         AdjG2PArgs ag;
         ag.P = Pk;
         ag.Fe = Fe;
