@@ -55,7 +55,7 @@ def load_peaks():
 # the dominant kernel, from one ncu capture of exactly this workload and
 # particle count on a B200: (workload, kernel, particles) -> bytes per launch.
 NCU_DRAM_BYTES = {
-    ("c4", "stress_p2g", 3172508): 403.245824e6 + 104.224512e6,
+    ("c4", "stress_p2g", 3172508): 403.351552e6 + 111.277312e6,
 }
 
 
