@@ -26,6 +26,15 @@
 #include "kernels.cuh"
 #include "spectral.cuh"
 
+// Minimum resident CTAs (of 128 threads) per SM asked of the compiler for the
+// two particle kernels of the adjoint.
+#ifndef EMPM_ADJ_G2P_MIN_CTAS
+#define EMPM_ADJ_G2P_MIN_CTAS 6
+#endif
+#ifndef EMPM_ADJ_P2G_MIN_CTAS
+#define EMPM_ADJ_P2G_MIN_CTAS 3
+#endif
+
 namespace empm {
 
 // second derivative of the quadratic B-spline weight at stencil offset o
@@ -56,34 +65,56 @@ struct AdjG2PArgs {
     F9Planes       gFe;    // out: F_elastic adjoint
 };
 
-__global__ void __launch_bounds__(128) k_adj_g2p(const AdjG2PArgs a) {
+// Lanes whose particles share an instance and base cell (contiguous in cell
+// order) sum their node-velocity adjoints with shuffles; the segment head
+// issues one reduction per node, as k_p2g_warpagg does for the momentum.
+// Every lane of the warp runs the node loop, invalid lanes with zeros.
+__global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const AdjG2PArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.L.n_total) return;
-    if (a.M.sel && __ldg(a.M.sel + p) != 0) {
-        a.gx[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-        f9_store(a.gFe, p, m3_zero());
-        return;
-    }
-    const StepConsts c = consts_of(a.L, find_instance_particle(a.L, p));
+    const int lane = threadIdx.x & 31;
+    const bool live = p < a.L.n_total;
+    const bool valid = live && !(a.M.sel && __ldg(a.M.sel + p) != 0);
+    const int inst = live ? find_instance_particle(a.L, p) : 0;
+    const StepConsts c = consts_of(a.L, inst);
     const float dt = c.step->dt;
-    const float4 xm = __ldg(a.P.x + p);
+    const float4 xm = valid ? __ldg(a.P.x + p) : make_float4(0.f, 0.f, 0.f, 0.f);
     const V3 x = v3(xm.x, xm.y, xm.z);
-    const Stencil st = make_stencil(x, c.inv_dx);
-    const bool in_grid = stencil_in_grid(st, c.G);
-    const GlobalFetch fetch{a.vel, &c};
-    const G2POut o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+    const Stencil st = make_stencil(x, valid ? c.inv_dx : 1.f);
+    const bool in_grid = valid && stencil_in_grid(st, c.G);
+    G2POut o;
+    o.v = v3(0.f, 0.f, 0.f);
+    o.C = m3_zero();
+    o.gradv = m3_zero();
+    if (valid) {
+        const GlobalFetch fetch{a.vel, &c};
+        o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+    }
+    // segments of lanes with the same validity, instance and base cell
+    const int b0 = valid ? st.b[0] : lane, b1 = valid ? st.b[1] : -1, b2 = valid ? st.b[2] : -1;
+    const int u0 = __shfl_up_sync(0xffffffffu, b0, 1), u1 = __shfl_up_sync(0xffffffffu, b1, 1),
+              u2 = __shfl_up_sync(0xffffffffu, b2, 1);
+    const int uv = __shfl_up_sync(0xffffffffu, (int)valid, 1);
+    const int ui = __shfl_up_sync(0xffffffffu, inst, 1);
+    const bool head = lane == 0 || uv != (int)valid || ui != inst || u0 != b0 || u1 != b1 || u2 != b2;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const unsigned above = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
+    const int end = above ? (__ffs(above) - 2) : 31;
+    const int seglen = head ? end - lane + 1 : 1;
+    const int maxlen = __reduce_max_sync(0xffffffffu, seglen);
 
     // x' = clamp(x + dt v'): the clamp passes the adjoint only strictly inside the band
     const float dx = 1.f / c.inv_dx;
     const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
     const V3 y = x + dt * o.v;
-    const float4 gx4 = __ldg(a.Gn.x + p), gv4 = __ldg(a.Gn.v + p);
+    const float4 gx4 = valid ? __ldg(a.Gn.x + p) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 gv4 = valid ? __ldg(a.Gn.v + p) : make_float4(0.f, 0.f, 0.f, 0.f);
     const V3 gxu = v3(y.x > lo && y.x < hi ? gx4.x : 0.f, y.y > lo && y.y < hi ? gx4.y : 0.f,
                       y.z > lo && y.z < hi ? gx4.z : 0.f);
     const V3 gvt = v3(gv4.x, gv4.y, gv4.z) + dt * gxu;
-    const M3 gC = f9_load(a.Gn.C, p), gF = f9_load(a.Gn.F, p);
+    const M3 gC = valid ? f9_load(a.Gn.C, p) : m3_zero();
+    const M3 gF = valid ? f9_load(a.Gn.F, p) : m3_zero();
     // F' = (I + dt grad v) F_e
-    const M3 Fe = f9_load(a.Fe, p);
+    const M3 Fe = valid ? f9_load(a.Fe, p) : m3_zero();
     const M3 gGv = dt * (gF * transpose(Fe));
     const M3 gFe = transpose(m3_identity() + dt * o.gradv) * gF;
 
@@ -102,20 +133,32 @@ __global__ void __launch_bounds__(128) k_adj_g2p(const AdjG2PArgs a) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
-                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= c.G || iy >= c.G || iz >= c.G)) continue;
-                const long long addr = gaddr(c, ix, iy, iz);
-                const float4 g4 = __ldg(a.vel + addr);
-                const V3 vg = v3(g4.x, g4.y, g4.z);
-                const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
-                const float w = wx * wy * wz;
-                const V3 dw = c.inv_dx * v3(st.dw[0][i] * wy * wz, wx * st.dw[1][j] * wz, wx * wy * st.dw[2][k]);
-                const V3 q = q0 + (float)i * Q0 + (float)j * Q1 + (float)k * Q2;
-                const V3 gvg = w * q + gGv * dw;
-                red_add_v4(a.gacc + addr, make_float4(gvg.x, gvg.y, gvg.z, 0.f));
-                gxa = gxa + dot(vg, q) * dw + idx2 * weight_hessian_times(st, i, j, k, gGvT * vg);
+                const bool node_ok = valid && (in_grid || (ix >= 0 && iy >= 0 && iz >= 0 && ix < c.G && iy < c.G &&
+                                                           iz < c.G));
+                const long long addr = node_ok ? gaddr(c, ix, iy, iz) : 0;
+                V3 gvg = v3(0.f, 0.f, 0.f);
+                if (node_ok) {
+                    const float4 g4 = __ldg(a.vel + addr);
+                    const V3 vg = v3(g4.x, g4.y, g4.z);
+                    const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
+                    const float w = wx * wy * wz;
+                    const V3 dw = c.inv_dx * v3(st.dw[0][i] * wy * wz, wx * st.dw[1][j] * wz, wx * wy * st.dw[2][k]);
+                    const V3 q = q0 + (float)i * Q0 + (float)j * Q1 + (float)k * Q2;
+                    gvg = w * q + gGv * dw;
+                    gxa = gxa + dot(vg, q) * dw + idx2 * weight_hessian_times(st, i, j, k, gGvT * vg);
+                }
+                for (int d = 1; d < maxlen; d <<= 1) {
+                    const float tx = __shfl_down_sync(0xffffffffu, gvg.x, d);
+                    const float ty = __shfl_down_sync(0xffffffffu, gvg.y, d);
+                    const float tz = __shfl_down_sync(0xffffffffu, gvg.z, d);
+                    if (lane + d <= end) { gvg.x += tx; gvg.y += ty; gvg.z += tz; }
+                }
+                if (head && node_ok) red_add_v4(a.gacc + addr, make_float4(gvg.x, gvg.y, gvg.z, 0.f));
             }
-    a.gx[p] = make_float4(gxa.x, gxa.y, gxa.z, 0.f);
-    f9_store(a.gFe, p, gFe);
+    if (live) {
+        a.gx[p] = make_float4(gxa.x, gxa.y, gxa.z, 0.f);
+        f9_store(a.gFe, p, gFe);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -196,7 +239,7 @@ struct AdjP2GArgs {
     float*         g_mass; // accumulated over substeps
 };
 
-__global__ void __launch_bounds__(128) k_adj_p2g(const AdjP2GArgs a) {
+__global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const AdjP2GArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.L.n_total) return;
     if (a.M.sel && __ldg(a.M.sel + p) != 0) {
