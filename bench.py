@@ -437,10 +437,20 @@ def run_ours_c4(args):
     specs, dt, T = W.c4(T=args.substeps or 300)
     total = sum(s.n for s in specs)
     batch = BatchedMPM(specs, device=dev)
-    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap"):
-        val = getattr(args, opt)
-        if val is not None:
-            setattr(batch, opt, val)
+    explicit = [o for o in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap") if getattr(args, o) is not None]
+    for opt in explicit:
+        setattr(batch, opt, getattr(args, opt))
+    tuned = None
+    if not explicit and not args.no_autotune:
+        # launch options from the autotuner, on this population, outside the timed region
+        from empm_b200 import autotune as A
+
+        t_tune = time.perf_counter()
+        res = A.tune_batch(batch, dt, substeps=50)
+        tuned = {"options": res["options"], "candidates": len(res["ms"]), "seconds": time.perf_counter() - t_tune,
+                 "best_ms_per_substep": min(res["ms"].values()),
+                 "default_ms_per_substep": res["ms"].get(json.dumps(dict(sort_every=16, p2g_mode=2, tile_cap=1024,
+                                                                         g2p_tile=0), sort_keys=True))}
     init = [t.clone() for t in (batch._x4[0], batch._v4[0], batch._C[0], batch._F[0], batch.mu, batch.lam,
                                 batch.yield_stress)]
 
@@ -607,7 +617,8 @@ def run_ours_c4(args):
                    "l2": "inputs larger than L2 (working set ~1 GB > 126 MB), no flush",
                    "launch": "one CUDA graph per 50-substep block for the whole population",
                    "options": {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode,
-                               "g2p_tile": batch.g2p_tile},
+                               "g2p_tile": batch.g2p_tile, "tile_cap": batch.tile_cap},
+                   "autotune": tuned,
                    "substep_us": substep_ms * 1e3,
                    "substep_hbm_frac": (total * bp["substep"] / (substep_ms / 1e3) / 1e9) / peak,
                    "plain_value": plain_value,
@@ -1005,6 +1016,8 @@ def main():
     ap.add_argument("--p2g-mode", dest="p2g_mode", type=int, default=None, help="0 direct, 1 tile, 2 warp-aggregated")
     ap.add_argument("--g2p-tile", dest="g2p_tile", type=int, default=None)
     ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
+    ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
+                    help="c4: keep the default launch options instead of tuning them on the population")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_c4(args) if args.workload == "c4" else run_reference(args)
