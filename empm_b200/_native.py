@@ -121,6 +121,8 @@ def lib():
         "empm_adjoint_segment": ([P, ctypes.POINTER(EmpmParticles), P, P, P, ctypes.POINTER(EmpmMaterial), P, I,
                                   ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterialGrad), P], I),
         "empm_prepare_adjoint": ([P, P, P, P, P, P, P, P, P, I, P], I),
+        "empm_chamfer": ([P, P, I, I, P, P, I, I, I, P, P, P, P, P], I),
+        "empm_chamfer_backward": ([P, P, I, P, P, I, I, P, P, P, P, P, P, P], I),
         "empm_debug_stress_adjoint": ([ctypes.POINTER(EmpmModelParams), P, P, P, P, ctypes.c_float, P, P, P, P, P,
                                        P, I, P], I),
         "empm_ctx_grid": ([P, ctypes.POINTER(P), ctypes.POINTER(P)], I),

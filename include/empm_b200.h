@@ -339,6 +339,28 @@ int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* 
 int  empm_prepare_adjoint(const float* E, const float* nu, const float* g_mu, const float* g_lam, float* g_E,
                           float* g_nu, const float* vol, const float* g_mass, float* g_density, int n, void* stream);
 
+/* ---- training losses --------------------------------------------------------- */
+
+/* Chamfer distance of many point-set pairs in one launch, the loss of the
+ * reference trainer (pytorch3d chamfer_distance with point_reduction "mean",
+ * phys_sim/engine/trainer_warp_mpm.py:542-561,617-642,745-765). Pair p owns
+ * rows [x_off[p], x_off[p+1]) of x and [y_off[p], y_off[p+1]) of y (device
+ * int arrays of n_pairs + 1 entries; x, y: [rows, 3] floats). Returns, per
+ * pair, sum_xy[p] = sum over x of min_y |x - y|^2 and sum_yx[p] likewise; the
+ * chamfer distance is sum_xy / nx_p + sum_yx / ny_p. nn_x / nn_y receive the
+ * index (row of the other set) of each point's nearest neighbour, for the
+ * gradient. max_nx / max_ny: the largest set size of any pair (launch shape).
+ * Exact brute force over shared-memory tiles. */
+int  empm_chamfer(const float* x, const int* x_off, int nx, int max_nx, const float* y, const int* y_off, int ny,
+                  int max_ny, int n_pairs, float* sum_xy, float* sum_yx, int* nn_x, int* nn_y, void* stream);
+
+/* Gradient in x of sum_p (g_xy[p] * sum_xy[p] + g_yx[p] * sum_yx[p]) for the
+ * neighbours found by empm_chamfer, ADDED to grad_x ([nx, 3]). scratch_pair:
+ * device int array of max(nx, ny) entries. */
+int  empm_chamfer_backward(const float* x, const int* x_off, int nx, const float* y, const int* y_off, int ny,
+                           int n_pairs, const int* nn_x, const int* nn_y, const float* g_xy, const float* g_yx,
+                           float* grad_x, int* scratch_pair, void* stream);
+
 /* ---- diagnostics (used by the parity tests) ------------------------------ */
 
 /* Adjoint of empm_debug_stress for n particles (row-major [N,3,3] like it):
