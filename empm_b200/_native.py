@@ -122,6 +122,7 @@ def lib():
                                   ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterialGrad), P], I),
         "empm_prepare_adjoint": ([P, P, P, P, P, P, P, P, P, I, P], I),
         "empm_chamfer": ([P, P, I, I, P, P, I, I, I, P, P, P, P, P], I),
+        "empm_restart_F": ([P, ctypes.POINTER(EmpmParticles), P, P, P], I),
         "empm_chamfer_backward": ([P, P, I, P, P, I, I, P, P, P, P, P, P, P], I),
         "empm_debug_stress_adjoint": ([ctypes.POINTER(EmpmModelParams), P, P, P, P, ctypes.c_float, P, P, P, P, P,
                                        P, I, P], I),

@@ -1,0 +1,79 @@
+// restart.cuh — the static-pose restart, MPMWARPDiff.restart_and_compute_F_C
+// (phys_sim/diff_simulator/warp_mpm/mpm_solver_diff.py:1214-1262).
+//
+// Particles sit at a static pose x and are given their deformation gradient
+// towards target positions: the displacement target - x is scattered to the
+// grid with weight * mass (set_F_C_p2g, mpm_utils.py:836-866), normalised by
+// the grid mass without gravity or boundary conditions
+// (grid_normalization_and_gravity with dt = 0, :426-438), and gathered back as
+// F_trial = I + sum grid_v (x) dweight (set_F_C_g2p, :869-919). Every x then
+// becomes its target; C is left as it is. Unsimulated particles keep their
+// F_trial but are moved as well, as in the reference.
+#pragma once
+#include "kernels.cuh"
+
+namespace empm {
+
+__global__ void __launch_bounds__(128) k_restart_p2g(ParticleArrays P, const float* __restrict__ target,
+                                                     const int* __restrict__ sel, Launch L, float4* grid,
+                                                     unsigned char* flags) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= L.n_total) return;
+    if (sel && __ldg(sel + p) != 0) return;
+    const StepConsts c = consts_of(L, find_instance_particle(L, p));
+    const float4 xm = __ldg(P.x + p);
+    const Stencil st = make_stencil(v3(xm.x, xm.y, xm.z), c.inv_dx);
+    const V3 disp = v3(__ldg(target + 3 * p) - xm.x, __ldg(target + 3 * p + 1) - xm.y,
+                       __ldg(target + 3 * p + 2) - xm.z);
+    const bool in_grid = stencil_in_grid(st, c.G);
+    if (!in_grid) atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
+                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= c.G || iy >= c.G || iz >= c.G)) continue;
+                const float wm = st.w[0][i] * st.w[1][j] * st.w[2][k] * xm.w;
+                red_add_v4(grid + gaddr(c, ix, iy, iz), make_float4(wm * disp.x, wm * disp.y, wm * disp.z, wm));
+            }
+    mark_stencil_blocks(flags, st, c);
+}
+
+// node displacement = accumulated (mass * displacement) / mass; zero the accumulator
+__global__ void __launch_bounds__(256) k_restart_grid(float4* mom, float4* vel, const int* active) {
+    const long long total = (long long)__ldg(active) * 64;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long node = ((long long)__ldg(active + 1 + (idx >> 6)) << 6) | (idx & 63);
+        const float4 m = mom[node];
+        mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 v = make_float4(0.f, 0.f, 0.f, m.w);
+        if (m.w > 1e-15f) {
+            const float inv = 1.f / m.w;
+            v.x = m.x * inv;
+            v.y = m.y * inv;
+            v.z = m.z * inv;
+        }
+        vel[node] = v;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_restart_g2p(ParticleArrays P, const float* __restrict__ target,
+                                                     const int* __restrict__ sel, Launch L, const float4* vel) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= L.n_total) return;
+    const float4 xm = __ldg(P.x + p);
+    if (!(sel && __ldg(sel + p) != 0)) {
+        const StepConsts c = consts_of(L, find_instance_particle(L, p));
+        const Stencil st = make_stencil(v3(xm.x, xm.y, xm.z), c.inv_dx);
+        const bool in_grid = stencil_in_grid(st, c.G);
+        const GlobalFetch fetch{vel, &c};
+        const G2POut o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+        f9_store(P.F, p, m3_identity() + o.gradv);
+    }
+    P.x[p] = make_float4(__ldg(target + 3 * p), __ldg(target + 3 * p + 1), __ldg(target + 3 * p + 2), xm.w);
+}
+
+}  // namespace empm

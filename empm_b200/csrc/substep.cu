@@ -9,6 +9,7 @@
 #include <cub/device/device_scan.cuh>
 #include "kernels.cuh"
 #include "adjoint.cuh"
+#include "restart.cuh"
 #include "ctx.hpp"
 
 using namespace empm;
@@ -1254,6 +1255,29 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         k_permute_grad<<<blocks_for(n, 256), 256, 0, s>>>(back);
         CK(cudaGetLastError(), "k_permute_grad");
     }
+    return EMPM_OK;
+}
+
+extern "C" int empm_restart_F(EmpmCtx* ctx, EmpmParticles* p, const float* target, const int* selection,
+                              void* stream) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    int rc = check_particles(ctx, p, "particles");
+    if (rc) return rc;
+    if (!target) return empm_set_error(ctx, EMPM_ERR_INVALID, "target is NULL");
+    const int n = ctx->n_particles;
+    if (n == 0) return EMPM_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Launch L = make_launch(ctx, 0);
+    const ParticleArrays P = particle_arrays(p, n);
+    k_restart_p2g<<<blocks_for(n, 128), 128, 0, s>>>(P, target, selection, L, ctx->grid_mom, ctx->flags);
+    CK(cudaGetLastError(), "k_restart_p2g");
+    CK(cudaMemsetAsync(ctx->active, 0, sizeof(int), s), "reset touched-block count");
+    k_collect_blocks<false><<<blocks_for(ctx->nblocks, 256), 256, 0, s>>>(ctx->flags, (int)ctx->nblocks, ctx->active);
+    CK(cudaGetLastError(), "k_collect_blocks");
+    k_restart_grid<<<ctx->sm_count * 8, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active);
+    CK(cudaGetLastError(), "k_restart_grid");
+    k_restart_g2p<<<blocks_for(n, 128), 128, 0, s>>>(P, target, selection, L, ctx->grid_vel);
+    CK(cudaGetLastError(), "k_restart_g2p");
     return EMPM_OK;
 }
 

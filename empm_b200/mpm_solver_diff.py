@@ -561,5 +561,12 @@ class MPMWARPDiff(object):
         self.particle_velocity_modifier_params.append(p)
         self.particle_velocity_modifiers.append(N.MOD_MOVER)
 
-    def restart_and_compute_F_C(self, mpm_model, mpm_state, target_pos, device):
-        raise NotImplementedError("restart_and_compute_F_C (static-pose restart) is not implemented yet")
+    def restart_and_compute_F_C(self, mpm_model, mpm_state, target_pos, device="cuda:0"):
+        """Deformation gradient of a static pose towards target positions, then
+        x = target (mpm_solver_diff.py:1214-1262). target_pos: [N, 3] tensor."""
+        n = mpm_state.n_particles
+        ctx = self._context(mpm_model, n, mpm_state.device)
+        tgt = torch.as_tensor(target_pos, device=mpm_state.device).detach().to(DTYPE).reshape(n, 3).contiguous()
+        with torch.cuda.device(mpm_state.device):
+            N.check(ctx.L.empm_restart_F(ctx.ptr, mpm_state._particles(), tgt.data_ptr(), mpm_state._sel_ptr(),
+                                         _stream_ptr(mpm_state.device)), ctx.ptr)

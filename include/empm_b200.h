@@ -339,6 +339,16 @@ int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* 
 int  empm_prepare_adjoint(const float* E, const float* nu, const float* g_mu, const float* g_lam, float* g_E,
                           float* g_nu, const float* vol, const float* g_mass, float* g_density, int n, void* stream);
 
+/* Static-pose restart: replaces MPMWARPDiff.restart_and_compute_F_C
+ * (mpm_solver_diff.py:1214-1262; kernels set_F_C_p2g / set_F_C_g2p,
+ * mpm_utils.py:836-919). The displacement target - x of every simulated
+ * particle is scattered to its instance's grid with weight * mass, normalised
+ * by the grid mass (no gravity, no boundary conditions), and gathered back as
+ * F_trial = I + sum grid_v (x) dweight. Then every particle's x becomes its
+ * target (float [n, 3]); C is unchanged. selection: NULL or device int [n]
+ * (non-zero: F_trial kept). */
+int  empm_restart_F(EmpmCtx* ctx, EmpmParticles* particles, const float* target, const int* selection, void* stream);
+
 /* ---- training losses --------------------------------------------------------- */
 
 /* Chamfer distance of many point-set pairs in one launch, the loss of the

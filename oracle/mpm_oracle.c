@@ -522,6 +522,66 @@ void or_substep(const OrModel* m, int n, const int* sel, real* mu, real* lam, re
     or_g2p(m, n, sel, x, F, grid_v_out, dt, x1, v1, C1, Ft1);
 }
 
+/* MPMWARPDiff.restart_and_compute_F_C (mpm_solver_diff.py:1214-1262): the
+ * displacement target - x is scattered to the grid with weight * mass
+ * (set_F_C_p2g, mpm_utils.py:836-866), normalised by the grid mass
+ * (grid_normalization_and_gravity with dt = 0, :426-438) and gathered back as
+ * F_trial = I + sum grid_v (x) dweight (set_F_C_g2p, :869-919); every x then
+ * becomes its target (set_vec3_to_vec3). C is not touched. Nodes outside the
+ * grid are skipped. grid_m / grid_v: scratch of G^3 / 3 G^3 reals. */
+void or_restart(const OrModel* m, int n, const int* sel, real* x, const real* mass, const real* target, real* Ft,
+                real* grid_m, real* grid_v) {
+    const int G = m->G;
+    const long long g3 = (long long)G * G * G;
+    memset(grid_m, 0, sizeof(real) * g3);
+    memset(grid_v, 0, sizeof(real) * 3 * g3);
+    for (int p = 0; p < n; ++p) {
+        if (sel && sel[p] != 0) continue;
+        int base[3];
+        real fx[3], w[3][3], dw[3][3];
+        or_stencil(x + 3 * p, m->inv_dx, base, fx, w, dw);
+        const real disp[3] = {target[3 * p] - x[3 * p], target[3 * p + 1] - x[3 * p + 1],
+                              target[3 * p + 2] - x[3 * p + 2]};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) {
+                    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
+                    if (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G) continue;
+                    const real weight = w[0][i] * w[1][j] * w[2][k];
+                    const long long node = ((long long)ix * G + iy) * G + iz;
+                    for (int r = 0; r < 3; ++r) grid_v[3 * node + r] += weight * mass[p] * disp[r];
+                    grid_m[node] += weight * mass[p];
+                }
+    }
+    for (long long node = 0; node < g3; ++node) {
+        if (grid_m[node] > 1e-15) {
+            for (int r = 0; r < 3; ++r) grid_v[3 * node + r] = grid_v[3 * node + r] / grid_m[node];
+        }
+    }
+    for (int p = 0; p < n; ++p) {
+        if (sel && sel[p] != 0) continue;
+        int base[3];
+        real fx[3], w[3][3], dw[3][3];
+        or_stencil(x + 3 * p, m->inv_dx, base, fx, w, dw);
+        real nF[9];
+        memset(nF, 0, sizeof(nF));
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) {
+                    const int ix = base[0] + i, iy = base[1] + j, iz = base[2] + k;
+                    if (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G) continue;
+                    const real* gv = grid_v + 3 * (((long long)ix * G + iy) * G + iz);
+                    const real dwt[3] = {dw[0][i] * w[1][j] * w[2][k] * m->inv_dx,
+                                         w[0][i] * dw[1][j] * w[2][k] * m->inv_dx,
+                                         w[0][i] * w[1][j] * dw[2][k] * m->inv_dx};
+                    for (int r = 0; r < 3; ++r)
+                        for (int c = 0; c < 3; ++c) nF[3 * r + c] += gv[r] * dwt[c];
+                }
+        for (int r = 0; r < 9; ++r) Ft[9 * p + r] = (r % 4 == 0) + nF[r];
+    }
+    for (int p = 0; p < 3 * n; ++p) x[p] = target[p];
+}
+
 int or_real_size(void) { return (int)sizeof(real); }
 int or_num_threads(void) {
 #ifdef _OPENMP

@@ -89,8 +89,10 @@ class _Lib:
         L.or_g2p.argtypes = [M, ctypes.c_int, P, P, P, P, real, P, P, P, P]
         L.or_svd3.argtypes = [P, P, P, P]
         L.or_mu_lam.argtypes = [ctypes.c_int, P, P, P, P]
+        L.or_restart.argtypes = [M, ctypes.c_int, P, P, P, P, P, P, P]
         L.or_num_threads.restype = ctypes.c_int
-        for f in ("or_substep", "or_stress", "or_p2g", "or_grid_update", "or_g2p", "or_svd3", "or_mu_lam"):
+        for f in ("or_substep", "or_stress", "or_p2g", "or_grid_update", "or_g2p", "or_svd3", "or_mu_lam",
+                  "or_restart"):
             getattr(L, f).restype = None
 
 
@@ -140,6 +142,26 @@ def stress(material: int, F_trial: np.ndarray, mu: np.ndarray, lam: np.ndarray, 
     m.plastic_viscosity, m.alpha = plastic_viscosity, alpha
     L.lib.or_stress(ctypes.byref(m), n, None, _ptr(Ft), _ptr(mu), _ptr(lam), _ptr(ys), R(dt), _ptr(Fe), _ptr(S))
     return Fe, S, mu, lam, ys
+
+
+def restart(G: int, x: np.ndarray, mass: np.ndarray, target: np.ndarray, selection=None, grid_lim: float = 1.0,
+            precision: str = "fp64"):
+    """F_trial and positions after MPMWARPDiff.restart_and_compute_F_C.
+    Returns (F_trial [n, 3, 3], x [n, 3])."""
+    L = lib(precision)
+    R = L.np_real
+    n = x.shape[0]
+    xs = np.ascontiguousarray(x, dtype=R).reshape(n, 3).copy()
+    ms = np.ascontiguousarray(mass, dtype=R).reshape(n)
+    tg = np.ascontiguousarray(target, dtype=R).reshape(n, 3)
+    Ft = np.tile(np.eye(3, dtype=R).reshape(1, 9), (n, 1))
+    m = L.OrModel()
+    m.G, m.grid_lim, m.dx, m.inv_dx = int(G), grid_lim, grid_lim / G, float(G / grid_lim)
+    sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.int32)
+    gm = np.zeros(G ** 3, R)
+    gv = np.zeros(3 * G ** 3, R)
+    L.lib.or_restart(ctypes.byref(m), n, _ptr(sel), _ptr(xs), _ptr(ms), _ptr(tg), _ptr(Ft), _ptr(gm), _ptr(gv))
+    return Ft.reshape(n, 3, 3), xs
 
 
 @dataclass

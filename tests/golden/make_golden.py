@@ -241,6 +241,24 @@ def kernel_g2p(ref, rng):
                         F_out=nxt.particle_F_trial.data.copy())}
 
 
+def kernel_restart(ref, rng):
+    """MPMWARPDiff.restart_and_compute_F_C (mpm_solver_diff.py:1214-1262): F
+    from a displacement field scattered to the grid and gathered back."""
+    wp = ref.wp
+    n, G = 80, 12
+    st, model = make_state(ref, n, G)
+    x = f32(rng.uniform(0.3, 0.7, (n, 3)))
+    target = f32(x + 0.02 * rng.standard_normal((n, 3)))
+    mass = f32(rng.uniform(0.5, 1.5, n) * 1e-4)
+    st.particle_x.data[...] = x
+    st.particle_mass.data[...] = mass
+    solver = ref.solver.MPMWARPDiff()
+    solver.initialize(n, n_grid=G, device="cpu")
+    solver.restart_and_compute_F_C(model, st, wp.from_numpy(target, dtype=wp.vec3), device="cpu")
+    return {"restart": dict(G=G, x=x, target=target, mass=mass, F_out=st.particle_F_trial.data.copy(),
+                            x_out=st.particle_x.data.copy())}
+
+
 # ---------------------------------------------------------------------------
 # rollouts through WarpMPMWrapper (the reference's public API)
 # ---------------------------------------------------------------------------
@@ -343,7 +361,7 @@ def main():
     args = ap.parse_args()
     ref = load_reference(args.reference)
     jobs = dict(kernel_stress=kernel_stress, kernel_p2g=kernel_p2g, kernel_grid=kernel_grid,
-                kernel_g2p=kernel_g2p, rollouts=rollouts)
+                kernel_g2p=kernel_g2p, rollouts=rollouts, kernel_restart=kernel_restart)
     for i, (name, fn) in enumerate(jobs.items()):
         if args.only and name != args.only:
             continue

@@ -156,3 +156,13 @@ def test_oracle_svd_properties():
         assert np.linalg.det(V) == pytest.approx(1.0, abs=1e-12)
         assert s[0] >= s[1] >= abs(s[2]) - 1e-12 * s[0]
         assert np.sign(s[2]) == np.sign(np.linalg.det(A)) or abs(s[2]) < 1e-8 * s[0]
+
+
+def test_restart_matches_reference_kernels():
+    """restart_and_compute_F_C, against the reference's own kernels run under
+    the FP64 Warp stand-in (tests/golden/kernel_restart.npz)."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "kernel_restart.npz"))
+    F, x = O.restart(int(d["restart/G"]), d["restart/x"], d["restart/mass"], d["restart/target"])
+    assert np.abs(F - d["restart/F_out"]).max() <= 1e-10
+    assert np.array_equal(x, d["restart/x_out"])
