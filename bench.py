@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the MLS-MPM substep on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c3|c4|c5] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c3|c4|c5|lbs] [--impl ours|reference]
 
 Workloads (metric: particle-substeps/s, whole job; replicas on N>1 GPUs, weak scaling):
   c4 (default)  batched CMA-ES population: 32 plasticine instances, 3.17M
@@ -12,6 +12,8 @@ Workloads (metric: particle-substeps/s, whole job; replicas on N>1 GPUs, weak sc
                 particles plasticine 128^3 with a moving box collider)
   c3            gradient of a 400-substep rollout (checkpointed forward + adjoint)
   c5            serving stream of mixed rollout / gradient requests
+  lbs           Gaussian motion interpolation (metric gaussian-frames/s): 200k
+                particle bones, 2M Gaussians, one rendered frame per step
 
 Timed region: W untimed steps, then K steps bracketed by a barrier and
 torch.cuda.synchronize(), CUDA events on the launch stream, max over ranks.
@@ -56,6 +58,7 @@ def load_peaks():
 # particle count on a B200: (workload, kernel, particles) -> bytes per launch.
 NCU_DRAM_BYTES = {
     ("c4", "stress_p2g", 3172508): 403.351552e6 + 111.277312e6,
+    ("lbs", "blend", 2000000): 196.818688e6 + 41.4976e6,
 }
 
 
@@ -993,12 +996,223 @@ def run_ours_c5(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# lbs: moving the rendered Gaussians with the particles, one frame per step
+# ---------------------------------------------------------------------------
+LBS_METRIC = "gaussian-frames/s"
+LBS_K = 16
+# algorithmic HBM bytes per Gaussian of the blend kernel: xyz and quat read
+# (12 + 16), 16 int32 bone indices read (64), xyz and quat written (12 + 16);
+# the 64-byte rows of the bone table stay in L2
+LBS_BLEND_BYTES = 12 + 16 + 4 * LBS_K + 12 + 16
+
+
+def lbs_description(n_bones, n_gauss):
+    return (f"Gaussian motion interpolation: {n_bones} particle bones (a 2-degree turn + translation + jitter), "
+            f"{n_gauss} Gaussians, {LBS_K} relations per bone, {LBS_K} bones per Gaussian; one frame per step "
+            "(bone rotation fit + blend, neighbour lists found once before timing)")
+
+
+def lbs_cpu_frame(prev, cur, xyz, quat, relations, widx, sample, threads=None):
+    """Seconds per frame of the NumPy restatement: the bone fit over every
+    bone plus the blend of `sample` Gaussians, scaled to all of them."""
+    from oracle import lbs_oracle as LO
+
+    t0 = time.perf_counter()
+    R, _ = LO.bone_rotations(prev, cur - prev, relations)
+    t1 = time.perf_counter()
+    w = LO.idw_weights(prev, xyz[:sample], widx[:sample])
+    LO.blend_sparse(prev, cur - prev, R[:, 0], xyz[:sample], widx[:sample], w, quat[:sample])
+    t2 = time.perf_counter()
+    return (t1 - t0) + (t2 - t1) * xyz.shape[0] / sample, t1 - t0, t2 - t1
+
+
+def run_ours_lbs(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from empm_b200 import dynamic_utils as du
+    from empm_b200 import workloads as W
+
+    n_bones = args.particles or 200_000
+    n_gauss = args.gaussians or 2_000_000
+    h_prev, h_cur, h_xyz, h_q = W.lbs_frame(n_bones=n_bones, n_gauss=n_gauss)
+    prev, cur = torch.as_tensor(h_prev, device=dev), torch.as_tensor(h_cur, device=dev)
+    xyz, quat = torch.as_tensor(h_xyz, device=dev), torch.as_tensor(h_q, device=dev)
+    mi = du.MotionInterpolator(k_relations=LBS_K, k_weights=LBS_K)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    mi(prev, cur, xyz, quat)   # first frame: both neighbour searches
+    s1.record()
+    torch.cuda.synchronize()
+    setup_ms = s0.elapsed_time(s1)
+
+    def step():
+        return mi(prev, cur, xyz, quat)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * n_gauss * args.steps / (ms / 1e3)
+
+    # per-kernel: the bone stage and the blend, CUDA events on the launch stream
+    reps = max(args.steps, 5)
+    b0, b1, b2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    motions = cur - prev
+    b0.record()
+    for _ in range(reps):
+        mi.bt.fit(prev, motions, mi.relations, du.QUAT_KORNIA)
+    b1.record()
+    for _ in range(reps):
+        du._blend(mi.bt, n_bones, xyz, quat, mi.weights_indices, 4, None)
+    b2.record()
+    torch.cuda.synchronize()
+    bones_ms, blend_ms = b0.elapsed_time(b1) / reps, b1.elapsed_time(b2) / reps
+    peak, peak_kind = load_peaks()
+    achieved = n_gauss * LBS_BLEND_BYTES / (blend_ms / 1e3) / 1e9
+
+    # end to end with host buffers: particle positions and Gaussians in,
+    # moved Gaussians out, every step
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    hp, hc, hx, hq = pin(h_prev), pin(h_cur), pin(h_xyz), pin(h_q)
+    ox = torch.empty_like(hx).pin_memory()
+    oq = torch.empty_like(hq).pin_memory()
+    dp, dc, dx, dq = (torch.empty(a.shape, dtype=torch.float32, device=dev) for a in (hp, hc, hx, hq))
+
+    def e2e_step():
+        for d, h in ((dp, hp), (dc, hc), (dx, hx), (dq, hq)):
+            d.copy_(h, non_blocking=True)
+        nx, nq = mi(dp, dc, dx, dq)
+        ox.copy_(nx, non_blocking=True)
+        oq.copy_(nq, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    q1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1))
+    e2e_value = world * n_gauss * args.steps / (e2e_ms / 1e3)
+    h2d = 2 * n_bones * 12 + n_gauss * (12 + 16)
+    d2h = n_gauss * (12 + 16)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = min(n_gauss, 200_000)
+        rel = mi.relations.long().cpu().numpy()
+        widx = mi.weights_indices.long().cpu().numpy()
+        sec, t_fit, t_blend = lbs_cpu_frame(h_prev, h_cur, h_xyz, h_q, rel, widx, sample)
+        cpu = {"value": n_gauss / sec, "unit": LBS_METRIC, "cores": 1, "kind": "port",
+               "sample": f"NumPy FP64 restatement (oracle/lbs_oracle.py): bone fit of all {n_bones} bones "
+                         f"({t_fit:.2f} s) + blend of {sample} Gaussians ({t_blend:.2f} s), scaled to {n_gauss}"}
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": LBS_METRIC, "value": value, "unit": LBS_METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": lbs_description(n_bones, n_gauss), "bones": n_bones, "gaussians": n_gauss,
+                   "k": LBS_K, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "Gaussian streams larger than L2 (240 MB > 126 MB), no flush; the 64-byte bone rows "
+                         f"({n_bones * 64 / 1e6:.1f} MB) are L2-resident by design",
+                   "setup_ms": setup_ms, "bones_ms": bones_ms, "blend_ms": blend_ms},
+        "roofline": {"bound": "hbm", "kernel": "k_lbs_blend16", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": measured_traffic("lbs", "blend", n_gauss),
+                     "limiter": "L1TEX throughput of the bone-row gathers (ncu: 91 % of peak, 2 sectors per bone)",
+                     "algorithmic_bytes_per_gaussian": LBS_BLEND_BYTES, "launch_ms": blend_ms,
+                     "timing": "CUDA events around repeated launches on the launch stream"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": LBS_METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_lbs(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from empm_b200 import workloads as W
+
+    n_bones = args.particles or 200_000
+    n_gauss = args.gaussians or 2_000_000
+    prev, cur, xyz, q = W.lbs_frame(n_bones=n_bones, n_gauss=n_gauss)
+    from scipy.spatial import cKDTree
+
+    sample = min(n_gauss, 100_000)
+    # neighbour lists (found once, not timed) from a k-d tree
+    tree = cKDTree(prev)
+    rel = tree.query(prev, k=LBS_K + 1)[1][:, 1:]
+    widx = tree.query(xyz[:sample], k=LBS_K)[1]
+    times = []
+    for i in range(args.warmup + args.steps):
+        sec, _, _ = lbs_cpu_frame(prev, cur, xyz[:sample], q[:sample], rel, widx, sample)
+        if i >= args.warmup:
+            times.append(sec * n_gauss / sample)
+    ms = 1e3 * float(np.mean(times))
+    value = n_gauss / (ms / 1e3)
+    sample_txt = (f"NumPy FP64 restatement of the reference's dynamic_utils path (oracle/lbs_oracle.py): bone fit "
+                  f"of all {n_bones} bones + blend of {sample} Gaussians per step, scaled to {n_gauss}")
+    print(json.dumps({
+        "impl": "reference", "metric": LBS_METRIC, "value": value, "unit": LBS_METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": lbs_description(n_bones, n_gauss), "sample_per_step": sample_txt},
+        "cpu_baseline": {"value": value, "unit": LBS_METRIC, "cores": 1, "kind": "port", "sample": sample_txt},
+        "e2e": {"value": value, "unit": LBS_METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c4", choices=["c1", "c2", "c3", "c4", "c5", "lbs"])
+    ap.add_argument("--gaussians", type=int, default=None, help="lbs: number of Gaussians")
     ap.add_argument("--c5-rate", dest="c5_rate", type=float, default=20.0, help="c5: arrivals per second")
     ap.add_argument("--c5-seconds", dest="c5_seconds", type=float, default=60.0, help="c5: arrival window")
     ap.add_argument("--c5-budget-gb", dest="c5_budget_gb", type=float, default=60.0, help="c5: HBM budget")
@@ -1019,6 +1233,8 @@ def main():
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="c4: keep the default launch options instead of tuning them on the population")
     args = ap.parse_args()
+    if args.workload == "lbs":
+        return run_reference_lbs(args) if args.impl == "reference" else run_ours_lbs(args)
     if args.impl == "reference":
         return run_reference_c4(args) if args.workload == "c4" else run_reference(args)
     if args.workload == "c3":

@@ -122,10 +122,16 @@ def lib():
                                   ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterialGrad), P], I),
         "empm_prepare_adjoint": ([P, P, P, P, P, P, P, P, P, I, P], I),
         "empm_chamfer": ([P, P, I, I, P, P, I, I, I, P, P, P, P, P], I),
-        "empm_restart_F": ([P, ctypes.POINTER(EmpmParticles), P, P, P], I),
+        "empm_restart_F": ([P, ctypes.POINTER(EmpmParticles), P, P, P, P], I),
         "empm_chamfer_backward": ([P, P, I, P, P, I, I, P, P, P, P, P, P, P], I),
         "empm_debug_stress_adjoint": ([ctypes.POINTER(EmpmModelParams), P, P, P, P, ctypes.c_float, P, P, P, P, P,
                                        P, I, P], I),
+        "empm_knn": ([P, I, P, I, I, I, P, I, P, P], I),
+        "empm_idw_weights": ([P, I, P, I, P, I, I, P, P, P], I),
+        "empm_lbs_bones": ([P, P, I, P, I, I, I, P, P, P, P], I),
+        "empm_lbs_blend": ([P, I, P, P, I, P, I, I, P, P, P, P, P, P], I),
+        "empm_lbs_blend_dense": ([P, I, P, P, I, P, P, P, P, P], I),
+        "empm_rotation_to_quat": ([P, I, I, P, P], I),
         "empm_ctx_grid": ([P, ctypes.POINTER(P), ctypes.POINTER(P)], I),
         "empm_ctx_timing": ([P, I, I], I),
         "empm_ctx_set_option": ([P, I, I], I),

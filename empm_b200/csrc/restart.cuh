@@ -8,7 +8,8 @@
 // (grid_normalization_and_gravity with dt = 0, :426-438), and gathered back as
 // F_trial = I + sum grid_v (x) dweight (set_F_C_g2p, :869-919). Every x then
 // becomes its target; C is left as it is. Unsimulated particles keep their
-// F_trial but are moved as well, as in the reference.
+// F_trial but are moved as well, as in the reference. With update_cov_with_F
+// the packed covariances get the same displacement gradient (:918-919).
 #pragma once
 #include "kernels.cuh"
 
@@ -60,8 +61,25 @@ __global__ void __launch_bounds__(256) k_restart_grid(float4* mom, float4* vel, 
     }
 }
 
+// PhysGaussian covariance update (update_cov, mpm_utils.py:306-326):
+// cov += dt (G cov + cov G^T) on the packed upper triangle
+// (c00, c01, c02, c11, c12, c22) of particle p.
+__device__ __forceinline__ void update_cov(float* cov, int p, const M3& G, float dt) {
+    float* c = cov + 6 * (long long)p;
+    M3 S;
+    S.m[0] = c[0]; S.m[1] = c[1]; S.m[2] = c[2];
+    S.m[3] = c[1]; S.m[4] = c[3]; S.m[5] = c[4];
+    S.m[6] = c[2]; S.m[7] = c[4]; S.m[8] = c[5];
+    const M3 N = S + dt * (G * S + S * transpose(G));
+    c[0] = N.m[0]; c[1] = N.m[1]; c[2] = N.m[2];
+    c[3] = N.m[4]; c[4] = N.m[5]; c[5] = N.m[8];
+}
+
+// cov (optional): covariance update with the displacement gradient and
+// dt = 1, as set_F_C_g2p does when update_cov_with_F is set (:918-919)
 __global__ void __launch_bounds__(128) k_restart_g2p(ParticleArrays P, const float* __restrict__ target,
-                                                     const int* __restrict__ sel, Launch L, const float4* vel) {
+                                                     const int* __restrict__ sel, Launch L, const float4* vel,
+                                                     float* cov) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= L.n_total) return;
     const float4 xm = __ldg(P.x + p);
@@ -72,6 +90,7 @@ __global__ void __launch_bounds__(128) k_restart_g2p(ParticleArrays P, const flo
         const GlobalFetch fetch{vel, &c};
         const G2POut o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
         f9_store(P.F, p, m3_identity() + o.gradv);
+        if (cov) update_cov(cov, p, o.gradv, 1.f);
     }
     P.x[p] = make_float4(__ldg(target + 3 * p), __ldg(target + 3 * p + 1), __ldg(target + 3 * p + 2), xm.w);
 }

@@ -1259,7 +1259,7 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
 }
 
 extern "C" int empm_restart_F(EmpmCtx* ctx, EmpmParticles* p, const float* target, const int* selection,
-                              void* stream) {
+                              float* cov, void* stream) {
     if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
     int rc = check_particles(ctx, p, "particles");
     if (rc) return rc;
@@ -1276,7 +1276,7 @@ extern "C" int empm_restart_F(EmpmCtx* ctx, EmpmParticles* p, const float* targe
     CK(cudaGetLastError(), "k_collect_blocks");
     k_restart_grid<<<ctx->sm_count * 8, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active);
     CK(cudaGetLastError(), "k_restart_grid");
-    k_restart_g2p<<<blocks_for(n, 128), 128, 0, s>>>(P, target, selection, L, ctx->grid_vel);
+    k_restart_g2p<<<blocks_for(n, 128), 128, 0, s>>>(P, target, selection, L, ctx->grid_vel, cov);
     CK(cudaGetLastError(), "k_restart_g2p");
     return EMPM_OK;
 }

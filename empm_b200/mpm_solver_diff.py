@@ -563,10 +563,13 @@ class MPMWARPDiff(object):
 
     def restart_and_compute_F_C(self, mpm_model, mpm_state, target_pos, device="cuda:0"):
         """Deformation gradient of a static pose towards target positions, then
-        x = target (mpm_solver_diff.py:1214-1262). target_pos: [N, 3] tensor."""
+        x = target (mpm_solver_diff.py:1214-1262). target_pos: [N, 3] tensor.
+        With mpm_model.update_cov_with_F set, particle_cov gets the PhysGaussian
+        covariance update with the same displacement gradient (mpm_utils.py:918-919)."""
         n = mpm_state.n_particles
         ctx = self._context(mpm_model, n, mpm_state.device)
         tgt = torch.as_tensor(target_pos, device=mpm_state.device).detach().to(DTYPE).reshape(n, 3).contiguous()
         with torch.cuda.device(mpm_state.device):
-            N.check(ctx.L.empm_restart_F(ctx.ptr, mpm_state._particles(), tgt.data_ptr(), mpm_state._sel_ptr(),
+            cov = mpm_state.particle_cov.data_ptr() if getattr(mpm_model, "update_cov_with_F", False) else None
+            N.check(ctx.L.empm_restart_F(ctx.ptr, mpm_state._particles(), tgt.data_ptr(), mpm_state._sel_ptr(), cov,
                                          _stream_ptr(mpm_state.device)), ctx.ptr)

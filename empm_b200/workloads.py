@@ -219,3 +219,25 @@ def c5_request(grad: bool, n: int, G: int, T: int, seed: int, dt: float = 1e-4):
         nu=rng.uniform(0.2, 0.45, n).astype(np.float32), yield_stress=rng.uniform(5e2, 5e3, n).astype(np.float32),
         n_grid=G, material="plasticine", gravity=(0.0, -9.8, 0.0), colliders=_floor_walls(G))
     return Request(spec=spec, n_substeps=T, dt=dt, grad=grad, target=x.copy() if grad else None)
+
+
+def lbs_frame(seed: int = 6, n_bones: int = 200_000, n_gauss: int = 2_000_000):
+    """One rendered frame of Gaussian motion interpolation (synthetic): the
+    particles of a 200k-particle body (the differentiable rollout's size, in
+    [0.35, 0.65]^3) turn 2 degrees about (0.3, 1, 0.2) around their centre,
+    translate by (2, -4, 1) mm and jitter by N(0, 0.2 mm); 2M Gaussians with
+    random unit quaternions fill [0.33, 0.67]^3. Returns float32 arrays
+    (prev, cur, xyz, quat)."""
+    rng = np.random.default_rng(seed)
+    prev = rng.uniform(0.35, 0.65, (n_bones, 3))
+    c = prev.mean(0)
+    axis = np.array([0.3, 1.0, 0.2]) / np.linalg.norm([0.3, 1.0, 0.2])
+    ang = np.deg2rad(2.0)
+    K = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    R = np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * K @ K
+    cur = (prev - c) @ R.T + c + np.array([0.002, -0.004, 0.001]) + rng.normal(0, 2e-4, (n_bones, 3))
+    xyz = rng.uniform(0.33, 0.67, (n_gauss, 3))
+    q = rng.normal(size=(n_gauss, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+    return f(prev), f(cur), f(xyz), f(q)

@@ -346,8 +346,12 @@ int  empm_prepare_adjoint(const float* E, const float* nu, const float* g_mu, co
  * by the grid mass (no gravity, no boundary conditions), and gathered back as
  * F_trial = I + sum grid_v (x) dweight. Then every particle's x becomes its
  * target (float [n, 3]); C is unchanged. selection: NULL or device int [n]
- * (non-zero: F_trial kept). */
-int  empm_restart_F(EmpmCtx* ctx, EmpmParticles* particles, const float* target, const int* selection, void* stream);
+ * (non-zero: F_trial kept). cov: NULL, or device float [n, 6] packed
+ * covariances (c00, c01, c02, c11, c12, c22) updated as cov += G cov + cov G^T
+ * with G = F_trial - I, the PhysGaussian update the reference applies here
+ * when update_cov_with_F is set (update_cov, mpm_utils.py:306-326, :918-919). */
+int  empm_restart_F(EmpmCtx* ctx, EmpmParticles* particles, const float* target, const int* selection, float* cov,
+                    void* stream);
 
 /* ---- training losses --------------------------------------------------------- */
 
@@ -370,6 +374,66 @@ int  empm_chamfer(const float* x, const int* x_off, int nx, int max_nx, const fl
 int  empm_chamfer_backward(const float* x, const int* x_off, int nx, const float* y, const int* y_off, int ny,
                            int n_pairs, const int* nn_x, const int* nn_y, const float* g_xy, const float* g_yx,
                            float* grad_x, int* scratch_pair, void* stream);
+
+/* ---- Gaussian motion interpolation (linear blend skinning) ------------------ */
+
+/* Per-frame transfer of the simulated particle motion to the rendered
+ * Gaussians, third_party/gaussian_splatting/dynamic_utils.py. Index arrays
+ * (relations, neighbour indices) are [rows, k] of int64 (idx_bytes 8, what
+ * torch.topk returns) or int32 (idx_bytes 4). Indices outside [0, n_bones)
+ * are not read: the affected outputs become NaN and bit 1 of *status (device
+ * int, or counts[EMPM_LBS_STATUS]) is set; the reference's indexing raises. */
+#define EMPM_KNN_MAX_K     32
+#define EMPM_QUAT_KORNIA   0   /* kornia 0.8.1 rotation_matrix_to_quaternion (dynamic_utils.py:465-475) */
+#define EMPM_QUAT_MAT2QUAT 1   /* mat2quat, dynamic_utils.py:25-64 */
+#define EMPM_LBS_COUNTS    8   /* ints of the counts array of empm_lbs_bones */
+#define EMPM_LBS_STATUS    6   /* counts[EMPM_LBS_STATUS]: status bits of the bone stage */
+#define EMPM_LBS_TABLE_FLOATS 16   /* floats per bone of the bone table */
+
+/* Exact k nearest neighbours (k <= EMPM_KNN_MAX_K): for every query row, the
+ * k rows of points closest to it, nearest first, equal distances in index
+ * order. exclude_self != 0 (queries == points) leaves each point out of its
+ * own list. Replaces get_topk_indices (dynamic_utils.py:248-265: topk of K+1
+ * with the first dropped) and the search of knn_weights_sparse (:295-302).
+ * out_dist (optional): the Euclidean distances. */
+int  empm_knn(const float* queries, int n_queries, const float* points, int n_points, int k, int exclude_self,
+              void* out_idx, int idx_bytes, float* out_dist, void* stream);
+
+/* Inverse-distance weights of the k given bones of every point:
+ * w = 1 / (|x - b| + 1e-6), normalised over the k
+ * (calc_weights_vals_from_indices, dynamic_utils.py:282-292). */
+int  empm_idw_weights(const float* bones, int n_bones, const float* pts, int n, const void* idx, int idx_bytes,
+                      int k, float* weights, int* status, void* stream);
+
+/* Bone stage of interpolate_motions(_speedup) (dynamic_utils.py:315-409):
+ * per bone the rotation fitted to its n_adj neighbours' motion, resolved over
+ * all bones as the reference assigns them, and its unit quaternion in the
+ * given convention. Writes table [n_bones * EMPM_LBS_TABLE_FLOATS] (32-byte
+ * aligned) and uses work [n_bones * 10] floats and counts [EMPM_LBS_COUNTS]
+ * ints (device; counts[0..2] = bones of rank 0, 1, 2-3). */
+int  empm_lbs_bones(const float* bones, const float* motions, int n_bones, const void* relations, int idx_bytes,
+                    int n_adj, int convention, float* table, float* work, int* counts, void* stream);
+
+/* Gaussian stage of interpolate_motions_speedup (dynamic_utils.py:428-483):
+ * xyz_out = sum_k w (R (x - b) + m + b) over the k bones of each Gaussian;
+ * quat_out = normalize(sum_k w q_bone) * quat_in ((w, x, y, z); skipped when
+ * quat_in is NULL). weights NULL: the weights of empm_idw_weights for the
+ * table's bones, computed in the same pass (and written to weights_out when
+ * given), as the reference's per-frame loop recomputes them before the call
+ * (trainer_warp_mpm.py:1644-1655). Outputs may alias the inputs. */
+int  empm_lbs_blend(const float* table, int n_bones, const float* xyz, const float* quat_in, int n, const void* idx,
+                    int idx_bytes, int k, const float* weights, float* weights_out, float* xyz_out, float* quat_out,
+                    int* status, void* stream);
+
+/* Gaussian stage of interpolate_motions (dynamic_utils.py:165-216) with
+ * dense [n, n_bones] weights; weights NULL: inverse distance to every bone,
+ * 1 / max(d, 1e-4) normalised, also written to weights_out when given. */
+int  empm_lbs_blend_dense(const float* table, int n_bones, const float* xyz, const float* quat_in, int n,
+                          const float* weights, float* weights_out, float* xyz_out, float* quat_out, void* stream);
+
+/* Quaternions (w, x, y, z) of n row-major rotation matrices, unnormalised,
+ * in the given convention (mat2quat, dynamic_utils.py:25-64, or kornia's). */
+int  empm_rotation_to_quat(const float* R9, int n, int convention, float* q, void* stream);
 
 /* ---- diagnostics (used by the parity tests) ------------------------------ */
 

@@ -529,8 +529,10 @@ void or_substep(const OrModel* m, int n, const int* sel, real* mu, real* lam, re
  * F_trial = I + sum grid_v (x) dweight (set_F_C_g2p, :869-919); every x then
  * becomes its target (set_vec3_to_vec3). C is not touched. Nodes outside the
  * grid are skipped. grid_m / grid_v: scratch of G^3 / 3 G^3 reals. */
+/* cov (optional, packed c00 c01 c02 c11 c12 c22 per particle): update_cov
+ * with the displacement gradient and dt = 1 (mpm_utils.py:306-326, 918-919). */
 void or_restart(const OrModel* m, int n, const int* sel, real* x, const real* mass, const real* target, real* Ft,
-                real* grid_m, real* grid_v) {
+                real* grid_m, real* grid_v, real* cov) {
     const int G = m->G;
     const long long g3 = (long long)G * G * G;
     memset(grid_m, 0, sizeof(real) * g3);
@@ -578,6 +580,21 @@ void or_restart(const OrModel* m, int n, const int* sel, real* x, const real* ma
                         for (int c = 0; c < 3; ++c) nF[3 * r + c] += gv[r] * dwt[c];
                 }
         for (int r = 0; r < 9; ++r) Ft[9 * p + r] = (r % 4 == 0) + nF[r];
+        if (cov) {
+            real* c = cov + 6 * p;
+            const real S[9] = {c[0], c[1], c[2], c[1], c[3], c[4], c[2], c[4], c[5]};
+            real N[9];
+            for (int r = 0; r < 3; ++r)
+                for (int q = 0; q < 3; ++q) {
+                    real gs = 0, sg = 0;
+                    for (int t = 0; t < 3; ++t) {
+                        gs += nF[3 * r + t] * S[3 * t + q];
+                        sg += S[3 * r + t] * nF[3 * q + t];
+                    }
+                    N[3 * r + q] = S[3 * r + q] + (gs + sg);
+                }
+            c[0] = N[0]; c[1] = N[1]; c[2] = N[2]; c[3] = N[4]; c[4] = N[5]; c[5] = N[8];
+        }
     }
     for (int p = 0; p < 3 * n; ++p) x[p] = target[p];
 }

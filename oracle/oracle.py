@@ -145,9 +145,10 @@ def stress(material: int, F_trial: np.ndarray, mu: np.ndarray, lam: np.ndarray, 
 
 
 def restart(G: int, x: np.ndarray, mass: np.ndarray, target: np.ndarray, selection=None, grid_lim: float = 1.0,
-            precision: str = "fp64"):
+            precision: str = "fp64", cov=None):
     """F_trial and positions after MPMWARPDiff.restart_and_compute_F_C.
-    Returns (F_trial [n, 3, 3], x [n, 3])."""
+    Returns (F_trial [n, 3, 3], x [n, 3]), plus the updated packed covariances
+    [n, 6] when cov is given (update_cov_with_F)."""
     L = lib(precision)
     R = L.np_real
     n = x.shape[0]
@@ -160,7 +161,11 @@ def restart(G: int, x: np.ndarray, mass: np.ndarray, target: np.ndarray, selecti
     sel = None if selection is None else np.ascontiguousarray(selection, dtype=np.int32)
     gm = np.zeros(G ** 3, R)
     gv = np.zeros(3 * G ** 3, R)
-    L.lib.or_restart(ctypes.byref(m), n, _ptr(sel), _ptr(xs), _ptr(ms), _ptr(tg), _ptr(Ft), _ptr(gm), _ptr(gv))
+    cv = None if cov is None else np.ascontiguousarray(cov, dtype=R).reshape(n, 6).copy()
+    L.lib.or_restart(ctypes.byref(m), n, _ptr(sel), _ptr(xs), _ptr(ms), _ptr(tg), _ptr(Ft), _ptr(gm), _ptr(gv),
+                     _ptr(cv))
+    if cv is not None:
+        return Ft.reshape(n, 3, 3), xs, cv
     return Ft.reshape(n, 3, 3), xs
 
 

@@ -75,6 +75,7 @@ def load_reference(ref_root: str):
     ref.utils = importlib.import_module("mpm_utils")
     ref.solver = importlib.import_module("mpm_solver_diff")
     ref.wrapper = importlib.import_module("warp_mpm.warp_mpm_wrapper")
+    ref.root = ref_root
     return ref
 
 
@@ -255,8 +256,23 @@ def kernel_restart(ref, rng):
     solver = ref.solver.MPMWARPDiff()
     solver.initialize(n, n_grid=G, device="cpu")
     solver.restart_and_compute_F_C(model, st, wp.from_numpy(target, dtype=wp.vec3), device="cpu")
-    return {"restart": dict(G=G, x=x, target=target, mass=mass, F_out=st.particle_F_trial.data.copy(),
-                            x_out=st.particle_x.data.copy())}
+    out = {"restart": dict(G=G, x=x, target=target, mass=mass, F_out=st.particle_F_trial.data.copy(),
+                           x_out=st.particle_x.data.copy())}
+    # the same with the PhysGaussian covariance update switched on
+    st, model = make_state(ref, n, G)
+    st.particle_x.data[...] = x
+    st.particle_mass.data[...] = mass
+    A = rng.standard_normal((n, 3, 3)) * 1e-2
+    S = A @ np.transpose(A, (0, 2, 1)) + 1e-4 * np.eye(3)
+    cov = f32(np.stack([S[:, 0, 0], S[:, 0, 1], S[:, 0, 2], S[:, 1, 1], S[:, 1, 2], S[:, 2, 2]], 1).reshape(-1))
+    st.particle_cov.data[...] = cov
+    model.update_cov_with_F = True
+    solver = ref.solver.MPMWARPDiff()
+    solver.initialize(n, n_grid=G, device="cpu")
+    solver.restart_and_compute_F_C(model, st, wp.from_numpy(target, dtype=wp.vec3), device="cpu")
+    out["restart_cov"] = dict(G=G, x=x, target=target, mass=mass, cov=cov, F_out=st.particle_F_trial.data.copy(),
+                              cov_out=st.particle_cov.data.copy())
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -344,6 +360,134 @@ def rollouts(ref, rng):
     return out
 
 
+def load_dynamic_utils(ref_root: str):
+    """third_party/gaussian_splatting/dynamic_utils.py, unmodified. It imports
+    kornia (0.8.1, not installed here) at module level; a stub module stands in
+    whose rotation_matrix_to_quaternion raises, so interpolate_motions_speedup
+    takes its own mat2quat fallback (dynamic_utils.py:474-478)."""
+    kornia = types.ModuleType("kornia")
+    geometry = types.ModuleType("kornia.geometry")
+    conversions = types.ModuleType("kornia.geometry.conversions")
+
+    def rotation_matrix_to_quaternion(*a, **k):
+        raise NotImplementedError("kornia is not installed")
+
+    conversions.rotation_matrix_to_quaternion = rotation_matrix_to_quaternion
+    geometry.conversions = conversions
+    kornia.geometry = geometry
+    sys.modules.update({"kornia": kornia, "kornia.geometry": geometry, "kornia.geometry.conversions": conversions})
+    path = os.path.join(ref_root, "third_party", "gaussian_splatting")
+    sys.path.insert(0, path)
+    try:
+        return importlib.import_module("dynamic_utils")
+    finally:
+        sys.path.remove(path)
+
+
+def lbs(ref, rng):
+    """Gaussian motion interpolation cases (float32 tensors, CPU)."""
+    import torch
+    du = load_dynamic_utils(ref.root)
+    t = lambda a: torch.as_tensor(np.asarray(a, np.float32))
+    out = {}
+
+    def rot_about(axis, ang):
+        axis = np.asarray(axis, np.float64) / np.linalg.norm(axis)
+        K = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+        return np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * K @ K
+
+    def random_quats(n):
+        q = rng.normal(size=(n, 4))
+        return q / np.linalg.norm(q, axis=1, keepdims=True)
+
+    # 1. generic: a blob of bones turning 20 degrees, translating, with noise
+    nb, ng = 600, 3000
+    bones = rng.uniform(0.3, 0.7, size=(nb, 3))
+    c = bones.mean(0)
+    R = rot_about([0.3, 1.0, 0.2], np.deg2rad(20.0))
+    motions = (bones - c) @ R.T + c + np.array([0.01, -0.02, 0.005]) - bones + rng.normal(0, 1e-3, (nb, 3))
+    gauss = rng.uniform(0.28, 0.72, size=(ng, 3))
+    quat = random_quats(ng)
+    bones_t, motions_t, gauss_t, quat_t = t(bones), t(motions), t(gauss), t(quat)
+    relations = du.get_topk_indices(bones_t, K=16)
+    weights, widx = du.knn_weights_sparse(bones_t, gauss_t, K=16)
+    weights2 = du.calc_weights_vals_from_indices(bones_t, gauss_t, widx)
+    xyz, rot, _ = du.interpolate_motions_speedup(bones=bones_t, motions=motions_t, relations=relations, xyz=gauss_t,
+                                                 quat=quat_t, weights=weights2, weights_indices=widx, device="cpu")
+    dense_w = du.knn_weights(bones_t, gauss_t, K=16)
+    xyz_d, rot_d, _ = du.interpolate_motions(bones=bones_t, motions=motions_t, relations=relations, xyz=gauss_t,
+                                             quat=quat_t, weights=dense_w, device="cpu")
+    out["generic"] = dict(bones=bones_t.numpy(), motions=motions_t.numpy(), gauss=gauss_t.numpy(),
+                          quat=quat_t.numpy(), relations=relations.numpy(), knn_weights=weights.numpy(),
+                          knn_idx=widx.numpy(), weights=weights2.numpy(), xyz=xyz.numpy(), rot=rot.numpy(),
+                          xyz_dense=xyz_d.numpy(), rot_dense=rot_d.numpy())
+
+    # 2. dense default weights (inverse distance to every bone)
+    nb2, ng2 = 120, 400
+    b2 = bones[:nb2]
+    m2 = motions[:nb2]
+    g2 = gauss[:ng2]
+    rel2 = du.get_topk_indices(t(b2), K=8)
+    xyz2, rot2, w2 = du.interpolate_motions(bones=t(b2), motions=t(m2), relations=rel2, xyz=t(g2), quat=t(quat[:ng2]),
+                                            device="cpu")
+    out["dense_default"] = dict(bones=t(b2).numpy(), motions=t(m2).numpy(), gauss=t(g2).numpy(),
+                                quat=t(quat[:ng2]).numpy(), relations=rel2.numpy(), xyz=xyz2.numpy(),
+                                rot=rot2.numpy(), weights=w2.numpy())
+
+    # 3-5. rank-deficient bones, with hand-built relations. Line bones sit on
+    #    the x axis at dyadic positions and move onto the y axis, so their F is
+    #    exactly rank 1 (axis e_y).
+    def line_case(n_line, extra):
+        tt = np.arange(n_line) / 64.0
+        line = np.stack([0.25 + tt, np.full(n_line, 0.5), np.full(n_line, 0.5)], 1)
+        line_m = np.stack([-tt, tt, np.zeros(n_line)], 1)
+        bb = np.concatenate([line, extra[0]]) if extra is not None else line
+        mm = np.concatenate([line_m, extra[1]]) if extra is not None else line_m
+        return bb, mm
+
+    gen_b = bones[:40]
+    gen_m = motions[:40]
+    # 3. every bone rank 1
+    bb, mm = line_case(24, None)
+    rel = np.array([[j for j in range(24) if j != i][:8] for i in range(24)])
+    case = {"rank1_all": (bb, mm, rel)}
+    # 4. exactly one rank-1 bone among generic ones: its rotation goes to all
+    bb, mm = line_case(10, (gen_b, gen_m))
+    gen_rel = du.get_topk_indices(t(gen_b), K=8).numpy() + 10
+    rel = np.concatenate([np.array([[j for j in range(10) if j != 0][:8]]),
+                          np.tile(gen_rel[:1], (9, 1)), gen_rel])
+    case["rank1_one"] = (bb, mm, rel)
+    # 5. two rank-1 bones: every bone gets the identity
+    rel5 = rel.copy()
+    rel5[1] = np.array([j for j in range(10) if j != 1][:8])
+    case["rank1_two"] = (bb, mm, rel5)
+    # 6. rank-0 bones (all neighbours coincide with the bone): identity everywhere
+    b6 = np.concatenate([gen_b, np.repeat(gen_b[:1], 4, 0)])
+    m6 = np.concatenate([gen_m, np.repeat(gen_m[:1], 4, 0)])
+    rel6 = np.concatenate([du.get_topk_indices(t(gen_b), K=4).numpy(), np.array([[41, 42, 43, 40]] * 4)])
+    rel6[0] = [40, 41, 42, 43]
+    case["rank0_some"] = (b6, m6, rel6)
+    for name, (bb_, mm_, rel_) in case.items():
+        g = rng.uniform(0.2, 0.8, size=(200, 3))
+        q = random_quats(200)
+        w, wi = du.knn_weights_sparse(t(bb_), t(g), K=4)
+        xyz_c, rot_c, _ = du.interpolate_motions_speedup(bones=t(bb_), motions=t(mm_),
+                                                         relations=torch.as_tensor(rel_), xyz=t(g), quat=t(q),
+                                                         weights=w, weights_indices=wi, device="cpu")
+        out[name] = dict(bones=t(bb_).numpy(), motions=t(mm_).numpy(), relations=np.asarray(rel_), gauss=t(g).numpy(),
+                         quat=t(q).numpy(), weights=w.numpy(), knn_idx=wi.numpy(), xyz=xyz_c.numpy(),
+                         rot=rot_c.numpy())
+
+    # 7. the quaternion helpers on random rotations, including near-180-degree ones
+    Rs = np.stack([rot_about(rng.normal(size=3), a) for a in
+                   np.concatenate([rng.uniform(0, np.pi, 200), np.pi - rng.uniform(0, 1e-3, 20)])])
+    Rs_t = t(Rs)
+    q50 = t(random_quats(50))
+    out["quat"] = dict(R=Rs_t.numpy(), mat2quat=du.mat2quat(Rs_t).numpy(), quat_in=q50.numpy(),
+                       quat2mat=du.quat2mat(q50).numpy())
+    return out
+
+
 def save(name, d):
     flat = {}
     for key, val in d.items():
@@ -361,7 +505,7 @@ def main():
     args = ap.parse_args()
     ref = load_reference(args.reference)
     jobs = dict(kernel_stress=kernel_stress, kernel_p2g=kernel_p2g, kernel_grid=kernel_grid,
-                kernel_g2p=kernel_g2p, rollouts=rollouts, kernel_restart=kernel_restart)
+                kernel_g2p=kernel_g2p, rollouts=rollouts, kernel_restart=kernel_restart, lbs=lbs)
     for i, (name, fn) in enumerate(jobs.items()):
         if args.only and name != args.only:
             continue

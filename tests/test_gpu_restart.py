@@ -44,6 +44,40 @@ def test_restart_matches_reference_kernels():
     assert float(st.particle_C.abs().max()) == 0.0
 
 
+def test_restart_covariance_update_matches_reference_kernels():
+    """update_cov_with_F: particle_cov += G cov + cov G^T with the restart's
+    displacement gradient G, as the reference's set_F_C_g2p does."""
+    d = np.load(os.path.join(HERE, "golden", "kernel_restart.npz"))
+    G, x, mass, target = int(d["restart_cov/G"]), d["restart_cov/x"], d["restart_cov/mass"], d["restart_cov/target"]
+    n = x.shape[0]
+    st = MPMStateStruct()
+    st.init(n, device=DEV)
+    st.from_torch(_t(x), _t(np.full(n, 1e-6)), _t(d["restart_cov/cov"]), None, n_grid=G, device=DEV)
+    st.particle_mass = _t(mass)
+    md = MPMModelStruct()
+    md.init(n, device=DEV)
+    md.init_other_params(n_grid=G)
+    md.update_cov_with_F = True
+    sv = MPMWARPDiff()
+    sv.initialize(n, n_grid=G, device=DEV)
+    sv.restart_and_compute_F_C(md, st, _t(target), device=DEV)
+    torch.cuda.synchronize()
+    cov = st.particle_cov.double().cpu().numpy()
+    ref = d["restart_cov/cov_out"]
+    err = np.abs(cov - ref).max()
+    print(f"restart covariance max err {err:.2e}")
+    assert err <= 2e-5 * np.abs(ref).max()
+    # off by default, as in the reference
+    st2 = MPMStateStruct()
+    st2.init(n, device=DEV)
+    st2.from_torch(_t(x), _t(np.full(n, 1e-6)), _t(d["restart_cov/cov"]), None, n_grid=G, device=DEV)
+    st2.particle_mass = _t(mass)
+    md.update_cov_with_F = False
+    sv.restart_and_compute_F_C(md, st2, _t(target), device=DEV)
+    torch.cuda.synchronize()
+    assert np.array_equal(st2.particle_cov.cpu().numpy(), d["restart_cov/cov"].astype(np.float32))
+
+
 def test_simulation_function_with_static_pose():
     rng = np.random.default_rng(9)
     n, G = 2000, 32

@@ -166,3 +166,10 @@ def test_restart_matches_reference_kernels():
     F, x = O.restart(int(d["restart/G"]), d["restart/x"], d["restart/mass"], d["restart/target"])
     assert np.abs(F - d["restart/F_out"]).max() <= 1e-10
     assert np.array_equal(x, d["restart/x_out"])
+    # with update_cov_with_F: the PhysGaussian covariance update
+    n = d["restart_cov/x"].shape[0]
+    F, x, cov = O.restart(int(d["restart_cov/G"]), d["restart_cov/x"], d["restart_cov/mass"], d["restart_cov/target"],
+                          cov=d["restart_cov/cov"])
+    assert np.abs(F - d["restart_cov/F_out"]).max() <= 1e-10
+    assert np.abs(cov.reshape(-1) - d["restart_cov/cov_out"]).max() <= 1e-12
+    assert np.abs(d["restart_cov/cov_out"] - d["restart_cov/cov"]).max() > 1e-4   # the update did something
