@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     o.gradv = m3_zero();
     if (valid) {
         const GlobalFetch fetch{a.vel, &c};
-        o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+        o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
     }
     // segments of lanes with the same validity, instance and base cell
     const int b0 = valid ? st.b[0] : lane, b1 = valid ? st.b[1] : -1, b2 = valid ? st.b[2] : -1;

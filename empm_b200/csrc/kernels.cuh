@@ -107,6 +107,40 @@ __device__ __forceinline__ long long gaddr(const StepConsts& c, int i, int j, in
     return ((long long)(c.boff + block_of(i, j, k, c.NB)) << 6) | ((i & 3) << 4) | ((j & 3) << 2) | (k & 3);
 }
 
+// Addresses of the 27 nodes of a stencil with base node b: gaddr of node
+// b + (i, j, k) is x(i) + y[j] + z[k]. The block index sits above the 6 bits of
+// the local index, so gaddr's OR is a sum of one term per axis; x(i) carries
+// the instance's block offset. Valid only for nodes inside the grid.
+struct StencilAddr {
+    int bx, boff, nb2;   // x[i] is rebuilt from these where it is used (fewer live registers)
+    int y[3], z[3];
+    EMPM_HD long long x(int i) const {
+        const int ix = bx + i;
+        return ((long long)(boff + (ix >> 2) * nb2) << 6) | ((ix & 3) << 4);
+    }
+    EMPM_HD long long at(int i, int j, int k) const { return x(i) + (long long)(y[j] + z[k]); }
+};
+
+EMPM_HD StencilAddr stencil_addr(int boff, int NB, const int b[3]) {
+    StencilAddr a;
+    a.bx = b[0];
+    a.boff = boff;
+    a.nb2 = NB * NB;
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        const int iy = b[1] + o, iz = b[2] + o;
+        a.y[o] = (((iy >> 2) * NB) << 6) | ((iy & 3) << 2);
+        a.z[o] = ((iz >> 2) << 6) | (iz & 3);
+    }
+    return a;
+}
+
+// stencil node (i, j, k) inside the instance's grid (for stencils that are not entirely inside)
+EMPM_HD bool node_in_grid(const int b[3], int i, int j, int k, int G) {
+    const int ix = b[0] + i, iy = b[1] + j, iz = b[2] + k;
+    return ix >= 0 && iy >= 0 && iz >= 0 && ix < G && iy < G && iz < G;
+}
+
 // -------------------------------------------------------------------------
 // particle arrays
 // -------------------------------------------------------------------------
@@ -170,9 +204,8 @@ __device__ __forceinline__ void scatter_global(const P2GParticle& q, const StepC
     if (!in_grid) atomicOr(c.status, EMPM_STATUS_OUT_OF_BAND);
     const P2GPre pre = p2g_pre(q, c.dx, c.inv_dx, c.step->dt);
     p2g_emit(pre, [&](int i, int j, int k, float4 v) {
-        const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
-        if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) return;
-        red_add_v4(grid + gaddr(c, ix, iy, iz), v);
+        if (in_grid || node_in_grid(q.st.b, i, j, k, G))
+            red_add_v4(grid + gaddr(c, q.st.b[0] + i, q.st.b[1] + j, q.st.b[2] + k), v);
     });
     mark_stencil_blocks(flags, q.st, c);
 }
@@ -327,7 +360,7 @@ __device__ __forceinline__ void g2p_particle(const ParticleArrays& P, F9Planes F
     const V3 x = v3(xm.x, xm.y, xm.z);
     const Stencil st = make_stencil(x, c.inv_dx);
     const bool in_grid = stencil_in_grid(st, c.G);
-    const G2POut o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+    const G2POut o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
     const float dx = 1.f / c.inv_dx;
     const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
     V3 nx = x + dt * o.v;
@@ -344,15 +377,25 @@ __device__ __forceinline__ void g2p_particle(const ParticleArrays& P, F9Planes F
     if (flags) atomicOr(c.status, flags);
 }
 
+// Node velocities from the blocked grid. bind() precomputes the stencil's
+// node addresses; nodes outside the grid read as zero.
 struct GlobalFetch {
     const float4* vel;
     const StepConsts* c;
-    __device__ __forceinline__ V3 operator()(const Stencil& st, bool in_grid, int i, int j, int k) const {
-        const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
-        const int G = c->G;
-        if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= G || iy >= G || iz >= G)) return v3(0.f, 0.f, 0.f);
-        const float4 g = __ldg(vel + gaddr(*c, ix, iy, iz));
-        return v3(g.x, g.y, g.z);
+    struct Bound {
+        const float4* vel;
+        StencilAddr sa;
+        const int* b;
+        int G;
+        bool in_grid;
+        __device__ __forceinline__ V3 operator()(int i, int j, int k) const {
+            if (!in_grid && !node_in_grid(b, i, j, k, G)) return v3(0.f, 0.f, 0.f);
+            const float4 g = __ldg(vel + sa.at(i, j, k));
+            return v3(g.x, g.y, g.z);
+        }
+    };
+    __device__ __forceinline__ Bound bind(const Stencil& st, bool in_grid) const {
+        return Bound{vel, stencil_addr(c->boff, c->NB, st.b), st.b, c->G, in_grid};
     }
 };
 
@@ -379,11 +422,11 @@ __global__ void k_sort_keys(const float4* x, Launch L, int* keys, int* ranks, in
     const int G = __ldg(&I->G), NB = __ldg(&I->NB);
     const float inv_dx = __ldg(&I->inv_dx);
     const float4 xm = __ldg(x + p);
-    const float gp[3] = {xm.x * inv_dx, xm.y * inv_dx, xm.z * inv_dx};
+    const float xs[3] = {xm.x, xm.y, xm.z};
     int b[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        int t = (int)(gp[a] - 0.5f);
+        const int t = base_node(xs[a], inv_dx);
         b[a] = t < 0 ? 0 : (t >= G ? G - 1 : t);
     }
     const int blk = __ldg(&I->boff) + block_of(b[0], b[1], b[2], NB);
@@ -529,6 +572,8 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
         pre.B = m3_zero();
         pre.S = m3_zero();
     }
+    // the node address is formed only in the head lanes (keeping precomputed
+    // per-axis address terms live across the 27 nodes measured slower here)
     p2g_emit(pre, [&](int i, int j, int k, float4 v) {
         for (int d = 1; d < maxlen; d <<= 1) {
             const float tx = __shfl_down_sync(0xffffffffu, v.x, d);
@@ -537,11 +582,8 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
             const float tw = __shfl_down_sync(0xffffffffu, v.w, d);
             if (lane + d <= end) { v.x += tx; v.y += ty; v.z += tz; v.w += tw; }
         }
-        if (head && valid) {
-            const int ix = q.st.b[0] + i, iy = q.st.b[1] + j, iz = q.st.b[2] + k;
-            if (in_grid || (ix >= 0 && iy >= 0 && iz >= 0 && ix < G && iy < G && iz < G))
-                red_add_v4(grid + gaddr(c, ix, iy, iz), v);
-        }
+        if (head && valid && (in_grid || node_in_grid(q.st.b, i, j, k, G)))
+            red_add_v4(grid + gaddr(c, q.st.b[0] + i, q.st.b[1] + j, q.st.b[2] + k), v);
     });
     if (head && valid) mark_stencil_blocks(flags, q.st, c);
 }
@@ -630,9 +672,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a
         int base[3] = {0, 0, 0};
         if (active) {
             const float4 xm = __ldg(a.P.x + p);
-            base[0] = (int)(xm.x * c.inv_dx - 0.5f);
-            base[1] = (int)(xm.y * c.inv_dx - 0.5f);
-            base[2] = (int)(xm.z * c.inv_dx - 0.5f);
+            base[0] = base_node(xm.x, c.inv_dx);
+            base[1] = base_node(xm.y, c.inv_dx);
+            base[2] = base_node(xm.z, c.inv_dx);
             if (a.M.sel && __ldg(a.M.sel + p) != 0) active = false;
         }
         const TileBox tb = chunk_box(active, base, s_min, s_max);
@@ -692,12 +734,28 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_p2g_tiled(const TiledArgs a
     }
 }
 
+// Node velocities from the chunk's shared-memory tile (the stencil lies in it).
 struct TileFetch {
     const float4* tile;
     int o0, o1, o2, e1, e2;
-    __device__ __forceinline__ V3 operator()(const Stencil& st, bool, int i, int j, int k) const {
-        const float4 g = tile[((st.b[0] + i - o0) * e1 + (st.b[1] + j - o1)) * e2 + (st.b[2] + k - o2)];
-        return v3(g.x, g.y, g.z);
+    struct Bound {
+        const float4* tile;
+        int x[3], y[3], z[3];   // tile index of node (i, j, k) = x[i] + y[j] + z[k]
+        __device__ __forceinline__ V3 operator()(int i, int j, int k) const {
+            const float4 g = tile[x[i] + y[j] + z[k]];
+            return v3(g.x, g.y, g.z);
+        }
+    };
+    __device__ __forceinline__ Bound bind(const Stencil& st, bool) const {
+        Bound b;
+        b.tile = tile;
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            b.x[o] = (st.b[0] + o - o0) * e1 * e2;
+            b.y[o] = (st.b[1] + o - o1) * e2;
+            b.z[o] = st.b[2] + o - o2;
+        }
+        return b;
     }
 };
 
@@ -715,9 +773,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_g2p_tiled(const TiledArgs a
         if (active) {
             if (a.M.sel && __ldg(a.M.sel + p) != 0) stenciled = false;
             const float4 xm = __ldg(a.P.x + p);
-            base[0] = (int)(xm.x * c.inv_dx - 0.5f);
-            base[1] = (int)(xm.y * c.inv_dx - 0.5f);
-            base[2] = (int)(xm.z * c.inv_dx - 0.5f);
+            base[0] = base_node(xm.x, c.inv_dx);
+            base[1] = base_node(xm.y, c.inv_dx);
+            base[2] = base_node(xm.z, c.inv_dx);
         }
         const TileBox tb = chunk_box(stenciled, base, s_min, s_max);
         const bool use_tile = tb.count > 0 && tb.count <= a.tile_cap && tb.o[0] >= 0 && tb.o[1] >= 0 && tb.o[2] >= 0 &&

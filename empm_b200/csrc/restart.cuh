@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(128) k_restart_g2p(ParticleArrays P, const flo
         const Stencil st = make_stencil(v3(xm.x, xm.y, xm.z), c.inv_dx);
         const bool in_grid = stencil_in_grid(st, c.G);
         const GlobalFetch fetch{vel, &c};
-        const G2POut o = g2p_gather(st, c.inv_dx, [&](int i, int j, int k) { return fetch(st, in_grid, i, j, k); });
+        const G2POut o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
         f9_store(P.F, p, m3_identity() + o.gradv);
         if (cov) update_cov(cov, p, o.gradv, 1.f);
     }

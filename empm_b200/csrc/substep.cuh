@@ -12,7 +12,9 @@ namespace empm {
 
 // Quadratic B-spline stencil of one particle (mpm_utils.py:368-383):
 // base = int(x * inv_dx - 0.5) (truncation), fx = x * inv_dx - base,
-// w[axis][offset], dw[axis][offset] = dw/dfx.
+// w[axis][offset], dw[axis][offset] = dw/dfx. The three weights sum to one
+// for any fx, so a base that rounds to the neighbouring node at a half-integer
+// boundary changes the contributions only by O(fx error^2).
 struct Stencil {
     int   b[3];
     float fx[3];
@@ -20,13 +22,23 @@ struct Stencil {
     float dw[3][3];
 };
 
+// Base node of one coordinate: int(x * inv_dx - 0.5), with the product and the
+// subtraction fused into one rounding. Every kernel derives a particle's base
+// node from this function (stencils, cell keys, shared-memory tile boxes),
+// so they agree bit for bit whatever the compiler does with separate
+// multiply-adds.
+EMPM_HD int base_node(float x, float inv_dx) { return (int)fmaf(x, inv_dx, -0.5f); }
+
+// fx = x * inv_dx - base, rounded once.
+EMPM_HD float base_frac(float x, float inv_dx, int b) { return fmaf(x, inv_dx, -(float)b); }
+
 EMPM_HD Stencil make_stencil(V3 x, float inv_dx) {
     Stencil st;
-    const float gp[3] = {x.x * inv_dx, x.y * inv_dx, x.z * inv_dx};
+    const float xs[3] = {x.x, x.y, x.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        st.b[a] = (int)(gp[a] - 0.5f);
-        const float f = gp[a] - (float)st.b[a];
+        st.b[a] = base_node(xs[a], inv_dx);
+        const float f = base_frac(xs[a], inv_dx, st.b[a]);
         st.fx[a] = f;
         const float wa = 1.5f - f, wb = f - 1.f, wc = f - 0.5f;
         st.w[a][0] = (wa * wa) * 0.5f;
