@@ -274,15 +274,15 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
     M3 gSv = m3_zero();             // sum gmv (x) dweight
     float gmass = 0.f;
     V3 gxa = v3(0.f, 0.f, 0.f);
+    const StencilAddr sa = stencil_addr(c.boff, c.NB, st.b);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j)
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
-                if (!in_grid && (ix < 0 || iy < 0 || iz < 0 || ix >= c.G || iy >= c.G || iz >= c.G)) continue;
-                const float4 g4 = __ldg(a.gmom + gaddr(c, ix, iy, iz));
+                if (!in_grid && !node_in_grid(st.b, i, j, k, c.G)) continue;
+                const float4 g4 = __ldg(a.gmom + sa.at(i, j, k));
                 const V3 gmv = v3(g4.x, g4.y, g4.z);
                 const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
                 const float w = wx * wy * wz;

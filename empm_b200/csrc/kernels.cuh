@@ -572,15 +572,24 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
         pre.B = m3_zero();
         pre.S = m3_zero();
     }
-    // the node address is formed only in the head lanes (keeping precomputed
-    // per-axis address terms live across the 27 nodes measured slower here)
+    // The reduction rounds are unrolled: each is skipped by a warp-uniform
+    // branch once 2^r >= maxlen, and the per-lane "partner inside my segment"
+    // tests are formed once instead of per node. The node address is formed
+    // only in the head lanes (keeping precomputed per-axis address terms live
+    // across the 27 nodes measured slower here).
+    const unsigned take = (lane + 1 <= end ? 1u : 0u) | (lane + 2 <= end ? 2u : 0u) | (lane + 4 <= end ? 4u : 0u) |
+                          (lane + 8 <= end ? 8u : 0u) | (lane + 16 <= end ? 16u : 0u);
     p2g_emit(pre, [&](int i, int j, int k, float4 v) {
-        for (int d = 1; d < maxlen; d <<= 1) {
-            const float tx = __shfl_down_sync(0xffffffffu, v.x, d);
-            const float ty = __shfl_down_sync(0xffffffffu, v.y, d);
-            const float tz = __shfl_down_sync(0xffffffffu, v.z, d);
-            const float tw = __shfl_down_sync(0xffffffffu, v.w, d);
-            if (lane + d <= end) { v.x += tx; v.y += ty; v.z += tz; v.w += tw; }
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            const int d = 1 << r;
+            if (d < maxlen) {
+                const float tx = __shfl_down_sync(0xffffffffu, v.x, d);
+                const float ty = __shfl_down_sync(0xffffffffu, v.y, d);
+                const float tz = __shfl_down_sync(0xffffffffu, v.z, d);
+                const float tw = __shfl_down_sync(0xffffffffu, v.w, d);
+                if (take & (1u << r)) { v.x += tx; v.y += ty; v.z += tz; v.w += tw; }
+            }
         }
         if (head && valid && (in_grid || node_in_grid(q.st.b, i, j, k, G)))
             red_add_v4(grid + gaddr(c, q.st.b[0] + i, q.st.b[1] + j, q.st.b[2] + k), v);
