@@ -57,7 +57,7 @@ def load_peaks():
 # the dominant kernel, from one ncu capture of exactly this workload and
 # particle count on a B200: (workload, kernel, particles) -> bytes per launch.
 NCU_DRAM_BYTES = {
-    ("c4", "stress_p2g", 3172508): 403.351552e6 + 111.277312e6,
+    ("c4", "stress_p2g", 3172508): 403.247104e6 + 110.688512e6,
     ("lbs", "blend", 2000000): 196.818688e6 + 41.4976e6,
 }
 
@@ -233,7 +233,7 @@ def run_ours(args):
 
     w = get_workload(args.workload, args.particles, args.grid, args.substeps)
     solver, md, st, other = W.build_product(w, device=dev)
-    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap"):
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap"):
         val = getattr(args, opt)
         if val is not None:
             setattr(solver, opt, val)
@@ -440,7 +440,7 @@ def run_ours_c4(args):
     specs, dt, T = W.c4(T=args.substeps or 300)
     total = sum(s.n for s in specs)
     batch = BatchedMPM(specs, device=dev)
-    explicit = [o for o in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap") if getattr(args, o) is not None]
+    explicit = [o for o in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap") if getattr(args, o) is not None]
     for opt in explicit:
         setattr(batch, opt, getattr(args, opt))
     tuned = None
@@ -453,7 +453,7 @@ def run_ours_c4(args):
         tuned = {"options": res["options"], "candidates": len(res["ms"]), "seconds": time.perf_counter() - t_tune,
                  "best_ms_per_substep": min(res["ms"].values()),
                  "default_ms_per_substep": res["ms"].get(json.dumps(dict(sort_every=16, p2g_mode=2, tile_cap=1024,
-                                                                         g2p_tile=0), sort_keys=True))}
+                                                                         seg_cap=4, g2p_tile=0), sort_keys=True))}
     init = [t.clone() for t in (batch._x4[0], batch._v4[0], batch._C[0], batch._F[0], batch.mu, batch.lam,
                                 batch.yield_stress)]
 
@@ -620,7 +620,8 @@ def run_ours_c4(args):
                    "l2": "inputs larger than L2 (working set ~1 GB > 126 MB), no flush",
                    "launch": "one CUDA graph per 50-substep block for the whole population",
                    "options": {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode,
-                               "g2p_tile": batch.g2p_tile, "tile_cap": batch.tile_cap},
+                               "g2p_tile": batch.g2p_tile, "tile_cap": batch.tile_cap,
+                               "seg_cap": batch.seg_cap},
                    "autotune": tuned,
                    "substep_us": substep_ms * 1e3,
                    "substep_hbm_frac": (total * bp["substep"] / (substep_ms / 1e3) / 1e9) / peak,
@@ -671,7 +672,7 @@ def run_ours_c3(args):
     target = W.c3(guess=False, **kw)
     every = args.checkpoint_every
     solver, md, st, other = W.build_product(target, device=dev)
-    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap"):
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap"):
         val = getattr(args, opt)
         if val is not None:
             setattr(solver, opt, val)
@@ -1230,6 +1231,8 @@ def main():
     ap.add_argument("--p2g-mode", dest="p2g_mode", type=int, default=None, help="0 direct, 1 tile, 2 warp-aggregated")
     ap.add_argument("--g2p-tile", dest="g2p_tile", type=int, default=None)
     ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
+    ap.add_argument("--seg-cap", dest="seg_cap", type=int, default=None,
+                    help="warp-aggregated P2G: longest same-cell run per reduction (4, 8, 16, 32)")
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="c4: keep the default launch options instead of tuning them on the population")
     args = ap.parse_args()

@@ -6,9 +6,9 @@ the FP64 oracle), so it can be picked by speed alone. The tuner times a few
 substeps of the caller's own workload under each candidate:
 
 * ``sort_every``: the period of the cell sort (8, 16, 32 substeps);
-* ``p2g_mode`` / ``tile_cap``: warp-aggregated reductions into the grid, or
-  accumulation in a per-CTA shared-memory node tile of 512 / 1024 / 2048 nodes
-  (the tile shape);
+* ``p2g_mode`` / ``tile_cap`` / ``seg_cap``: warp-aggregated reductions into
+  the grid over same-cell runs of at most 4 or 8 lanes, or accumulation in a
+  per-CTA shared-memory node tile of 512 / 1024 / 2048 nodes (the tile shape);
 * ``g2p_tile``: G2P gathering directly from L2 or from a staged tile.
 
 It restores the state after every trial, keeps the fastest candidate and
@@ -25,10 +25,11 @@ import os
 from typing import Dict, List, Optional, Sequence
 
 CANDIDATES: List[Dict[str, int]] = [
-    dict(sort_every=s, p2g_mode=m, tile_cap=c, g2p_tile=g)
-    for s, (m, c), g in itertools.product((8, 16, 32), ((2, 1024), (1, 512), (1, 1024), (1, 2048)), (0, 1))
+    dict(sort_every=s, p2g_mode=m, tile_cap=c, seg_cap=k, g2p_tile=g)
+    for s, (m, c, k), g in itertools.product(
+        (8, 16, 32), ((2, 1024, 4), (2, 1024, 8), (1, 512, 4), (1, 1024, 4), (1, 2048, 4)), (0, 1))
 ]
-OPTION_NAMES = ("sort_every", "p2g_mode", "tile_cap", "g2p_tile")
+OPTION_NAMES = ("sort_every", "p2g_mode", "tile_cap", "seg_cap", "g2p_tile")
 
 _MEMORY: Dict[str, Dict] = {}
 

@@ -123,6 +123,7 @@ class BatchedMPM:
         self.p2g_mode = 2
         self.g2p_tile = False
         self.tile_cap = 1024
+        self.seg_cap = 4           # warp-aggregated P2G: longest same-cell run per reduction
         self._opts = {}
         # per-instance collider lists / schedule builders
         self.solvers = []
@@ -235,7 +236,8 @@ class BatchedMPM:
 
     def _apply_options(self):
         opts = {N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_MODE: int(self.p2g_mode),
-                N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap)}
+                N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap),
+                N.OPT_SEG_CAP: int(self.seg_cap)}
         for k, v in opts.items():
             if self._opts.get(k) != v:
                 N.check(self.L.empm_ctx_set_option(self.ptr, k, v), self.ptr)

@@ -17,6 +17,7 @@ struct GraphKey {
     int           p2g_mode;
     int           g2p_tile;
     int           tile_cap;
+    int           seg_cap;
     unsigned long long params_version;
 };
 
@@ -99,6 +100,7 @@ struct EmpmCtx {
     int          p2g_mode = 2;             // 0 direct reductions, 1 shared-memory tile, 2 warp-aggregated
     int          g2p_tile = 0;
     int          tile_cap = 1024;          // nodes per shared-memory tile (16 B each)
+    int          seg_cap = 4;              // warp-aggregated P2G: longest same-cell run per head
     SortedBuffers sb;
     AdjointBuffers adj;
     // per-kernel event timing (stream path only)

@@ -538,7 +538,7 @@ __global__ void k_unsort(const UnsortArgs a) {
 // the segment's contributions are summed with shuffles and only the segment
 // head issues the 16-byte reduction to the grid.
 __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
-                                                     float4* grid, unsigned char* flags) {
+                                                     float4* grid, unsigned char* flags, int seg_cap) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const int inst = p < L.n_total ? find_instance_particle(L, p) : 0;
@@ -553,7 +553,12 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
               u2 = __shfl_up_sync(0xffffffffu, b2, 1);
     const int uv = __shfl_up_sync(0xffffffffu, (int)valid, 1);
     const int ui = __shfl_up_sync(0xffffffffu, inst, 1);
-    const bool head = lane == 0 || uv != (int)valid || ui != inst || u0 != b0 || u1 != b1 || u2 != b2;
+    const bool run_head = lane == 0 || uv != (int)valid || ui != inst || u0 != b0 || u1 != b1 || u2 != b2;
+    // runs longer than seg_cap (a power of two) get another head every
+    // seg_cap lanes: fewer shuffle rounds below, more reductions into the grid
+    const unsigned run_heads = __ballot_sync(0xffffffffu, run_head);
+    const int run_start = 31 - __clz(run_heads & (0xffffffffu >> (31 - lane)));
+    const bool head = run_head || ((lane - run_start) & (seg_cap - 1)) == 0;
     const unsigned heads = __ballot_sync(0xffffffffu, head);
     const unsigned above = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
     const int end = above ? (__ffs(above) - 2) : 31;

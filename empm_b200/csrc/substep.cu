@@ -279,6 +279,11 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
             if (value < 27 || value > 3072) return empm_set_error(ctx, EMPM_ERR_INVALID, "tile_cap %d out of [27, 3072]", value);
             ctx->tile_cap = value;
             break;
+        case EMPM_OPT_SEG_CAP:
+            if (value < 1 || value > 32 || (value & (value - 1)) != 0)
+                return empm_set_error(ctx, EMPM_ERR_INVALID, "seg_cap %d not a power of two in 1..32", value);
+            ctx->seg_cap = value;
+            break;
         default: return empm_set_error(ctx, EMPM_ERR_INVALID, "unknown option %d", option);
     }
     ctx->graph_valid = false;
@@ -693,7 +698,8 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaS
     const size_t smem = sizeof(float4) * (size_t)ctx->tile_cap;
     timing_mark(ctx, 0, 0, stream);
     if (ctx->p2g_mode == 2) {
-        k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, stream>>>(t.P, t.M, t.Fe, t.L, ctx->grid_mom, ctx->flags);
+        k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, stream>>>(t.P, t.M, t.Fe, t.L, ctx->grid_mom, ctx->flags,
+                                                              ctx->seg_cap);
     } else {
         k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
     }
@@ -819,6 +825,7 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
     key.p2g_mode = ctx->p2g_mode;
     key.g2p_tile = ctx->g2p_tile;
     key.tile_cap = ctx->tile_cap;
+    key.seg_cap = ctx->seg_cap;
     key.params_version = ctx->params_version;
     if (!ctx->graph_valid || memcmp(&key, &ctx->graph_key, sizeof(key)) != 0) {
         if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
@@ -1047,7 +1054,7 @@ static int launch_substep_arrays(EmpmCtx* ctx, const ParticleArrays& Pin, const 
     const int n = ctx->n_particles;
     const Launch L = make_launch(ctx, table);
     timing_mark(ctx, 0, 0, s);
-    if (warpagg) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags);
+    if (warpagg) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags, ctx->seg_cap);
     else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags);
     timing_mark(ctx, 0, 1, s);
     CK(cudaGetLastError(), "adjoint segment P2G");
@@ -1189,7 +1196,8 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         const Launch Lrec = make_launch(ctx, n_steps + k);
         const Launch Lk = make_launch(ctx, k);
         timing_mark(ctx, 0, 0, s);
-        if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
+        if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags,
+                                                                     ctx->seg_cap);
         else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
         timing_mark(ctx, 0, 1, s);
         CK(cudaGetLastError(), "P2G (adjoint recompute)");

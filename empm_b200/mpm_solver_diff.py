@@ -88,6 +88,7 @@ class MPMWARPDiff(object):
         self.p2g_mode = 2          # 0 direct, 1 shared-memory tile, 2 warp-aggregated
         self.g2p_tile = False
         self.tile_cap = 1024
+        self.seg_cap = 4           # warp-aggregated P2G: longest same-cell run per reduction
 
     def initialize(self, n_particles, n_grid=100, grid_lim=1.0, device="cuda:0"):
         self.n_particles = n_particles
@@ -155,7 +156,8 @@ class MPMWARPDiff(object):
         else:
             c.set_params(params)
         c.set_options({N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_MODE: int(self.p2g_mode),
-                       N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap)})
+                       N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap),
+                       N.OPT_SEG_CAP: int(self.seg_cap)})
         return c
 
     @staticmethod

@@ -265,6 +265,9 @@ int  empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMa
                                     over same-cell particles (default) */
 #define EMPM_OPT_G2P_TILE    3   /* 1 = G2P stages the node tile in shared memory (default), 0 = direct gathers */
 #define EMPM_OPT_TILE_CAP    4   /* nodes per shared-memory tile, 27..3072 (default 1024 = 16 KiB) */
+#define EMPM_OPT_SEG_CAP     5   /* warp-aggregated P2G: same-cell runs longer than this (a power of two,
+                                    1..32 lanes) are split, trading shuffle rounds for grid reductions
+                                    (default 4) */
 
 int  empm_ctx_set_option(EmpmCtx* ctx, int option, int value);
 

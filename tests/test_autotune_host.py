@@ -6,9 +6,10 @@ from empm_b200 import autotune as A
 
 def test_candidates_cover_every_launch_option():
     keys = {tuple(sorted(c.items())) for c in A.CANDIDATES}
-    assert len(keys) == len(A.CANDIDATES) == 24
+    assert len(keys) == len(A.CANDIDATES) == 30
     assert {c["sort_every"] for c in A.CANDIDATES} == {8, 16, 32}
-    assert {(c["p2g_mode"], c["tile_cap"]) for c in A.CANDIDATES} == {(2, 1024), (1, 512), (1, 1024), (1, 2048)}
+    assert {(c["p2g_mode"], c["tile_cap"], c["seg_cap"]) for c in A.CANDIDATES} == {
+        (2, 1024, 4), (2, 1024, 8), (1, 512, 4), (1, 1024, 4), (1, 2048, 4)}
     assert {c["g2p_tile"] for c in A.CANDIDATES} == {0, 1}
 
 

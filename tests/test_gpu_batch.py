@@ -112,13 +112,14 @@ def test_batch_graph_reuse_and_reload():
     assert max_abs(batch.positions(), x1) <= 1e-5
 
 
-@pytest.mark.parametrize("sort_every,p2g_mode", [(0, 0), (8, 2), (8, 1), (32, 0)])
-def test_batch_launch_options_agree(sort_every, p2g_mode):
+@pytest.mark.parametrize("sort_every,p2g_mode,seg_cap", [(0, 0, 4), (8, 2, 4), (8, 2, 2), (8, 2, 32), (8, 1, 4),
+                                                   (32, 0, 4)])
+def test_batch_launch_options_agree(sort_every, p2g_mode, seg_cap):
     specs = _specs()
     ref = BatchedMPM(specs, device=DEV)
     ref.rollout(2e-4, 24, block=12)
     b = BatchedMPM(specs, device=DEV)
-    b.sort_every, b.p2g_mode = sort_every, p2g_mode
+    b.sort_every, b.p2g_mode, b.seg_cap = sort_every, p2g_mode, seg_cap
     b.rollout(2e-4, 24, block=12)
     torch.cuda.synchronize()
     assert max_abs(b.positions(), ref.positions()) <= 1e-5

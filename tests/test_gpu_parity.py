@@ -306,16 +306,18 @@ def test_status_word_flags_cfl_and_nan():
     assert solver.read_status() == 0   # reading clears the word
 
 
-@pytest.mark.parametrize("sort_every,p2g_mode,g2p_tile,tile_cap", [
-    (0, 0, False, 1024),       # direct path
-    (1, 2, True, 1024),
-    (4, 1, False, 1024),
-    (16, 0, True, 1024),
-    (16, 1, True, 1024),
-    (16, 2, False, 1024),
-    (16, 1, True, 64),         # tiny tile: forces the fallback path for most chunks
+@pytest.mark.parametrize("sort_every,p2g_mode,g2p_tile,tile_cap,seg_cap", [
+    (0, 0, False, 1024, 4),       # direct path
+    (1, 2, True, 1024, 4),
+    (4, 1, False, 1024, 4),
+    (16, 0, True, 1024, 4),
+    (16, 1, True, 1024, 4),
+    (16, 2, False, 1024, 4),
+    (16, 2, False, 1024, 1),      # every lane its own reduction
+    (16, 2, False, 1024, 32),     # whole same-cell runs per reduction
+    (16, 1, True, 64, 4),         # tiny tile: forces the fallback path for most chunks
 ])
-def test_sorted_path_vs_oracle(sort_every, p2g_mode, g2p_tile, tile_cap):
+def test_sorted_path_vs_oracle(sort_every, p2g_mode, g2p_tile, tile_cap, seg_cap):
     n, G, T, dt = 20000, 48, 120, 2e-4
     x, v, vol, rho, E, nu, ys = _c1_like(n, G, 11, 5, T, dt, plastic=True)
     v = (np.random.default_rng(12).standard_normal((n, 3)) * 0.5).astype(np.float32)
@@ -332,6 +334,7 @@ def test_sorted_path_vs_oracle(sort_every, p2g_mode, g2p_tile, tile_cap):
     solver = MPMWARPDiff()
     solver.initialize(n, n_grid=G)
     solver.sort_every, solver.p2g_mode, solver.g2p_tile, solver.tile_cap = sort_every, p2g_mode, g2p_tile, tile_cap
+    solver.seg_cap = seg_cap
     solver.add_surface_collider((0.0, 3.0 / G, 0.0), (0.0, 1.0, 0.0), "sticky", 0.0)
     solver.set_velocity_on_cuboid([0.5, 0.68, 0.5], [0.08, 0.05, 0.08], [0.0, -1.0, 0.0])
     solver.add_bounding_box()
