@@ -286,10 +286,14 @@ __device__ __forceinline__ void p2g_emit(const P2GPre& p, Emit emit) {
     const Stencil& st = p.st;
     const V3 B0 = col(p.B, 0), B1 = col(p.B, 1), B2 = col(p.B, 2);
     const V3 S0 = col(p.S, 0), S1 = col(p.S, 1), S2 = col(p.S, 2);
-#pragma unroll
+    // the outer axis is a loop (weights picked by selects): a third of the
+    // code of the fully unrolled 27 nodes, for the instruction cache (a loop
+    // over the middle axis as well measured slower)
+#pragma unroll 1
     for (int i = 0; i < 3; ++i) {
         const V3 ai = p.a + (float)i * B0;
-        const float wx = st.w[0][i], dwx = st.dw[0][i];
+        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
+        const float dwx = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const V3 aij = ai + (float)j * B1;
