@@ -38,10 +38,26 @@ EMPM_HD M3 usv(const M3& U, V3 s, const M3& V) {
     return r;
 }
 
-// tau = U diag(d) V^T F^T
-EMPM_HD M3 spectral_stress(const M3& U, V3 d, const M3& V, const M3& F) {
-    return usv(U, d, V) * transpose(F);
+// U diag(t) U^T (symmetric)
+EMPM_HD M3 u_diag_ut(const M3& U, V3 t) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float a0 = U.m[3 * i + 0] * t.x, a1 = U.m[3 * i + 1] * t.y, a2 = U.m[3 * i + 2] * t.z;
+#pragma unroll
+        for (int j = i; j < 3; ++j) {
+            const float v = a0 * U.m[3 * j + 0] + a1 * U.m[3 * j + 1] + a2 * U.m[3 * j + 2];
+            r.m[3 * i + j] = v;
+            r.m[3 * j + i] = v;
+        }
+    }
+    return r;
 }
+
+// The stresses below have the form tau = U diag(d) V^T F^T with F the elastic
+// F = U diag(s) V^T, i.e. tau = U diag(d * s) U^T, symmetric already (the
+// reference symmetrises its explicit products, mpm_utils.py:665).
+EMPM_HD M3 spectral_stress(const M3& U, V3 d, V3 s) { return u_diag_ut(U, v3(d.x * s.x, d.y * s.y, d.z * s.z)); }
 
 // Von Mises projection on Hencky strain (mpm_utils.py:87-130; with damage
 // and softening :133-186 when `damage` is set). Updates s (singular values of
@@ -130,15 +146,15 @@ EMPM_HD ConstitutiveOut constitutive(const M3& Ft, float& mu, float& lam, float&
         case 5: von_mises(U, s, V, mu, lam, ys, ms, true, out.mat_changed, F); break;
         default: break;
     }
-    const float J = det(F);
+    // F = U diag(s) V^T (after the return maps too), so det F = s.x s.y s.z
+    const float J = s.x * s.y * s.z;
     M3 tau = m3_zero();
     switch (ms.material) {
         case 0:
-        case 5: {  // fixed-corotated (mpm_utils.py:8-15)
-            const M3 R = U * transpose(V);
-            tau = (2.f * mu) * ((F - R) * transpose(F));
+        case 5: {  // fixed-corotated (mpm_utils.py:8-15): 2 mu (F - R) F^T + lam J (J - 1) I, R = U V^T
             const float d = lam * J * (J - 1.f);
-            tau.m[0] += d; tau.m[4] += d; tau.m[8] += d;
+            tau = u_diag_ut(U, v3(2.f * mu * (s.x - 1.f) * s.x + d, 2.f * mu * (s.y - 1.f) * s.y + d,
+                                  2.f * mu * (s.z - 1.f) * s.z + d));
             break;
         }
         case 1:
@@ -147,7 +163,7 @@ EMPM_HD ConstitutiveOut constitutive(const M3& Ft, float& mu, float& lam, float&
             const V3 e = v3(logf(sg.x), logf(sg.y), logf(sg.z));
             const float ls = logf(sg.x) + logf(sg.y) + logf(sg.z);
             const V3 d = 2.f * mu * e + v3(lam * ls, lam * ls, lam * ls);
-            tau = spectral_stress(U, d, V, F);
+            tau = spectral_stress(U, d, s);
             break;
         }
         case 2: {  // Drucker-Prager (mpm_utils.py:69-84)
@@ -155,7 +171,7 @@ EMPM_HD ConstitutiveOut constitutive(const M3& Ft, float& mu, float& lam, float&
             const V3 d = v3(2.f * mu * logf(s.x) * (1.f / s.x) + lam * ls * (1.f / s.x),
                             2.f * mu * logf(s.y) * (1.f / s.y) + lam * ls * (1.f / s.y),
                             2.f * mu * logf(s.z) * (1.f / s.z) + lam * ls * (1.f / s.z));
-            tau = spectral_stress(U, d, V, F);
+            tau = spectral_stress(U, d, s);
             break;
         }
         case 6: {  // compressible neo-Hookean (mpm_utils.py:18-47)
@@ -165,13 +181,13 @@ EMPM_HD ConstitutiveOut constitutive(const M3& Ft, float& mu, float& lam, float&
             const float a = mu * powf(J, -2.f / 3.f);
             const float c = lam / 2.f * (J * J - 1.f);
             const V3 d = a * bh + v3(c, c, c);
-            tau = spectral_stress(U, d, V, F);
+            tau = spectral_stress(U, d, s);
             break;
         }
         default: break;  // snow (4) and unknown ids: zero stress
     }
     out.F = F;
-    out.tau = 0.5f * (tau + transpose(tau));
+    out.tau = tau;
     return out;
 }
 
