@@ -289,9 +289,11 @@ __device__ __forceinline__ void grid_update_blocks(const GridUpdateArgs& a) {
 __global__ void __launch_bounds__(256) k_grid_update_sparse(const GridUpdateArgs a) { grid_update_blocks<false>(a); }
 
 // Touched blocks -> list: active[0] counts them, active[1 + i] are their ids
-// (in no particular order). Clears the flags unless kKeep.
+// (in no particular order) and active[1 + nblocks + i] their instances (the
+// lookup done once per block here rather than once per node by the update).
+// Clears the flags unless kKeep. active holds 1 + 2 * nblocks ints.
 template <bool kKeep>
-__global__ void __launch_bounds__(256) k_collect_blocks(unsigned char* flags, int nblocks, int* active) {
+__global__ void __launch_bounds__(256) k_collect_blocks(unsigned char* flags, int nblocks, int* active, const Launch L) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const bool on = b < nblocks && flags[b] != 0;
@@ -302,7 +304,9 @@ __global__ void __launch_bounds__(256) k_collect_blocks(unsigned char* flags, in
     if (lane == leader) base = atomicAdd(active, __popc(m));
     base = __shfl_sync(0xffffffffu, base, leader);
     if (on) {
-        active[1 + base + __popc(m & ((1u << lane) - 1u))] = b;
+        const int slot = base + __popc(m & ((1u << lane) - 1u));
+        active[1 + slot] = b;
+        active[1 + nblocks + slot] = find_instance_block(L, b);
         if (!kKeep) flags[b] = 0;
     }
 }
@@ -315,7 +319,7 @@ __global__ void __launch_bounds__(256) k_grid_update_list(const GridUpdateArgs a
          idx += (long long)gridDim.x * blockDim.x) {
         const int b = __ldg(active + 1 + (idx >> 6));
         const int in_block = (int)(idx & 63);
-        const int inst = find_instance_block(a.L, b);
+        const int inst = __ldg(active + 1 + a.L.nblocks + (idx >> 6));
         const InstanceConsts* I = a.L.inst + inst;
         const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
         const long long node = ((long long)b << 6) | in_block;

@@ -222,7 +222,7 @@ extern "C" int empm_batch_create(const EmpmModelParams* params, const int* n_par
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_mom, grid_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->grid_vel, grid_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->flags, (size_t)blocks);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->active, sizeof(int) * ((size_t)blocks + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->active, sizeof(int) * (2 * (size_t)blocks + 1));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_mom, 0, grid_bytes);
     if (e == cudaSuccess) e = cudaMemset(ctx->grid_vel, 0, grid_bytes);
@@ -329,7 +329,7 @@ extern "C" int empm_batch_reserve(EmpmCtx* ctx, int max_particles, long long max
         CK(cudaMalloc(&ctx->grid_mom, grid_bytes), "reserve grid");
         CK(cudaMalloc(&ctx->grid_vel, grid_bytes), "reserve grid");
         CK(cudaMalloc(&ctx->flags, (size_t)max_blocks), "reserve grid");
-        CK(cudaMalloc(&ctx->active, sizeof(int) * ((size_t)max_blocks + 1)), "reserve grid");
+        CK(cudaMalloc(&ctx->active, sizeof(int) * (2 * (size_t)max_blocks + 1)), "reserve grid");
         CK(cudaMemset(ctx->grid_mom, 0, grid_bytes), "reserve grid");
         CK(cudaMemset(ctx->grid_vel, 0, grid_bytes), "reserve grid");
         CK(cudaMemset(ctx->flags, 0, (size_t)max_blocks), "reserve grid");
@@ -515,7 +515,7 @@ static int launch_grid_update_list(EmpmCtx* ctx, const Launch& L, cudaStream_t s
     g.L = L;
     CK(cudaMemsetAsync(ctx->active, 0, sizeof(int), stream), "reset touched-block count");
     k_collect_blocks<kKeep><<<blocks_for(ctx->nblocks, 256), 256, 0, stream>>>(ctx->flags, (int)ctx->nblocks,
-                                                                               ctx->active);
+                                                                               ctx->active, L);
     CK(cudaGetLastError(), "k_collect_blocks");
     k_grid_update_list<kKeep><<<ctx->sm_count * 8, 256, 0, stream>>>(g, ctx->active);
     CK(cudaGetLastError(), "k_grid_update_list");
@@ -1280,7 +1280,8 @@ extern "C" int empm_restart_F(EmpmCtx* ctx, EmpmParticles* p, const float* targe
     k_restart_p2g<<<blocks_for(n, 128), 128, 0, s>>>(P, target, selection, L, ctx->grid_mom, ctx->flags);
     CK(cudaGetLastError(), "k_restart_p2g");
     CK(cudaMemsetAsync(ctx->active, 0, sizeof(int), s), "reset touched-block count");
-    k_collect_blocks<false><<<blocks_for(ctx->nblocks, 256), 256, 0, s>>>(ctx->flags, (int)ctx->nblocks, ctx->active);
+    k_collect_blocks<false><<<blocks_for(ctx->nblocks, 256), 256, 0, s>>>(ctx->flags, (int)ctx->nblocks, ctx->active,
+                                                                          L);
     CK(cudaGetLastError(), "k_collect_blocks");
     k_restart_grid<<<ctx->sm_count * 8, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active);
     CK(cudaGetLastError(), "k_restart_grid");
