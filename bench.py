@@ -867,7 +867,7 @@ def run_ours_c5(args):
     from empm_b200.serving import MPMServer
 
     rate, seconds = args.c5_rate, args.c5_seconds
-    arrivals = W.c5_arrivals(seed=5 + rank, rate=rate, seconds=seconds)
+    arrivals = W.c5_arrivals(seed=5 + rank, rate=rate, seconds=seconds, grad_fraction=args.c5_grad_fraction)
     srv = MPMServer(hbm_budget=int(args.c5_budget_gb * (1 << 30)), device=dev).start()
     # warm-up: a few small requests of each kind
     warm = [srv.submit(W.c5_request(g, 20_000, 48, 60, 1000 + i)) for i, g in enumerate([False, True] * args.warmup)]
@@ -918,18 +918,22 @@ def run_ours_c5(args):
     # single-instance API (rollout, or checkpointed rollout + adjoint)
     prng = np.random.default_rng(55)
     sample = [arrivals[i] for i in prng.choice(len(arrivals), size=min(args.c5_plain, len(arrivals)), replace=False)]
-    plain_ps, plain_ms = 0, 0.0
+    plain_ps, plain_ms, kernel_ms = 0, 0.0, 0.0
     for (_, grad, n, G, T, sd) in sample:
         req = W.c5_request(grad, n, G, T, sd)
         solver, md, st = single_instance(req.spec, device=dev)
         other = st.partial_clone()
         target = torch.as_tensor(req.target, device=dev) if grad else None
         init = [a.clone() for a in (st._x4, st._v4, st._C, st._F_trial, md.mu, md.lam, md.yield_stress)]
-        for rep in range(2):   # the first run creates the context, captures graphs and allocates buffers
+
+        def restore():
             for dst, src in zip((st._x4, st._v4, st._C, st._F_trial, md.mu, md.lam, md.yield_stress), init):
                 dst.copy_(src)
             solver.time = 0.0
             torch.cuda.synchronize()
+
+        for rep in range(2):   # the first run creates the context, captures graphs and allocates buffers
+            restore()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             if grad:
@@ -940,10 +944,27 @@ def run_ours_c5(args):
                 solver.rollout(md, st, other, req.dt, T)
             e1.record()
             torch.cuda.synchronize()
-        plain_ms += e0.elapsed_time(e1)
+        t_rollout = e0.elapsed_time(e1)
+        plain_ms += t_rollout
         plain_ps += n * T
+        if grad:
+            kernel_ms += t_rollout   # the checkpointed adjoint is the only single-instance gradient path
+        else:
+            # the plain kernel path: one p2g2p_differentiable call per substep
+            restore()
+            solver.p2g2p_differentiable(md, st, other, req.dt)   # warm-up of the direct path
+            restore()
+            e0.record()
+            a1, b1 = st, other
+            for _ in range(T):
+                solver.p2g2p_differentiable(md, a1, b1, req.dt)
+                a1, b1 = b1, a1
+            e1.record()
+            torch.cuda.synchronize()
+            kernel_ms += e0.elapsed_time(e1)
         del solver, md, st, other, init
     plain_value = plain_ps / (plain_ms / 1e3)
+    plain_kernel_value = plain_ps / (kernel_ms / 1e3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -966,8 +987,9 @@ def run_ours_c5(args):
         "metric": "served " + METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": 1,
         "warmup": args.warmup, "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"serving stream: Poisson {rate:g} req/s x {seconds:g} s, 70% rollouts / 30% rollout "
-                               "+ gradient, particles log-U[10k,1M], grids U{48..160}, substeps U[50,1000], "
+        "config": {"workload": f"serving stream: Poisson {rate:g} req/s x {seconds:g} s, "
+                               f"{100 * (1 - args.c5_grad_fraction):g}% rollouts / {100 * args.c5_grad_fraction:g}% "
+                               "rollout + gradient, particles log-U[10k,1M], grids U{48..160}, substeps U[50,1000], "
                                "plasticine with per-particle E/nu/yield distributions, dt=1e-4",
                    "requests": len(rows), "completed": len(ok),
                    "statuses": {s_: sum(1 for r in rows if r[0] == s_) for s_ in sorted({r[0] for r in rows})},
@@ -979,6 +1001,10 @@ def run_ours_c5(args):
                    "makespan_s": makespan, "hbm_budget_gb": args.c5_budget_gb,
                    "engine": {k: stats[k] for k in ("blocks", "substeps", "relayouts")},
                    "plain_value": plain_value, "served_vs_plain": value / plain_value,
+                   "plain_kernel_value": plain_kernel_value, "served_vs_plain_kernel": value / plain_kernel_value,
+                   "plain_kernel": "the same sampled requests with the rollouts driven one p2g2p_differentiable call "
+                                   "per substep (the plain single-instance kernel path, as the reference's "
+                                   "advance_to drives its kernels); gradient requests as in plain",
                    "plain": f"{len(sample)} requests sampled from the stream, one at a time through the "
                             "single-instance API (rollout with a CUDA graph; gradient: checkpointed rollout + "
                             "adjoint with 50-substep segments), each timed on its second run (context, graphs "
@@ -1218,6 +1244,8 @@ def main():
     ap.add_argument("--c5-seconds", dest="c5_seconds", type=float, default=60.0, help="c5: arrival window")
     ap.add_argument("--c5-budget-gb", dest="c5_budget_gb", type=float, default=60.0, help="c5: HBM budget")
     ap.add_argument("--c5-plain", dest="c5_plain", type=int, default=12, help="c5: requests timed one at a time")
+    ap.add_argument("--c5-grad-fraction", dest="c5_grad_fraction", type=float, default=0.3,
+                    help="c5: fraction of requests that also ask for a gradient")
     ap.add_argument("--checkpoint-every", dest="checkpoint_every", type=int, default=20,
                     help="c3: substeps between checkpoints of the differentiable rollout")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

@@ -342,6 +342,8 @@ class GpuExecutor:
         self.mat = {k: [torch.zeros(P, dtype=DTYPE, device=dev) for _ in range(2)]
                     for k in ("vol", "mu", "lam", "ys")}
         self.Fe = torch.zeros(9 * P, dtype=DTYPE, device=dev)
+        # first plane chunks of an identity F (float4 planes A, B)
+        self._id_row = torch.tensor([1.0, 0.0, 0.0, 0.0], dtype=DTYPE, device=dev)
         self.ai = 0        # current arena
         self.cur = 0       # current ping-pong state within it
         self.layout: List[Ticket] = []      # tickets in arena order
@@ -427,27 +429,31 @@ class GpuExecutor:
         counts = [t.n for t in active]
         n_new = int(sum(counts))
         offs = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64) if counts else np.zeros(0, np.int64)
-        dev = self.device
         with torch.cuda.stream(self.fwd_stream):
-            # surviving instances: one gather per array
-            src_rows, dst_rows = [], []
+            # surviving instances keep their order: copy them as contiguous runs
+            # (survivors that were neighbours stay neighbours), device to device,
+            # so that the host never waits for the GPU here
+            runs = []   # [src, dst, n]
             for t, o in zip(active, offs):
                 if t.id in new_ids:
                     continue
                 so = self.offsets[t.id]
-                src_rows.append(np.arange(so, so + t.n))
-                dst_rows.append(np.arange(o, o + t.n))
-            if src_rows:
-                si = torch.as_tensor(np.concatenate(src_rows), device=dev)
-                di = torch.as_tensor(np.concatenate(dst_rows), device=dev)
-                c = self.cur
-                new["x4"][0].index_copy_(0, di, old["x4"][c].index_select(0, si))
-                new["v4"][0].index_copy_(0, di, old["v4"][c].index_select(0, si))
+                if runs and runs[-1][0] + runs[-1][2] == so and runs[-1][1] + runs[-1][2] == o:
+                    runs[-1][2] += t.n
+                else:
+                    runs.append([so, int(o), t.n])
+            c = self.cur
+            old_planes = {k: self._planes(old[k][c], n_old) for k in ("C", "F")}
+            new_planes = {k: self._planes(new[k][0], n_new) for k in ("C", "F")}
+            for so, do, n in runs:
+                src, dst = slice(so, so + n), slice(do, do + n)
+                new["x4"][0][dst].copy_(old["x4"][c][src])
+                new["v4"][0][dst].copy_(old["v4"][c][src])
                 for k in ("C", "F"):
-                    for po, pn in zip(self._planes(old[k][c], n_old), self._planes(new[k][0], n_new)):
-                        pn.index_copy_(0, di, po.index_select(0, si))
+                    for po, pn in zip(old_planes[k], new_planes[k]):
+                        pn[dst].copy_(po[src])
                 for k in ("vol", "mu", "lam", "ys"):
-                    self.mat[k][new_ai].index_copy_(0, di, self.mat[k][self.ai].index_select(0, si))
+                    self.mat[k][new_ai][dst].copy_(self.mat[k][self.ai][src])
             # admitted instances: initial state from the host
             for t, o in zip(active, offs):
                 if t.id in new_ids:
@@ -479,8 +485,8 @@ class GpuExecutor:
         B[sl] = 0.0
         Cc[sl] = 0.0
         A, B, Cc = self._planes(arena["F"][0], n_total)
-        A[sl] = torch.tensor([1.0, 0.0, 0.0, 0.0], device=dev)
-        B[sl] = torch.tensor([1.0, 0.0, 0.0, 0.0], device=dev)
+        A[sl] = self._id_row
+        B[sl] = self._id_row
         Cc[sl] = 1.0
         vol = self.mat["vol"][ai][sl]
         vol.copy_(h(s.vol))
@@ -562,8 +568,8 @@ class GpuExecutor:
         sl = slice(o, o + n)
         with torch.cuda.stream(self.fwd_stream):
             if not t.req.grad:
-                hx = torch.empty((n, 3), dtype=self.DTYPE).pin_memory()
-                hv = torch.empty((n, 3), dtype=self.DTYPE).pin_memory()
+                hx = torch.empty((n, 3), dtype=self.DTYPE, pin_memory=True)
+                hv = torch.empty((n, 3), dtype=self.DTYPE, pin_memory=True)
                 hx.copy_(a["x4"][self.cur][sl, :3], non_blocking=True)
                 hv.copy_(a["v4"][self.cur][sl, :3], non_blocking=True)
                 ev = torch.cuda.Event()
@@ -610,9 +616,9 @@ class GpuExecutor:
                         self.actx)
             g_E, g_nu, _ = prepare_adjoint(t._E, t._nu, g_mu, g_lam)
             out = torch.stack([loss, g_E.sum(), g_nu.sum(), g_ys.sum()])
-            hs = torch.empty(4, dtype=self.DTYPE).pin_memory()
-            hgv = torch.empty((n, 3), dtype=self.DTYPE).pin_memory()
-            hx = torch.empty((n, 3), dtype=self.DTYPE).pin_memory()
+            hs = torch.empty(4, dtype=self.DTYPE, pin_memory=True)
+            hgv = torch.empty((n, 3), dtype=self.DTYPE, pin_memory=True)
+            hx = torch.empty((n, 3), dtype=self.DTYPE, pin_memory=True)
             hs.copy_(out, non_blocking=True)
             hgv.copy_(grad.v4[:, :3], non_blocking=True)
             hx.copy_(x_final, non_blocking=True)

@@ -180,18 +180,20 @@ def c4(seed: int = 4, n_inst: int = 32, T: int = 300, n_lo: int = 20_000, n_hi: 
     return specs, 2e-4, T
 
 
-def c5_arrivals(seed: int = 5, rate: float = 20.0, seconds: float = 60.0):
+def c5_arrivals(seed: int = 5, rate: float = 20.0, seconds: float = 60.0, grad_fraction: float = 0.3):
     """Arrival schedule of the serving stream: Poisson arrivals at `rate`
-    requests/s for `seconds`; 70 % rollouts, 30 % rollout + gradient;
-    particles log-uniform in [10k, 1M], grids uniform in 48..160, substeps
-    uniform in [50, 1000]. Returns [(t_arrival_s, grad, n, G, T, seed)]."""
+    requests/s for `seconds`; a `grad_fraction` of them (30 %) are rollout +
+    gradient, the rest rollouts; particles log-uniform in [10k, 1M], grids
+    uniform in 48..160, substeps uniform in [50, 1000]. The same draws are made
+    whatever grad_fraction is, so other fractions keep the same requests.
+    Returns [(t_arrival_s, grad, n, G, T, seed)]."""
     rng = np.random.default_rng(seed)
     out, t = [], 0.0
     while True:
         t += float(rng.exponential(1.0 / rate))
         if t > seconds:
             return out
-        grad = bool(rng.uniform() < 0.3)
+        grad = bool(rng.uniform() < grad_fraction)
         n = int(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
         G = int(rng.integers(48, 161))
         T = int(rng.integers(50, 1001))
