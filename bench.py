@@ -672,7 +672,7 @@ def run_ours_c3(args):
     target = W.c3(guess=False, **kw)
     every = args.checkpoint_every
     solver, md, st, other = W.build_product(target, device=dev)
-    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap"):
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap", "adj_store"):
         val = getattr(args, opt)
         if val is not None:
             setattr(solver, opt, val)
@@ -826,6 +826,8 @@ def run_ours_c3(args):
                    "particles": n, "grid": w.G, "substeps_per_step": w.T, "dt": w.dt,
                    "step": "checkpointed forward + adjoint of every substep (gradients in x0, v0, C0, F0, "
                            "mu, lam, yield, mass; E and nu through the prepare adjoint)",
+                   "reverse_pass": "reads each substep's stored grid and elastic F" if solver.adj_store
+                   else "recomputes each substep's P2G and grid update",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (segment states ~0.5 GB > 126 MB), no flush",
                    "forward_ms": fwd_ms, "gradient_over_forward": (ms / args.steps) / fwd_ms,
@@ -1261,6 +1263,8 @@ def main():
     ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
     ap.add_argument("--seg-cap", dest="seg_cap", type=int, default=None,
                     help="warp-aggregated P2G: longest same-cell run per reduction (4, 8, 16, 32)")
+    ap.add_argument("--adj-store", dest="adj_store", type=int, default=None,
+                    help="c3: 1 = the reverse pass reads each substep's stored grid and elastic F, 0 = recomputes them")
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="c4: keep the default launch options instead of tuning them on the population")
     args = ap.parse_args()

@@ -19,7 +19,7 @@ EMPM_STATUS_NAN, EMPM_STATUS_CFL, EMPM_STATUS_OUT_OF_BAND = 1, 2, 4
 COLL_SURFACE, COLL_GEOMETRY, COLL_GRID_VELOCITY, COLL_CUBOID_VELOCITY, COLL_BOUNDING_BOX, COLL_GRID_MASK = 1, 2, 3, 4, 5, 6
 SHAPE_CUBE, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_HALFSPACE = 1, 2, 3, 4
 GATE_OFF, GATE_APPLY, GATE_ZERO_ALL = 0, 1, 2
-OPT_SORT_EVERY, OPT_P2G_MODE, OPT_G2P_TILE, OPT_TILE_CAP, OPT_SEG_CAP = 1, 2, 3, 4, 5
+OPT_SORT_EVERY, OPT_P2G_MODE, OPT_G2P_TILE, OPT_TILE_CAP, OPT_SEG_CAP, OPT_ADJ_STORE = 1, 2, 3, 4, 5, 6
 MOD_IMPULSE, MOD_IMPULSE_MASK, MOD_SET_VELOCITY, MOD_ROTATION, MOD_MOVER = 1, 2, 3, 4, 5
 
 F3 = ctypes.c_float * 3

@@ -60,6 +60,14 @@ struct AdjointBuffers {
     float4* gmom = nullptr;    // adjoint of the P2G accumulation (blocked grid)
     float*  gstate = nullptr;  // state adjoint in cell order (packed like states)
     float*  gmats = nullptr;   // mu | lam | yield | mass adjoints in cell order
+    // stored substeps (EMPM_OPT_ADJ_STORE): per substep of the segment, the
+    // touched blocks' node momentum and velocity (128 float4 per block), their
+    // list (count, ids) and the elastic F, so the reverse pass need not
+    // recompute P2G and the grid update
+    int     store_cap = 0;     // substeps the store holds (0 = not allocated)
+    float4* gsave = nullptr;   // store_cap x cap_blocks x 128 float4
+    int*    gsave_list = nullptr;  // store_cap x (1 + cap_blocks)
+    float*  fe_store = nullptr;    // store_cap x f9 planes of cap_n particles
     std::vector<EmpmStep> tables;   // host staging of the step tables
 };
 
@@ -101,6 +109,7 @@ struct EmpmCtx {
     int          g2p_tile = 0;
     int          tile_cap = 1024;          // nodes per shared-memory tile (16 B each)
     int          seg_cap = 4;              // warp-aggregated P2G: longest same-cell run per head
+    int          adj_store = 1;            // adjoint segments store substep grids instead of recomputing
     SortedBuffers sb;
     AdjointBuffers adj;
     // per-kernel event timing (stream path only)

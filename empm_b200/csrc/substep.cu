@@ -125,7 +125,17 @@ static void free_sorted(SortedBuffers& sb) {
     sb = SortedBuffers();
 }
 
+static void free_store(AdjointBuffers& ab) {
+    void* ptrs[] = {ab.gsave, ab.gsave_list, ab.fe_store};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    ab.gsave = nullptr;
+    ab.gsave_list = nullptr;
+    ab.fe_store = nullptr;
+    ab.store_cap = 0;
+}
+
 static void free_adjoint(AdjointBuffers& ab) {
+    free_store(ab);
     void* ptrs[] = {ab.states, ab.mats, ab.work, ab.fe, ab.gfe, ab.gx, ab.gacc, ab.gmom, ab.gstate, ab.gmats};
     for (void* q : ptrs) if (q) cudaFree(q);
     ab = AdjointBuffers();
@@ -279,6 +289,7 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
             if (value < 27 || value > 3072) return empm_set_error(ctx, EMPM_ERR_INVALID, "tile_cap %d out of [27, 3072]", value);
             ctx->tile_cap = value;
             break;
+        case EMPM_OPT_ADJ_STORE: ctx->adj_store = value != 0; break;
         case EMPM_OPT_SEG_CAP:
             if (value < 1 || value > 32 || (value & (value - 1)) != 0)
                 return empm_set_error(ctx, EMPM_ERR_INVALID, "seg_cap %d not a power of two in 1..32", value);
@@ -1056,6 +1067,23 @@ static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
         CK(cudaMalloc(&ab.mats, (size_t)n_steps * 3 * np * sizeof(float)), "adjoint segment material");
         ab.capacity = n_steps;
     }
+    if (ctx->adj_store && n_steps > ab.store_cap) {
+        // the store is an optimisation: when it does not fit, the reverse
+        // pass recomputes instead (free_store leaves store_cap at 0)
+        if (ab.store_cap) CK(cudaDeviceSynchronize(), "sync before adjoint store growth");
+        free_store(ab);
+        const size_t nb = (size_t)ab.cap_blocks;
+        cudaError_t e = cudaMalloc(&ab.gsave, (size_t)n_steps * nb * 128 * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMalloc(&ab.gsave_list, (size_t)n_steps * (nb + 1) * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&ab.fe_store, (size_t)n_steps * 9 * np * sizeof(float));
+        if (e == cudaSuccess) {
+            ab.store_cap = n_steps;
+        } else {
+            free_store(ab);
+            if (e != cudaErrorMemoryAllocation) return empm_check_cuda(ctx, e, "adjoint store");
+            cudaGetLastError();   // an allocation failure is not sticky; clear it
+        }
+    }
     return EMPM_OK;
 }
 
@@ -1189,12 +1217,42 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
     //    The last substep runs too, although the state after it is not needed:
     //    its P2G writes the velocity modifiers into that substep's stored
     //    velocities, which the recompute below (without modifiers) relies on.
+    //    With the store, each substep keeps its touched grid blocks and its
+    //    elastic F (P2G writes it straight into the substep's store slot).
+    const bool store = ab.store_cap >= n_steps;
+    const int grid_ctas = ctx->sm_count * 8;
+    auto fe_slot = [&](int k) { return f9_planes(ab.fe_store + (size_t)k * 9 * np, n); };
+    auto gsave_slot = [&](int k) { return ab.gsave + (size_t)k * (size_t)ab.cap_blocks * 128; };
+    auto glist_slot = [&](int k) { return ab.gsave_list + (size_t)k * ((size_t)ab.cap_blocks + 1); };
     for (int k = 0; k < n_steps; ++k) {
         CK(cudaMemcpyAsync(ab.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), d2d, s), "snapshot");
         const ParticleArrays Pin = particle_arrays(ab.states + (size_t)k * state_floats, n);
         const ParticleArrays Pout = particle_arrays(ab.states + (size_t)(k + 1) * state_floats, n);
-        rc = launch_substep_arrays(ctx, Pin, Pout, Mw, Fe, k, sorted, s);
+        if (!store) {
+            rc = launch_substep_arrays(ctx, Pin, Pout, Mw, Fe, k, sorted, s);
+            if (rc) return rc;
+            continue;
+        }
+        const F9Planes Fk = fe_slot(k);
+        const Launch Lk = make_launch(ctx, k);
+        timing_mark(ctx, 0, 0, s);
+        if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
+                                                                     ctx->seg_cap);
+        else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
+        timing_mark(ctx, 0, 1, s);
+        CK(cudaGetLastError(), "adjoint segment P2G");
+        timing_mark(ctx, 1, 0, s);
+        rc = launch_grid_update_list<true>(ctx, Lk, s);
         if (rc) return rc;
+        k_save_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active, gsave_slot(k), glist_slot(k));
+        CK(cudaGetLastError(), "k_save_grid");
+        k_clear_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->flags, ctx->active);
+        CK(cudaGetLastError(), "k_clear_grid");
+        timing_mark(ctx, 1, 1, s);
+        timing_mark(ctx, 2, 0, s);
+        k_g2p_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Fk, Mw, Pout, Lk, ctx->grid_vel);
+        timing_mark(ctx, 2, 1, s);
+        CK(cudaGetLastError(), "adjoint segment G2P");
     }
 
     // 3. substeps in reverse: recompute the grid, then the three adjoint kernels
@@ -1206,19 +1264,26 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         const ParticleArrays Pk = particle_arrays(ab.states + (size_t)k * state_floats, n);
         const Launch Lrec = make_launch(ctx, n_steps + k);
         const Launch Lk = make_launch(ctx, k);
-        timing_mark(ctx, 0, 0, s);
-        if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags,
-                                                                     ctx->seg_cap);
-        else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
-        timing_mark(ctx, 0, 1, s);
-        CK(cudaGetLastError(), "P2G (adjoint recompute)");
-        timing_mark(ctx, 1, 0, s);
-        rc = launch_grid_update_list<true>(ctx, Lrec, s);
-        timing_mark(ctx, 1, 1, s);
-        if (rc) return rc;
+        const F9Planes Fk = store ? fe_slot(k) : Fe;
+        if (store) {
+            k_restore_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->flags, gsave_slot(k),
+                                                     glist_slot(k));
+            CK(cudaGetLastError(), "k_restore_grid");
+        } else {
+            timing_mark(ctx, 0, 0, s);
+            if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags,
+                                                                         ctx->seg_cap);
+            else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
+            timing_mark(ctx, 0, 1, s);
+            CK(cudaGetLastError(), "P2G (adjoint recompute)");
+            timing_mark(ctx, 1, 0, s);
+            rc = launch_grid_update_list<true>(ctx, Lrec, s);
+            timing_mark(ctx, 1, 1, s);
+            if (rc) return rc;
+        }
         AdjG2PArgs ag;
         ag.P = Pk;
-        ag.Fe = Fe;
+        ag.Fe = Fk;
         ag.M = Mw;
         ag.Gn = Gp;
         ag.L = Lk;

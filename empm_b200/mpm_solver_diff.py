@@ -89,6 +89,7 @@ class MPMWARPDiff(object):
         self.g2p_tile = False
         self.tile_cap = 1024
         self.seg_cap = 4           # warp-aggregated P2G: longest same-cell run per reduction
+        self.adj_store = True      # adjoint keeps each substep's grid and elastic F instead of recomputing
 
     def initialize(self, n_particles, n_grid=100, grid_lim=1.0, device="cuda:0"):
         self.n_particles = n_particles
@@ -157,7 +158,7 @@ class MPMWARPDiff(object):
             c.set_params(params)
         c.set_options({N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_MODE: int(self.p2g_mode),
                        N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap),
-                       N.OPT_SEG_CAP: int(self.seg_cap)})
+                       N.OPT_SEG_CAP: int(self.seg_cap), N.OPT_ADJ_STORE: int(bool(self.adj_store))})
         return c
 
     @staticmethod

@@ -192,10 +192,12 @@ def capacity_for_budget(hbm_budget: int, max_instances: int = 64, grid_share: fl
                         adjoint_grid: int = 160, every: int = 50) -> Capacity:
     """Split an HBM budget (bytes) between the forward arena, the grids, the
     checkpoint pool and the adjoint engine (segment states of up to `every`
-    substeps, its own grids and sorted buffers)."""
+    substeps, its own grids and sorted buffers, and the per-substep store of
+    touched grid blocks and elastic F that its reverse pass reads)."""
     adj_blocks = grid_blocks(adjoint_grid)
     adjoint = adjoint_particles * ((every + 1) * 104 + every * 12 + 2 * 104 + 3 * 36 + 64 +
                                    SORTED_BYTES_PER_PARTICLE) + adj_blocks * 4 * 64 * 16
+    adjoint += every * (adj_blocks * (128 * 16 + 4) + adjoint_particles * 36)
     rest = hbm_budget - adjoint
     if rest <= 0:
         raise ValueError("HBM budget too small for the adjoint engine")

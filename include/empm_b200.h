@@ -268,6 +268,11 @@ int  empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMa
 #define EMPM_OPT_SEG_CAP     5   /* warp-aggregated P2G: same-cell runs longer than this (a power of two,
                                     1..32 lanes) are split, trading shuffle rounds for grid reductions
                                     (default 4) */
+#define EMPM_OPT_ADJ_STORE   6   /* empm_adjoint_segment: 1 = keep every substep's touched grid blocks and
+                                    elastic F from the segment's forward pass for the reverse pass (default;
+                                    n_steps x (2 KiB per grid block + 36 B per particle) of device memory,
+                                    recompute when that allocation fails); 0 = recompute P2G and the grid
+                                    update in the reverse pass */
 
 int  empm_ctx_set_option(EmpmCtx* ctx, int option, int value);
 
