@@ -844,8 +844,10 @@ def run_ours_c3(args):
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n * (12 + 12 + 4 + 4),
                 "d2h_bytes_per_step": n * 12 + 12,
                 "path": "MPMDifferentiableSimulation.apply + loss.backward() with pinned host inputs"},
-        # forward: 3 kernels per substep (+ sorts); adjoint: 3 forward + 2 recompute + 3 adjoint kernels per substep
-        "gpu_launches": 11 * w.T * args.steps,
+        # per substep, not counting the cell sorts: the checkpointed forward's 4 (P2G, block list, grid update,
+        # G2P); the segment re-run's 6 with the grid store (the 4, grid save, grid clear) and the reverse pass's
+        # 4 (grid restore, the 3 adjoint kernels), or 4 + 3 recomputing + 3 without the store
+        "gpu_launches": 14 * w.T * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)

@@ -31,8 +31,17 @@
 #ifndef EMPM_ADJ_G2P_MIN_CTAS
 #define EMPM_ADJ_G2P_MIN_CTAS 6
 #endif
+// 1: the G2P adjoint's scatter loops over the outer stencil axis at run time
+#ifndef EMPM_ADJ_G2P_ROLL
+#define EMPM_ADJ_G2P_ROLL 1
+#endif
 #ifndef EMPM_ADJ_P2G_MIN_CTAS
-#define EMPM_ADJ_P2G_MIN_CTAS 3
+#define EMPM_ADJ_P2G_MIN_CTAS 4
+#endif
+// 1: the P2G adjoint's gather loops over the outer stencil axis at run time
+// (a third of the unrolled code, for the instruction cache)
+#ifndef EMPM_ADJ_P2G_ROLL
+#define EMPM_ADJ_P2G_ROLL 1
 #endif
 
 namespace empm {
@@ -126,8 +135,15 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     const V3 Q0 = c4 * col(gC, 0), Q1 = c4 * col(gC, 1), Q2 = c4 * col(gC, 2);
     V3 gxa = gxu - (c4 * c.inv_dx) * (transpose(gC) * o.v);
     const M3 gGvT = transpose(gGv);
+#if EMPM_ADJ_G2P_ROLL
+#pragma unroll 1
+#else
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+#endif
+    for (int i = 0; i < 3; ++i) {
+        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
+        const float ux = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        const V3 qi = q0 + (float)i * Q0;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
 #pragma unroll
@@ -140,10 +156,11 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
                 if (node_ok) {
                     const float4 g4 = __ldg(a.vel + addr);
                     const V3 vg = v3(g4.x, g4.y, g4.z);
-                    const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
+                    const float wy = st.w[1][j], wz = st.w[2][k];
+                    const float uy = st.dw[1][j], uz = st.dw[2][k];
                     const float w = wx * wy * wz;
-                    const V3 dw = c.inv_dx * v3(st.dw[0][i] * wy * wz, wx * st.dw[1][j] * wz, wx * wy * st.dw[2][k]);
-                    const V3 q = q0 + (float)i * Q0 + (float)j * Q1 + (float)k * Q2;
+                    const V3 dw = c.inv_dx * v3(ux * wy * wz, wx * uy * wz, wx * wy * uz);
+                    const V3 q = qi + (float)j * Q1 + (float)k * Q2;
                     gvg = w * q + gGv * dw;
                     gxa = gxa + dot(vg, q) * dw + idx2 * weight_hessian_times(st, i, j, k, gGvT * vg);
                 }
@@ -155,6 +172,7 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
                 }
                 if (head && node_ok) red_add_v4(a.gacc + addr, make_float4(gvg.x, gvg.y, gvg.z, 0.f));
             }
+    }
     if (live) {
         a.gx[p] = make_float4(gxa.x, gxa.y, gxa.z, 0.f);
         f9_store(a.gFe, p, gFe);
@@ -258,25 +276,36 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
     const float4 vv = __ldg(a.P.v + p);
     const V3 v = v3(vv.x, vv.y, vv.z);
     const float vol = __ldg(a.M.vol + p);
-
-    SpectralEval e;
-    spectral_eval(f9_load(a.P.F, p), __ldg(a.M.mu + p), __ldg(a.M.lam + p), __ldg(a.M.ys + p), dt, c.ms, e);
-    const M3 Sv = (-vol) * spectral_tau(e);
     const M3 Cd = damp_affine(f9_load(a.P.C, p), c.rpic);
 
+    // The gather runs before the constitutive evaluation, so that the SVD and
+    // its dual-number Jacobians are not held in registers across it. The
+    // stress enters the gather only through the force term's x derivative,
+    // sum_n H_n Sv^T gmv_n (H_n the weight Hessian); the gather keeps its
+    // moments sum_n H_n[pair] gmv_n and contracts them with Sv afterwards.
     const Stencil st = make_stencil(x, c.inv_dx);
     const bool in_grid = stencil_in_grid(st, c.G);
     const float dx = c.dx;
     const float idx2 = c.inv_dx * c.inv_dx;
-    const M3 SvT = transpose(Sv);
     V3 Wg = v3(0.f, 0.f, 0.f);      // sum w gmv
     M3 gCd = m3_zero();             // sum w gmv (x) dpos
     M3 gSv = m3_zero();             // sum gmv (x) dweight
     float gmass = 0.f;
     V3 gxa = v3(0.f, 0.f, 0.f);
-    const StencilAddr sa = stencil_addr(c.boff, c.NB, st.b);
+    V3 Hg[6];                       // sum H[pair] gmv, pairs xx, yy, zz, xy, xz, yz (grid units)
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+    for (int r = 0; r < 6; ++r) Hg[r] = v3(0.f, 0.f, 0.f);
+    const StencilAddr sa = stencil_addr(c.boff, c.NB, st.b);
+#if EMPM_ADJ_P2G_ROLL
+#pragma unroll 1
+#else
+#pragma unroll
+#endif
+    for (int i = 0; i < 3; ++i) {
+        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
+        const float ux = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        const float hx = bspline_d2(i);
+        const float px = ((float)i - st.fx[0]) * dx;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
 #pragma unroll
@@ -284,25 +313,34 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
                 if (!in_grid && !node_in_grid(st.b, i, j, k, c.G)) continue;
                 const float4 g4 = __ldg(a.gmom + sa.at(i, j, k));
                 const V3 gmv = v3(g4.x, g4.y, g4.z);
-                const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
+                const float wy = st.w[1][j], wz = st.w[2][k];
+                const float uy = st.dw[1][j], uz = st.dw[2][k];
                 const float w = wx * wy * wz;
-                const V3 dw = c.inv_dx * v3(st.dw[0][i] * wy * wz, wx * st.dw[1][j] * wz, wx * wy * st.dw[2][k]);
-                const V3 dpos = v3(((float)i - st.fx[0]) * dx, ((float)j - st.fx[1]) * dx, ((float)k - st.fx[2]) * dx);
+                const V3 dw = c.inv_dx * v3(ux * wy * wz, wx * uy * wz, wx * wy * uz);
+                const V3 dpos = v3(px, ((float)j - st.fx[1]) * dx, ((float)k - st.fx[2]) * dx);
                 const float s = g4.w + dot(gmv, v + Cd * dpos);
                 gmass += w * s;
                 Wg = Wg + w * gmv;
                 gCd = gCd + outer(w * gmv, dpos);
                 gSv = gSv + outer(gmv, dw);
-                gxa = gxa + (mass * s) * dw + (dt * idx2) * weight_hessian_times(st, i, j, k, SvT * gmv);
+                gxa = gxa + (mass * s) * dw;
+                Hg[0] = Hg[0] + (hx * wy * wz) * gmv;
+                Hg[1] = Hg[1] + (wx * bspline_d2(j) * wz) * gmv;
+                Hg[2] = Hg[2] + (wx * wy * bspline_d2(k)) * gmv;
+                Hg[3] = Hg[3] + (ux * uy * wz) * gmv;
+                Hg[4] = Hg[4] + (ux * wy * uz) * gmv;
+                Hg[5] = Hg[5] + (wx * uy * uz) * gmv;
             }
+    }
     gxa = gxa - mass * (transpose(Cd) * Wg);
-    V3 gv = mass * Wg;
-    gCd = mass * gCd;
-    const M3 g_tau = (-vol * dt) * gSv;
-    M3 gC = m3_zero();
-    if (!(c.rpic < -0.001f)) gC = (1.f - c.rpic) * gCd + (c.rpic / 2.f) * (gCd - transpose(gCd));
 
-    const SpectralGrad sg = spectral_adjoint(e, f9_load(a.gFe, p), g_tau, a.g_mu[p], a.g_lam[p], a.g_ys[p]);
+    V3 gv = mass * Wg;
+    {
+        gCd = mass * gCd;
+        M3 gC = m3_zero();
+        if (!(c.rpic < -0.001f)) gC = (1.f - c.rpic) * gCd + (c.rpic / 2.f) * (gCd - transpose(gCd));
+        f9_store(a.G.C, p, gC);
+    }
 
     // velocity modifiers, in reverse order (mpm_solver_diff.py:977-991, 1022-1036,
     // 1098-1142, 1198-1212, 1332-1348, 1391-1410). A modifier that overwrites v
@@ -329,15 +367,31 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
             }
         }
     }
-    const float4 gxg = __ldg(a.gx + p);
-    a.G.x[p] = make_float4(gxa.x + gxg.x, gxa.y + gxg.y, gxa.z + gxg.z, 0.f);
     a.G.v[p] = make_float4(gv.x, gv.y, gv.z, 0.f);
-    f9_store(a.G.C, p, gC);
+    a.g_mass[p] += gmass;
+    const M3 g_tau = (-vol * dt) * gSv;
+
+    SpectralEval e;
+    spectral_eval(f9_load(a.P.F, p), __ldg(a.M.mu + p), __ldg(a.M.lam + p), __ldg(a.M.ys + p), dt, c.ms, e);
+    {
+        // sum_n H_n Sv^T gmv_n, component a = sum_b dot(column b of Sv, sum_n H_n[a][b] gmv_n)
+        const M3 Sv = (-vol) * spectral_tau(e);
+        const V3 c0 = v3(Sv.m[0], Sv.m[3], Sv.m[6]);
+        const V3 c1 = v3(Sv.m[1], Sv.m[4], Sv.m[7]);
+        const V3 c2 = v3(Sv.m[2], Sv.m[5], Sv.m[8]);
+        const V3 hS = v3(dot(c0, Hg[0]) + dot(c1, Hg[3]) + dot(c2, Hg[4]),
+                         dot(c0, Hg[3]) + dot(c1, Hg[1]) + dot(c2, Hg[5]),
+                         dot(c0, Hg[4]) + dot(c1, Hg[5]) + dot(c2, Hg[2]));
+        gxa = gxa + (dt * idx2) * hS;
+        const float4 gxg = __ldg(a.gx + p);
+        a.G.x[p] = make_float4(gxa.x + gxg.x, gxa.y + gxg.y, gxa.z + gxg.z, 0.f);
+    }
+
+    const SpectralGrad sg = spectral_adjoint(e, f9_load(a.gFe, p), g_tau, a.g_mu[p], a.g_lam[p], a.g_ys[p]);
     f9_store(a.G.F, p, sg.gFt);
     a.g_mu[p] = sg.g_mu;
     a.g_lam[p] = sg.g_lam;
     a.g_ys[p] = sg.g_ys;
-    a.g_mass[p] += gmass;
 }
 
 // dL/dE, dL/dnu from dL/dmu, dL/dlam (compute_mu_lam_from_E_nu, mpm_utils.py:277-283),
