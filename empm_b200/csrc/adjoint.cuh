@@ -72,6 +72,7 @@ struct AdjG2PArgs {
     float4*        gacc;   // node velocity adjoint (accumulated here)
     float4*        gx;     // out: x adjoint through G2P
     F9Planes       gFe;    // out: F_elastic adjoint
+    int            seg_cap;  // longest same-cell run summed with shuffles (a power of two)
 };
 
 // Lanes whose particles share an instance and base cell (contiguous in cell
@@ -104,12 +105,19 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
               u2 = __shfl_up_sync(0xffffffffu, b2, 1);
     const int uv = __shfl_up_sync(0xffffffffu, (int)valid, 1);
     const int ui = __shfl_up_sync(0xffffffffu, inst, 1);
-    const bool head = lane == 0 || uv != (int)valid || ui != inst || u0 != b0 || u1 != b1 || u2 != b2;
+    const bool run_head = lane == 0 || uv != (int)valid || ui != inst || u0 != b0 || u1 != b1 || u2 != b2;
+    // runs longer than seg_cap (a power of two) get another head every seg_cap
+    // lanes, as in k_p2g_warpagg
+    const unsigned run_heads = __ballot_sync(0xffffffffu, run_head);
+    const int run_start = 31 - __clz(run_heads & (0xffffffffu >> (31 - lane)));
+    const bool head = run_head || ((lane - run_start) & (a.seg_cap - 1)) == 0;
     const unsigned heads = __ballot_sync(0xffffffffu, head);
     const unsigned above = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
     const int end = above ? (__ffs(above) - 2) : 31;
     const int seglen = head ? end - lane + 1 : 1;
     const int maxlen = __reduce_max_sync(0xffffffffu, seglen);
+    const unsigned take = (lane + 1 <= end ? 1u : 0u) | (lane + 2 <= end ? 2u : 0u) | (lane + 4 <= end ? 4u : 0u) |
+                          (lane + 8 <= end ? 8u : 0u) | (lane + 16 <= end ? 16u : 0u);
 
     // x' = clamp(x + dt v'): the clamp passes the adjoint only strictly inside the band
     const float dx = 1.f / c.inv_dx;
@@ -164,11 +172,16 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
                     gvg = w * q + gGv * dw;
                     gxa = gxa + dot(vg, q) * dw + idx2 * weight_hessian_times(st, i, j, k, gGvT * vg);
                 }
-                for (int d = 1; d < maxlen; d <<= 1) {
-                    const float tx = __shfl_down_sync(0xffffffffu, gvg.x, d);
-                    const float ty = __shfl_down_sync(0xffffffffu, gvg.y, d);
-                    const float tz = __shfl_down_sync(0xffffffffu, gvg.z, d);
-                    if (lane + d <= end) { gvg.x += tx; gvg.y += ty; gvg.z += tz; }
+                // reduction rounds unrolled, each skipped by a warp-uniform branch
+#pragma unroll
+                for (int r = 0; r < 5; ++r) {
+                    const int d = 1 << r;
+                    if (d < maxlen) {
+                        const float tx = __shfl_down_sync(0xffffffffu, gvg.x, d);
+                        const float ty = __shfl_down_sync(0xffffffffu, gvg.y, d);
+                        const float tz = __shfl_down_sync(0xffffffffu, gvg.z, d);
+                        if (take & (1u << r)) { gvg.x += tx; gvg.y += ty; gvg.z += tz; }
+                    }
                 }
                 if (head && node_ok) red_add_v4(a.gacc + addr, make_float4(gvg.x, gvg.y, gvg.z, 0.f));
             }

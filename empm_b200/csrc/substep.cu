@@ -1291,6 +1291,7 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         ag.gacc = ab.gacc;
         ag.gx = ab.gx;
         ag.gFe = gFe;
+        ag.seg_cap = ctx->seg_cap;
         timing_mark(ctx, 3, 0, s);
         k_adj_g2p<<<blocks_for(n, 128), 128, 0, s>>>(ag);
         timing_mark(ctx, 3, 1, s);
