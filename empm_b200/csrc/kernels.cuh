@@ -541,8 +541,14 @@ __global__ void k_unsort(const UnsortArgs a) {
 // segment of the warp (cell-sorted order); for each of the 27 stencil nodes
 // the segment's contributions are summed with shuffles and only the segment
 // head issues the 16-byte reduction to the grid.
+//
+// Same-cell runs are split every seg_cap = 2^ROUNDS lanes, so a segment sums
+// in at most ROUNDS shuffle rounds; the rounds a run cap never needs are not
+// compiled in (smaller code for the instruction cache).
+template <int ROUNDS>
 __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
-                                                     float4* grid, unsigned char* flags, int seg_cap) {
+                                                     float4* grid, unsigned char* flags) {
+    constexpr int seg_cap = 1 << ROUNDS;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const int inst = p < L.n_total ? find_instance_particle(L, p) : 0;
@@ -586,11 +592,12 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
     // tests are formed once instead of per node. The node address is formed
     // only in the head lanes (keeping precomputed per-axis address terms live
     // across the 27 nodes measured slower here).
-    const unsigned take = (lane + 1 <= end ? 1u : 0u) | (lane + 2 <= end ? 2u : 0u) | (lane + 4 <= end ? 4u : 0u) |
-                          (lane + 8 <= end ? 8u : 0u) | (lane + 16 <= end ? 16u : 0u);
+    unsigned take = 0;
+#pragma unroll
+    for (int r = 0; r < ROUNDS; ++r) take |= lane + (1 << r) <= end ? 1u << r : 0u;
     p2g_emit(pre, [&](int i, int j, int k, float4 v) {
 #pragma unroll
-        for (int r = 0; r < 5; ++r) {
+        for (int r = 0; r < ROUNDS; ++r) {
             const int d = 1 << r;
             if (d < maxlen) {
                 const float tx = __shfl_down_sync(0xffffffffu, v.x, d);
@@ -604,6 +611,20 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
             red_add_v4(grid + gaddr(c, q.st.b[0] + i, q.st.b[1] + j, q.st.b[2] + k), v);
     });
     if (head && valid) mark_stencil_blocks(flags, q.st, c);
+}
+
+// k_p2g_warpagg for a run cap seg_cap (a power of two in 1..32)
+static inline void launch_p2g_warpagg(int grid_ctas, int threads, cudaStream_t s, const ParticleArrays& P,
+                                      const MaterialArrays& M, const F9Planes& Fe, const Launch& L, float4* mom,
+                                      unsigned char* flags, int seg_cap) {
+    switch (seg_cap) {
+        case 1: k_p2g_warpagg<0><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;
+        case 2: k_p2g_warpagg<1><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;
+        case 4: k_p2g_warpagg<2><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;
+        case 8: k_p2g_warpagg<3><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;
+        case 16: k_p2g_warpagg<4><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;
+        default: k_p2g_warpagg<5><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;
+    }
 }
 
 // -------------------------------------------------------------------------

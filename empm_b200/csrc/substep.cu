@@ -720,8 +720,8 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaS
     timing_mark(ctx, 0, 0, stream);
     if (ctx->p2g_mode == 2) {
         const int tp = particle_threads(ctx, n, 256);
-        k_p2g_warpagg<<<blocks_for(n, tp), tp, 0, stream>>>(t.P, t.M, t.Fe, t.L, ctx->grid_mom, ctx->flags,
-                                                              ctx->seg_cap);
+        launch_p2g_warpagg(blocks_for(n, tp), tp, stream, t.P, t.M, t.Fe, t.L, ctx->grid_mom, ctx->flags,
+                           ctx->seg_cap);
     } else {
         k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
     }
@@ -1093,7 +1093,7 @@ static int launch_substep_arrays(EmpmCtx* ctx, const ParticleArrays& Pin, const 
     const int n = ctx->n_particles;
     const Launch L = make_launch(ctx, table);
     timing_mark(ctx, 0, 0, s);
-    if (warpagg) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags, ctx->seg_cap);
+    if (warpagg) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, M, Fe, L, ctx->grid_mom, ctx->flags, ctx->seg_cap);
     else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags);
     timing_mark(ctx, 0, 1, s);
     CK(cudaGetLastError(), "adjoint segment P2G");
@@ -1236,8 +1236,8 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         const F9Planes Fk = fe_slot(k);
         const Launch Lk = make_launch(ctx, k);
         timing_mark(ctx, 0, 0, s);
-        if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
-                                                                     ctx->seg_cap);
+        if (sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
+                                       ctx->seg_cap);
         else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
         timing_mark(ctx, 0, 1, s);
         CK(cudaGetLastError(), "adjoint segment P2G");
@@ -1271,8 +1271,8 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
             CK(cudaGetLastError(), "k_restore_grid");
         } else {
             timing_mark(ctx, 0, 0, s);
-            if (sorted) k_p2g_warpagg<<<blocks_for(n, 256), 256, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags,
-                                                                         ctx->seg_cap);
+            if (sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags,
+                                           ctx->seg_cap);
             else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
             timing_mark(ctx, 0, 1, s);
             CK(cudaGetLastError(), "P2G (adjoint recompute)");
