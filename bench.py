@@ -694,10 +694,14 @@ def run_ours_c3(args):
         md.yield_stress.copy_(init["ys"])
         solver.time = 0.0
 
+    tape_store = None if args.tape_store is None else bool(args.tape_store)
+    stored = []
+
     def grad_step():
         reset()
-        tape = CheckpointedRollout(solver, md, st, w.dt, w.T, checkpoint_every=every)
+        tape = CheckpointedRollout(solver, md, st, w.dt, w.T, checkpoint_every=every, store=tape_store)
         final = tape.forward()
+        stored.append(tape.stored)
         diff = final.particle_x - x_target
         res = tape.backward(g_x=2.0 * diff / n)
         g_E, g_nu, _ = prepare_adjoint(md.E, md.nu, res["mu"], res["lam"])
@@ -826,8 +830,10 @@ def run_ours_c3(args):
                    "particles": n, "grid": w.G, "substeps_per_step": w.T, "dt": w.dt,
                    "step": "checkpointed forward + adjoint of every substep (gradients in x0, v0, C0, F0, "
                            "mu, lam, yield, mass; E and nu through the prepare adjoint)",
-                   "reverse_pass": "reads each substep's stored grid and elastic F" if solver.adj_store
-                   else "recomputes each substep's P2G and grid update",
+                   "reverse_pass": ("segments stored by the forward pass (no re-run)" if stored[-1] else
+                                    "checkpoints, each segment re-run " +
+                                    ("keeping its grids and elastic F" if solver.adj_store
+                                     else "and its grids recomputed")),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (segment states ~0.5 GB > 126 MB), no flush",
                    "forward_ms": fwd_ms, "gradient_over_forward": (ms / args.steps) / fwd_ms,
@@ -844,10 +850,10 @@ def run_ours_c3(args):
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n * (12 + 12 + 4 + 4),
                 "d2h_bytes_per_step": n * 12 + 12,
                 "path": "MPMDifferentiableSimulation.apply + loss.backward() with pinned host inputs"},
-        # per substep, not counting the cell sorts: the checkpointed forward's 4 (P2G, block list, grid update,
-        # G2P); the segment re-run's 6 with the grid store (the 4, grid save, grid clear) and the reverse pass's
-        # 4 (grid restore, the 3 adjoint kernels), or 4 + 3 recomputing + 3 without the store
-        "gpu_launches": 14 * w.T * args.steps,
+        # per substep, not counting the cell sorts and permutations: with stored segments the forward's 6 (P2G,
+        # block list, grid update, grid save, grid clear, G2P) and the reverse pass's 4 (grid restore, the 3
+        # adjoint kernels); with checkpoints also the plain forward's 4 before them
+        "gpu_launches": (10 if stored[-1] else 14) * w.T * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -1265,6 +1271,8 @@ def main():
     ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
     ap.add_argument("--seg-cap", dest="seg_cap", type=int, default=None,
                     help="warp-aggregated P2G: longest same-cell run per reduction (4, 8, 16, 32)")
+    ap.add_argument("--tape-store", dest="tape_store", type=int, default=None,
+                    help="c3: 1 = the forward pass stores every segment, 0 = checkpoints (default: store when it fits)")
     ap.add_argument("--adj-store", dest="adj_store", type=int, default=None,
                     help="c3: 1 = the reverse pass reads each substep's stored grid and elastic F, 0 = recomputes them")
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",

@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libempm_b200.so")
 
 EMPM_OK = 0
+EMPM_ERR_INVALID, EMPM_ERR_CUDA, EMPM_ERR_OOM, EMPM_ERR_UNSUPPORTED = -1, -2, -3, -4
 EMPM_MAX_COLLIDERS = 16
 EMPM_MAX_MODIFIERS = 8
 EMPM_STATUS_NAN, EMPM_STATUS_CFL, EMPM_STATUS_OUT_OF_BAND = 1, 2, 4
@@ -121,6 +122,12 @@ def lib():
         "empm_adjoint_segment": ([P, ctypes.POINTER(EmpmParticles), P, P, P, ctypes.POINTER(EmpmMaterial), P, I,
                                   ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterialGrad), P], I),
         "empm_prepare_adjoint": ([P, P, P, P, P, P, P, P, P, I, P], I),
+        "empm_segment_bytes": ([P, I, ctypes.POINTER(ctypes.c_size_t)], I),
+        "empm_segment_create": ([P, I, ctypes.POINTER(P)], I),
+        "empm_segment_destroy": ([P], I),
+        "empm_segment_forward": ([P, P, ctypes.POINTER(EmpmParticles), P, P, P, ctypes.POINTER(EmpmMaterial), P, I,
+                                  ctypes.POINTER(EmpmParticles), P], I),
+        "empm_segment_reverse": ([P, P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterialGrad), P], I),
         "empm_chamfer": ([P, P, I, I, P, P, I, I, I, P, P, P, P, P], I),
         "empm_restart_F": ([P, ctypes.POINTER(EmpmParticles), P, P, P, P], I),
         "empm_chamfer_backward": ([P, P, I, P, P, I, I, P, P, P, P, P, P, P], I),

@@ -86,6 +86,22 @@ class _Checkpoint:
         return N.EmpmParticles(self.x4.data_ptr(), self.v4.data_ptr(), self.C.data_ptr(), self.F.data_ptr())
 
 
+class _StoredSegment:
+    """A segment kept on the device by empm_segment_forward for its reverse
+    pass. Released segments go back to their context's pool."""
+
+    def __init__(self, ctx, ptr: ctypes.c_void_p, step: int, n_steps: int):
+        self.ctx = ctx
+        self.ptr = ptr
+        self.step = step
+        self.n_steps = n_steps
+
+    def release(self) -> None:
+        if self.ptr is not None:
+            self.ctx.give_segment(self.ptr, self.n_steps)
+        self.ptr = None
+
+
 class CheckpointedRollout:
     """Forward rollout that can be differentiated afterwards.
 
@@ -93,10 +109,21 @@ class CheckpointedRollout:
     ``i % record_every == 0`` (the Trail function's recording). Segments end at
     those substeps, so the adjoint of a record is injected exactly where the
     record was taken.
+
+    Segments are either stored or checkpointed. A stored segment keeps, from
+    the forward pass, everything its reverse pass reads (empm_segment_*). The
+    reverse pass then runs only the adjoint kernels, as Warp's tape replays the
+    recorded launches. A checkpointed segment keeps its start state, and its
+    reverse pass recomputes it first (empm_adjoint_segment). ``store``: True
+    stores every segment and raises MemoryError when they do not fit; False
+    checkpoints. None stores when the whole rollout fits ``store_budget`` bytes
+    (default: half of the device memory free at the forward pass) and the
+    allocation succeeds, and checkpoints otherwise.
     """
 
     def __init__(self, solver, model: MPMModelStruct, state: MPMStateStruct, dt: float, n_steps: int,
-                 checkpoint_every: int = 20, record_every: Optional[int] = None, step_callback=None):
+                 checkpoint_every: int = 20, record_every: Optional[int] = None, step_callback=None,
+                 store: Optional[bool] = None, store_budget: Optional[int] = None):
         if n_steps < 1:
             raise ValueError("n_steps must be >= 1")
         if checkpoint_every < 1:
@@ -109,9 +136,69 @@ class CheckpointedRollout:
         self.record_steps: List[int] = [] if record_every is None else list(range(0, self.n_steps, int(record_every)))
         self.step_callback = step_callback
         self.state = state
+        self.store = store
+        self.store_budget = store_budget
         self.records: List[Tensor] = []
         self.ckpts: List[_Checkpoint] = []
+        self.segments: List[_StoredSegment] = []
         self.final: Optional[MPMStateStruct] = None
+
+    @property
+    def stored(self) -> bool:
+        """True when the forward pass stored its segments."""
+        return bool(self.segments)
+
+    def release(self) -> None:
+        """Free the stored segments (a later backward is then impossible)."""
+        for sg in self.segments:
+            sg.release()
+        self.segments = []
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:   # interpreter shutdown: the library may be gone
+            pass
+
+    def _allocate_segments(self, ctx, dev) -> bool:
+        """Stored segments for every segment of the rollout, or False (nothing
+        kept) when they exceed the budget or do not fit."""
+        if self.store is False:
+            return False
+        L = N.lib()
+        lengths = [s1 - s0 for s0, s1 in zip(self.bounds[:-1], self.bounds[1:])]
+        total = new = 0
+        nb = ctypes.c_size_t()
+        for n_seg in set(lengths):
+            N.check(L.empm_segment_bytes(ctx.ptr, n_seg, ctypes.byref(nb)), ctx.ptr)
+            total += nb.value * lengths.count(n_seg)
+            new += nb.value * max(0, lengths.count(n_seg) - ctx.pooled(n_seg))
+        budget = self.store_budget
+        if budget is None:
+            # segments already in the pool count as available
+            budget = torch.cuda.mem_get_info(dev)[0] // 2 + (total - new)
+        if total > budget:
+            if self.store:
+                raise MemoryError(f"storing the rollout needs {total} bytes, over the budget of {budget}")
+            return False
+        segs = []
+        for s0, n_seg in zip(self.bounds[:-1], lengths):
+            p = ctx.take_segment(n_seg)
+            if p is None:
+                p = ctypes.c_void_p()
+                with torch.cuda.device(dev):
+                    rc = L.empm_segment_create(ctx.ptr, n_seg, ctypes.byref(p))
+                if rc != N.EMPM_OK:
+                    for sg in segs:
+                        sg.release()
+                    if rc == N.EMPM_ERR_OOM and not self.store:
+                        return False
+                    if rc == N.EMPM_ERR_OOM:
+                        raise MemoryError(N.last_error(ctx.ptr))
+                    N.check(rc, ctx.ptr)
+            segs.append(_StoredSegment(ctx, p, s0, n_seg))
+        self.segments = segs
+        return True
 
     def _bounds(self) -> List[int]:
         b = set(range(0, self.n_steps, self.every))
@@ -129,21 +216,37 @@ class CheckpointedRollout:
         for _ in range(self.n_steps):
             times.append(times[-1] + self.dt)
         self.bounds = self._bounds()
+        self.release()
+        self.ckpts = []
+        self.records = []
+        store = self._allocate_segments(ctx, st.device)
         a = st.partial_clone(requires_grad=False)
         for src, dst in ((st._x4, a._x4), (st._v4, a._v4), (st._C, a._C), (st._F_trial, a._F_trial)):
             dst.copy_(src)
         b = st.partial_clone(requires_grad=False)
         cur, other = a, b
         record_set = set(self.record_steps)
-        for s0, s1 in zip(self.bounds[:-1], self.bounds[1:]):
-            self.ckpts.append(_Checkpoint(s0, cur._x4.clone(), cur._v4.clone(), cur._C.clone(), cur._F_trial.clone(),
-                                          model.mu.clone(), model.lam.clone(), model.yield_stress.clone()))
+        stream = _stream_ptr(st.device)
+        for i, (s0, s1) in enumerate(zip(self.bounds[:-1], self.bounds[1:])):
             L = s1 - s0
             seg = (N.EmpmStep * L).from_buffer(self.table, s0 * ctypes.sizeof(N.EmpmStep))
             solver.time = times[s0]
-            res = solver.rollout(model, cur, other, self.dt, L, schedule=(seg, times[s1]))
-            if res is not cur:
+            if store:
+                mat = N.EmpmMaterial(cur.particle_vol.data_ptr(), model.mu.data_ptr(), model.lam.data_ptr(),
+                                     model.yield_stress.data_ptr(), cur._sel_ptr(), other._F.data_ptr())
+                with torch.cuda.device(st.device):
+                    N.check(N.lib().empm_segment_forward(ctx.ptr, self.segments[i].ptr, cur._particles(),
+                                                         model.mu.data_ptr(), model.lam.data_ptr(),
+                                                         model.yield_stress.data_ptr(), mat, seg, L,
+                                                         other._particles(), stream), ctx.ptr)
                 cur, other = other, cur
+            else:
+                self.ckpts.append(_Checkpoint(s0, cur._x4.clone(), cur._v4.clone(), cur._C.clone(),
+                                              cur._F_trial.clone(), model.mu.clone(), model.lam.clone(),
+                                              model.yield_stress.clone()))
+                res = solver.rollout(model, cur, other, self.dt, L, schedule=(seg, times[s1]))
+                if res is not cur:
+                    cur, other = other, cur
             if (s1 - 1) in record_set:
                 self.records.append(cur.particle_x.clone())
         solver.time = t_end
@@ -173,6 +276,15 @@ class CheckpointedRollout:
         ctx = self.solver._context(model, n, dev, max_steps=self.n_steps)
         L = N.lib()
         stream = _stream_ptr(dev)
+        if self.segments:
+            for sg, s1 in reversed(list(zip(self.segments, self.bounds[1:]))):
+                r = rec_index.get(s1 - 1)
+                if r is not None and g_records is not None and g_records[r] is not None:
+                    grad.add(g_x=g_records[r])
+                with torch.cuda.device(dev):
+                    N.check(L.empm_segment_reverse(ctx.ptr, sg.ptr, grad.particles(), gmat, stream), ctx.ptr)
+            return {"x": grad.x(), "v": grad.v(), "C": grad.C_mat(), "F": grad.F_mat(), "mu": g_mu, "lam": g_lam,
+                    "yield_stress": g_ys, "mass": g_mass}
         for ck, s1 in reversed(list(zip(self.ckpts, self.bounds[1:]))):
             r = rec_index.get(s1 - 1)
             if r is not None and g_records is not None and g_records[r] is not None:

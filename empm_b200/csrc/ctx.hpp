@@ -122,5 +122,26 @@ struct EmpmCtx {
     char         err[512] = {0};
 };
 
+// A segment of a differentiable rollout kept on the device from its forward
+// pass (empm_segment_forward) to its reverse pass (empm_segment_reverse): the
+// state before every substep, the mu / lam / yield snapshots, each substep's
+// touched grid blocks and elastic F, vol / selection / caller index in the
+// order it ran in, and its step tables.
+struct EmpmSegment {
+    EmpmCtx* ctx = nullptr;
+    int      n = 0, n_steps = 0, n_inst = 0;
+    size_t   np = 0, cap_blocks = 0;
+    bool     sorted = false, has_sel = false, ready = false;
+    float*   states = nullptr;    // (n_steps + 1) packed states
+    float*   mats = nullptr;      // n_steps x (mu | lam | yield)
+    float4*  gsave = nullptr;     // n_steps x cap_blocks x 128 float4
+    int*     glist = nullptr;     // n_steps x (1 + cap_blocks)
+    float*   fe = nullptr;        // n_steps x f9 planes
+    float*   vol = nullptr;       // [np]
+    int*     sel = nullptr;       // [np]
+    int*     pid = nullptr;       // [np] caller index of each position (cell order)
+    std::vector<EmpmStep> tables;
+};
+
 int empm_set_error(EmpmCtx* ctx, int code, const char* fmt, ...);
 int empm_check_cuda(EmpmCtx* ctx, cudaError_t e, const char* what);

@@ -1106,6 +1106,186 @@ static int launch_substep_arrays(EmpmCtx* ctx, const ParticleArrays& Pin, const 
     return EMPM_OK;
 }
 
+// Where a segment's forward data lives, for its reverse pass: the state
+// before every substep, mu / lam / yield snapshots, and with the store each
+// substep's touched grid blocks and elastic F; vol, selection and caller
+// index in the order the segment runs in.
+struct SegmentData {
+    int n = 0, n_steps = 0;
+    size_t np = 0;
+    bool sorted = false;
+    bool store = false;
+    float* states = nullptr;   // (n_steps + 1) packed states
+    float* mats = nullptr;     // n_steps x (mu | lam | yield)
+    float4* gsave = nullptr;   // n_steps x cap_blocks x 128 float4
+    int* glist = nullptr;      // n_steps x (1 + cap_blocks)
+    float* fe = nullptr;       // n_steps x f9 planes
+    size_t cap_blocks = 0;
+    MaterialArrays base;
+};
+
+// Forward over the segment from d.states[0] with mu / lam / yield in the
+// adjoint work arrays (updated in place), keeping the state before every
+// substep and the material snapshots. The last substep runs too, although
+// the state after it is only needed by the caller: its P2G writes the
+// velocity modifiers into that substep's stored velocities, which the reverse
+// pass reads. With the store, P2G writes each substep's elastic F straight
+// into its store slot and the touched grid blocks are saved after the grid
+// update.
+static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
+    AdjointBuffers& ab = ctx->adj;
+    const int n = d.n;
+    const size_t np = d.np;
+    const size_t state_floats = 26 * np;
+    MaterialArrays Mw = d.base;
+    Mw.mu = ab.work;
+    Mw.lam = ab.work + np;
+    Mw.ys = ab.work + 2 * np;
+    const F9Planes Fe = f9_planes(ab.fe, n);
+    const int grid_ctas = ctx->sm_count * 8;
+    for (int k = 0; k < d.n_steps; ++k) {
+        CK(cudaMemcpyAsync(d.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, s),
+           "snapshot");
+        const ParticleArrays Pin = particle_arrays(d.states + (size_t)k * state_floats, n);
+        const ParticleArrays Pout = particle_arrays(d.states + (size_t)(k + 1) * state_floats, n);
+        if (!d.store) {
+            const int rc = launch_substep_arrays(ctx, Pin, Pout, Mw, Fe, k, d.sorted, s);
+            if (rc) return rc;
+            continue;
+        }
+        const F9Planes Fk = f9_planes(d.fe + (size_t)k * 9 * np, n);
+        const Launch Lk = make_launch(ctx, k);
+        timing_mark(ctx, 0, 0, s);
+        if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
+                                         ctx->seg_cap);
+        else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
+        timing_mark(ctx, 0, 1, s);
+        CK(cudaGetLastError(), "adjoint segment P2G");
+        timing_mark(ctx, 1, 0, s);
+        const int rc = launch_grid_update_list<true>(ctx, Lk, s);
+        if (rc) return rc;
+        k_save_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active,
+                                              d.gsave + (size_t)k * d.cap_blocks * 128,
+                                              d.glist + (size_t)k * (d.cap_blocks + 1));
+        CK(cudaGetLastError(), "k_save_grid");
+        k_clear_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->flags, ctx->active);
+        CK(cudaGetLastError(), "k_clear_grid");
+        timing_mark(ctx, 1, 1, s);
+        timing_mark(ctx, 2, 0, s);
+        k_g2p_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Fk, Mw, Pout, Lk, ctx->grid_vel);
+        timing_mark(ctx, 2, 1, s);
+        CK(cudaGetLastError(), "adjoint segment G2P");
+    }
+    return EMPM_OK;
+}
+
+// The reverse pass: for each substep from the last, its grid (restored from
+// the store, or recomputed from the stored state with the step tables
+// [n_steps, 2 n_steps) that omit the velocity modifiers), then the three
+// adjoint kernels; finally the adjoint back into the caller's order.
+// Gp / gm_*: the incoming adjoint in the segment's order (updated in place).
+static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp, float* gm_mu, float* gm_lam,
+                           float* gm_ys, float* gm_mass, EmpmParticles* grad, EmpmMaterialGrad* gmat,
+                           cudaStream_t s) {
+    AdjointBuffers& ab = ctx->adj;
+    const int n = d.n, n_steps = d.n_steps;
+    const size_t np = d.np;
+    const size_t state_floats = 26 * np;
+    MaterialArrays Mw = d.base;
+    Mw.mu = ab.work;
+    Mw.lam = ab.work + np;
+    Mw.ys = ab.work + 2 * np;
+    const F9Planes Fe = f9_planes(ab.fe, n);
+    const F9Planes gFe = f9_planes(ab.gfe, n);
+    const int grid_ctas = ctx->sm_count * 8;
+    long long nb = (ctx->nblocks + 3) / 4;
+    if (nb > grid_ctas) nb = grid_ctas;
+    for (int k = n_steps - 1; k >= 0; --k) {
+        float* snap = d.mats + (size_t)k * 3 * np;
+        const ParticleArrays Pk = particle_arrays(d.states + (size_t)k * state_floats, n);
+        const Launch Lk = make_launch(ctx, k);
+        F9Planes Fk = Fe;
+        if (d.store) {
+            Fk = f9_planes(d.fe + (size_t)k * 9 * np, n);
+            k_restore_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->flags,
+                                                     d.gsave + (size_t)k * d.cap_blocks * 128,
+                                                     d.glist + (size_t)k * (d.cap_blocks + 1));
+            CK(cudaGetLastError(), "k_restore_grid");
+        } else {
+            CK(cudaMemcpyAsync(ab.work, snap, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, s),
+               "restore snapshot");
+            const Launch Lrec = make_launch(ctx, n_steps + k);
+            timing_mark(ctx, 0, 0, s);
+            if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pk, Mw, Fe, Lrec, ctx->grid_mom,
+                                             ctx->flags, ctx->seg_cap);
+            else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
+            timing_mark(ctx, 0, 1, s);
+            CK(cudaGetLastError(), "P2G (adjoint recompute)");
+            timing_mark(ctx, 1, 0, s);
+            const int rc = launch_grid_update_list<true>(ctx, Lrec, s);
+            timing_mark(ctx, 1, 1, s);
+            if (rc) return rc;
+        }
+        AdjG2PArgs ag;
+        ag.P = Pk;
+        ag.Fe = Fk;
+        ag.M = Mw;
+        ag.Gn = Gp;
+        ag.L = Lk;
+        ag.vel = ctx->grid_vel;
+        ag.gacc = ab.gacc;
+        ag.gx = ab.gx;
+        ag.gFe = gFe;
+        ag.seg_cap = ctx->seg_cap;
+        timing_mark(ctx, 3, 0, s);
+        k_adj_g2p<<<blocks_for(n, 128), 128, 0, s>>>(ag);
+        timing_mark(ctx, 3, 1, s);
+        CK(cudaGetLastError(), "k_adj_g2p");
+        AdjGridArgs gg;
+        gg.mom = ctx->grid_mom;
+        gg.gacc = ab.gacc;
+        gg.gmom = ab.gmom;
+        gg.flags = ctx->flags;
+        gg.L = Lk;
+        timing_mark(ctx, 4, 0, s);
+        k_adj_grid<<<(int)nb, 256, 0, s>>>(gg);
+        timing_mark(ctx, 4, 1, s);
+        CK(cudaGetLastError(), "k_adj_grid");
+        AdjP2GArgs ap;
+        ap.P = Pk;
+        ap.M = Mw;
+        ap.M.mu = snap;
+        ap.M.lam = snap + np;
+        ap.M.ys = snap + 2 * np;
+        ap.L = Lk;
+        ap.gmom = ab.gmom;
+        ap.gx = ab.gx;
+        ap.gFe = gFe;
+        ap.G = Gp;
+        ap.g_mu = gm_mu;
+        ap.g_lam = gm_lam;
+        ap.g_ys = gm_ys;
+        ap.g_mass = gm_mass;
+        timing_mark(ctx, 5, 0, s);
+        k_adj_p2g<<<blocks_for(n, 128), 128, 0, s>>>(ap);
+        timing_mark(ctx, 5, 1, s);
+        CK(cudaGetLastError(), "k_adj_p2g");
+    }
+    if (d.sorted) {
+        GradPermuteArgs back;
+        back.src = Gp;
+        back.dst = particle_arrays(grad, n);
+        back.s_mu = gm_mu; back.s_lam = gm_lam; back.s_ys = gm_ys; back.s_mass = gm_mass;
+        back.d_mu = gmat->mu; back.d_lam = gmat->lam; back.d_ys = gmat->yield_stress; back.d_mass = gmat->mass;
+        back.pid = d.base.pid;
+        back.n = n;
+        back.to_sorted = 0;
+        k_permute_grad<<<blocks_for(n, 256), 256, 0, s>>>(back);
+        CK(cudaGetLastError(), "k_permute_grad");
+    }
+    return EMPM_OK;
+}
+
 extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* ckpt_mu,
                                     const float* ckpt_lam, const float* ckpt_yield, const EmpmMaterial* mat,
                                     const EmpmStep* steps, int n_steps, EmpmParticles* grad,
@@ -1206,141 +1386,263 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         CK(cudaMemcpyAsync(lam_w, ckpt_lam, sizeof(float) * n, d2d, s), "copy checkpoint");
         CK(cudaMemcpyAsync(ys_w, ckpt_yield, sizeof(float) * n, d2d, s), "copy checkpoint");
     }
-    MaterialArrays Mw = base;
-    Mw.mu = mu_w;
-    Mw.lam = lam_w;
-    Mw.ys = ys_w;
-    const F9Planes Fe = f9_planes(ab.fe, n);
-    const F9Planes gFe = f9_planes(ab.gfe, n);
+    SegmentData d;
+    d.n = n;
+    d.n_steps = n_steps;
+    d.np = np;
+    d.sorted = sorted;
+    d.store = ab.store_cap >= n_steps;
+    d.states = ab.states;
+    d.mats = ab.mats;
+    d.gsave = ab.gsave;
+    d.glist = ab.gsave_list;
+    d.fe = ab.fe_store;
+    d.cap_blocks = (size_t)ab.cap_blocks;
+    d.base = base;
+    rc = segment_forward(ctx, d, s);
+    if (rc) return rc;
+    return segment_reverse(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, grad, gmat, s);
+}
 
-    // 2. forward over the segment, keeping the state before every substep.
-    //    The last substep runs too, although the state after it is not needed:
-    //    its P2G writes the velocity modifiers into that substep's stored
-    //    velocities, which the recompute below (without modifiers) relies on.
-    //    With the store, each substep keeps its touched grid blocks and its
-    //    elastic F (P2G writes it straight into the substep's store slot).
-    const bool store = ab.store_cap >= n_steps;
-    const int grid_ctas = ctx->sm_count * 8;
-    auto fe_slot = [&](int k) { return f9_planes(ab.fe_store + (size_t)k * 9 * np, n); };
-    auto gsave_slot = [&](int k) { return ab.gsave + (size_t)k * (size_t)ab.cap_blocks * 128; };
-    auto glist_slot = [&](int k) { return ab.gsave_list + (size_t)k * ((size_t)ab.cap_blocks + 1); };
-    for (int k = 0; k < n_steps; ++k) {
-        CK(cudaMemcpyAsync(ab.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), d2d, s), "snapshot");
-        const ParticleArrays Pin = particle_arrays(ab.states + (size_t)k * state_floats, n);
-        const ParticleArrays Pout = particle_arrays(ab.states + (size_t)(k + 1) * state_floats, n);
-        if (!store) {
-            rc = launch_substep_arrays(ctx, Pin, Pout, Mw, Fe, k, sorted, s);
-            if (rc) return rc;
-            continue;
-        }
-        const F9Planes Fk = fe_slot(k);
-        const Launch Lk = make_launch(ctx, k);
-        timing_mark(ctx, 0, 0, s);
-        if (sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
-                                       ctx->seg_cap);
-        else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
-        timing_mark(ctx, 0, 1, s);
-        CK(cudaGetLastError(), "adjoint segment P2G");
-        timing_mark(ctx, 1, 0, s);
-        rc = launch_grid_update_list<true>(ctx, Lk, s);
-        if (rc) return rc;
-        k_save_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active, gsave_slot(k), glist_slot(k));
-        CK(cudaGetLastError(), "k_save_grid");
-        k_clear_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->flags, ctx->active);
-        CK(cudaGetLastError(), "k_clear_grid");
-        timing_mark(ctx, 1, 1, s);
-        timing_mark(ctx, 2, 0, s);
-        k_g2p_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Fk, Mw, Pout, Lk, ctx->grid_vel);
-        timing_mark(ctx, 2, 1, s);
-        CK(cudaGetLastError(), "adjoint segment G2P");
-    }
+// ---------------------------------------------------------------------------
+// stored segments: the forward keeps what the reverse pass needs
+// ---------------------------------------------------------------------------
+static size_t segment_bytes(size_t np, size_t cap_blocks, int n_steps) {
+    const size_t k = (size_t)n_steps;
+    return ((k + 1) * 26 * np + k * 3 * np + k * 9 * np + np) * sizeof(float) + 2 * np * sizeof(int) +
+           k * cap_blocks * 128 * sizeof(float4) + k * (cap_blocks + 1) * sizeof(int);
+}
 
-    // 3. substeps in reverse: recompute the grid, then the three adjoint kernels
-    long long nb = (ctx->nblocks + 3) / 4;
-    if (nb > ctx->sm_count * 8) nb = ctx->sm_count * 8;
-    for (int k = n_steps - 1; k >= 0; --k) {
-        float* snap = ab.mats + (size_t)k * 3 * np;
-        CK(cudaMemcpyAsync(ab.work, snap, 3 * np * sizeof(float), d2d, s), "restore snapshot");
-        const ParticleArrays Pk = particle_arrays(ab.states + (size_t)k * state_floats, n);
-        const Launch Lrec = make_launch(ctx, n_steps + k);
-        const Launch Lk = make_launch(ctx, k);
-        const F9Planes Fk = store ? fe_slot(k) : Fe;
-        if (store) {
-            k_restore_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->flags, gsave_slot(k),
-                                                     glist_slot(k));
-            CK(cudaGetLastError(), "k_restore_grid");
-        } else {
-            timing_mark(ctx, 0, 0, s);
-            if (sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags,
-                                           ctx->seg_cap);
-            else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
-            timing_mark(ctx, 0, 1, s);
-            CK(cudaGetLastError(), "P2G (adjoint recompute)");
-            timing_mark(ctx, 1, 0, s);
-            rc = launch_grid_update_list<true>(ctx, Lrec, s);
-            timing_mark(ctx, 1, 1, s);
-            if (rc) return rc;
-        }
-        AdjG2PArgs ag;
-        ag.P = Pk;
-        ag.Fe = Fk;
-        ag.M = Mw;
-        ag.Gn = Gp;
-        ag.L = Lk;
-        ag.vel = ctx->grid_vel;
-        ag.gacc = ab.gacc;
-        ag.gx = ab.gx;
-        ag.gFe = gFe;
-        ag.seg_cap = ctx->seg_cap;
-        timing_mark(ctx, 3, 0, s);
-        k_adj_g2p<<<blocks_for(n, 128), 128, 0, s>>>(ag);
-        timing_mark(ctx, 3, 1, s);
-        CK(cudaGetLastError(), "k_adj_g2p");
-        AdjGridArgs gg;
-        gg.mom = ctx->grid_mom;
-        gg.gacc = ab.gacc;
-        gg.gmom = ab.gmom;
-        gg.flags = ctx->flags;
-        gg.L = Lk;
-        timing_mark(ctx, 4, 0, s);
-        k_adj_grid<<<(int)nb, 256, 0, s>>>(gg);
-        timing_mark(ctx, 4, 1, s);
-        CK(cudaGetLastError(), "k_adj_grid");
-        AdjP2GArgs ap;
-        ap.P = Pk;
-        ap.M = Mw;
-        ap.M.mu = snap;
-        ap.M.lam = snap + np;
-        ap.M.ys = snap + 2 * np;
-        ap.L = Lk;
-        ap.gmom = ab.gmom;
-        ap.gx = ab.gx;
-        ap.gFe = gFe;
-        ap.G = Gp;
-        ap.g_mu = gm_mu;
-        ap.g_lam = gm_lam;
-        ap.g_ys = gm_ys;
-        ap.g_mass = gm_mass;
-        timing_mark(ctx, 5, 0, s);
-        k_adj_p2g<<<blocks_for(n, 128), 128, 0, s>>>(ap);
-        timing_mark(ctx, 5, 1, s);
-        CK(cudaGetLastError(), "k_adj_p2g");
-    }
+static void segment_free(EmpmSegment* seg) {
+    void* ptrs[] = {seg->states, seg->mats, seg->gsave, seg->glist, seg->fe, seg->vol, seg->sel, seg->pid};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    seg->states = seg->mats = seg->fe = seg->vol = nullptr;
+    seg->gsave = nullptr;
+    seg->glist = seg->sel = seg->pid = nullptr;
+}
 
-    // 4. outgoing adjoint back to the caller's order
-    if (sorted) {
-        GradPermuteArgs back;
-        back.src = Gp;
-        back.dst = particle_arrays(grad, n);
-        back.s_mu = gm_mu; back.s_lam = gm_lam; back.s_ys = gm_ys; back.s_mass = gm_mass;
-        back.d_mu = gmat->mu; back.d_lam = gmat->lam; back.d_ys = gmat->yield_stress; back.d_mass = gmat->mass;
-        back.pid = perm.pid;
-        back.n = n;
-        back.to_sorted = 0;
-        k_permute_grad<<<blocks_for(n, 256), 256, 0, s>>>(back);
-        CK(cudaGetLastError(), "k_permute_grad");
-    }
+extern "C" int empm_segment_bytes(EmpmCtx* ctx, int n_steps, size_t* out) {
+    if (!ctx || !out) return empm_set_error(ctx, EMPM_ERR_INVALID, "ctx or out is NULL");
+    if (n_steps < 1 || n_steps > 100000)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
+    *out = segment_bytes(padded4(ctx->n_particles), (size_t)ctx->cap_blocks, n_steps);
     return EMPM_OK;
+}
+
+extern "C" int empm_segment_create(EmpmCtx* ctx, int n_steps, EmpmSegment** out) {
+    if (!ctx || !out) return empm_set_error(ctx, EMPM_ERR_INVALID, "ctx or out is NULL");
+    *out = nullptr;
+    if (n_steps < 1 || n_steps > 100000)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
+    EmpmSegment* seg = new EmpmSegment();
+    seg->ctx = ctx;
+    seg->n = ctx->n_particles;
+    seg->n_steps = n_steps;
+    seg->n_inst = ctx->n_inst;
+    seg->np = padded4(ctx->n_particles);
+    seg->cap_blocks = (size_t)ctx->cap_blocks;
+    const size_t np = seg->np, k = (size_t)n_steps, nb = seg->cap_blocks;
+    cudaError_t e = cudaMalloc(&seg->states, (k + 1) * 26 * np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->mats, k * 3 * np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->fe, k * 9 * np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->gsave, k * nb * 128 * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->glist, k * (nb + 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->vol, np * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->sel, np * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->pid, np * sizeof(int));
+    if (e != cudaSuccess) {
+        segment_free(seg);
+        delete seg;
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();   // an allocation failure is not sticky; clear it
+            return empm_set_error(ctx, EMPM_ERR_OOM, "segment store of %d substeps (%zu bytes) does not fit", n_steps,
+                                  segment_bytes(np, nb, n_steps));
+        }
+        return empm_check_cuda(ctx, e, "segment store");
+    }
+    *out = seg;
+    return EMPM_OK;
+}
+
+extern "C" int empm_segment_destroy(EmpmSegment* seg) {
+    if (!seg) return EMPM_OK;
+    segment_free(seg);
+    delete seg;
+    return EMPM_OK;
+}
+
+static int check_segment(EmpmCtx* ctx, const EmpmSegment* seg) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    if (!seg) return empm_set_error(ctx, EMPM_ERR_INVALID, "segment is NULL");
+    if (seg->ctx != ctx) return empm_set_error(ctx, EMPM_ERR_INVALID, "segment belongs to another context");
+    if (seg->n != ctx->n_particles || seg->n_inst != ctx->n_inst || seg->cap_blocks != (size_t)ctx->cap_blocks)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "segment was made for %d particles, %d instances, %zu blocks; "
+                              "the context now has %d, %d, %lld", seg->n, seg->n_inst, seg->cap_blocks,
+                              ctx->n_particles, ctx->n_inst, (long long)ctx->cap_blocks);
+    return EMPM_OK;
+}
+
+static SegmentData segment_data(const EmpmSegment* seg) {
+    SegmentData d;
+    d.n = seg->n;
+    d.n_steps = seg->n_steps;
+    d.np = seg->np;
+    d.sorted = seg->sorted;
+    d.store = true;
+    d.states = seg->states;
+    d.mats = seg->mats;
+    d.gsave = seg->gsave;
+    d.glist = seg->glist;
+    d.fe = seg->fe;
+    d.cap_blocks = seg->cap_blocks;
+    d.base.vol = seg->vol;
+    d.base.mu = d.base.lam = d.base.ys = nullptr;
+    d.base.sel = seg->has_sel ? seg->sel : nullptr;
+    d.base.pid = seg->sorted ? seg->pid : nullptr;
+    return d;
+}
+
+extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmParticles* ckpt, const float* ckpt_mu,
+                                    const float* ckpt_lam, const float* ckpt_yield, const EmpmMaterial* mat,
+                                    const EmpmStep* steps, int n_steps, EmpmParticles* out, void* stream) {
+    int rc = check_segment(ctx, seg);
+    if (!rc) rc = check_particles(ctx, ckpt, "ckpt");
+    if (!rc) rc = check_particles(ctx, out, "out");
+    if (!rc) rc = check_material(ctx, mat);
+    if (rc) return rc;
+    if (!ckpt_mu || !ckpt_lam || !ckpt_yield)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "checkpoint mu / lam / yield pointer is NULL");
+    if (n_steps != seg->n_steps)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d, the segment holds %d", n_steps, seg->n_steps);
+    if (!steps) return empm_set_error(ctx, EMPM_ERR_INVALID, "steps is NULL");
+    const size_t per = (size_t)n_steps * ctx->n_inst;
+    for (size_t e = 0; e < per; ++e)
+        if (steps[e].hold) return empm_set_error(ctx, EMPM_ERR_UNSUPPORTED, "held substeps cannot be differentiated");
+    cudaStream_t s = (cudaStream_t)stream;
+    seg->ready = false;
+    seg->tables.assign(steps, steps + per);
+    rc = upload_steps(ctx, seg->tables.data(), n_steps, s);
+    if (rc) return rc;
+    const int n = seg->n;
+    if (n == 0) {
+        seg->ready = true;
+        return EMPM_OK;
+    }
+    rc = ensure_adjoint_buffers(ctx, 0);
+    if (rc) return rc;
+    AdjointBuffers& ab = ctx->adj;
+    const size_t np = seg->np;
+    const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
+    seg->sorted = ctx->sort_every > 0;
+    seg->has_sel = seg->sorted || mat->selection != nullptr;
+    if (seg->sorted) {
+        rc = ensure_sorted_buffers(ctx);
+        if (rc) return rc;
+        SortedState ss;
+        const ParticleArrays ua = particle_arrays(ckpt, n);
+        EmpmMaterial um = *mat;
+        um.mu = const_cast<float*>(ckpt_mu);
+        um.lam = const_cast<float*>(ckpt_lam);
+        um.yield_stress = const_cast<float*>(ckpt_yield);
+        rc = launch_sort(ctx, ss, &ua, &um, s);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(seg->states, ctx->sb.part[ss.pc], 26 * np * sizeof(float), d2d, s), "sorted checkpoint");
+        const MaterialArrays SM = sorted_material(ctx, ss.mc);
+        CK(cudaMemcpyAsync(ab.work, SM.mu, sizeof(float) * n, d2d, s), "sorted checkpoint");
+        CK(cudaMemcpyAsync(ab.work + np, SM.lam, sizeof(float) * n, d2d, s), "sorted checkpoint");
+        CK(cudaMemcpyAsync(ab.work + 2 * np, SM.ys, sizeof(float) * n, d2d, s), "sorted checkpoint");
+        CK(cudaMemcpyAsync(seg->vol, SM.vol, sizeof(float) * n, d2d, s), "sorted material");
+        CK(cudaMemcpyAsync(seg->sel, SM.sel, sizeof(int) * n, d2d, s), "sorted material");
+        CK(cudaMemcpyAsync(seg->pid, SM.pid, sizeof(int) * n, d2d, s), "sorted material");
+    } else {
+        const EmpmParticles s0 = packed_particles(seg->states, n);
+        CK(cudaMemcpyAsync(s0.x, ckpt->x, sizeof(float4) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(s0.v, ckpt->v, sizeof(float4) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(s0.C, ckpt->C, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(s0.F, ckpt->F, 9 * sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(ab.work, ckpt_mu, sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(ab.work + np, ckpt_lam, sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(ab.work + 2 * np, ckpt_yield, sizeof(float) * n, d2d, s), "copy checkpoint");
+        CK(cudaMemcpyAsync(seg->vol, mat->vol, sizeof(float) * n, d2d, s), "copy material");
+        if (seg->has_sel) CK(cudaMemcpyAsync(seg->sel, mat->selection, sizeof(int) * n, d2d, s), "copy material");
+    }
+    const SegmentData d = segment_data(seg);
+    rc = segment_forward(ctx, d, s);
+    if (rc) return rc;
+    // the state after the last substep, its elastic F and the updated
+    // material scalars, in the caller's order
+    float* last = seg->states + (size_t)n_steps * 26 * np;
+    float* fe_last = seg->fe + (size_t)(n_steps - 1) * 9 * np;
+    if (seg->sorted) {
+        UnsortArgs u;
+        u.src = particle_arrays(last, n);
+        u.dst = particle_arrays(out, n);
+        u.Fe_s = f9_planes(fe_last, n);
+        u.Fe_d = f9_planes(mat->F_elastic, n);
+        u.mu_s = ab.work; u.mu_d = mat->mu;
+        u.lam_s = ab.work + np; u.lam_d = mat->lam;
+        u.ys_s = ab.work + 2 * np; u.ys_d = mat->yield_stress;
+        u.pid = seg->pid;
+        u.n = n;
+        k_unsort<<<blocks_for(n, 256), 256, 0, s>>>(u);
+        CK(cudaGetLastError(), "k_unsort");
+    } else {
+        const EmpmParticles f = packed_particles(last, n);
+        CK(cudaMemcpyAsync(out->x, f.x, sizeof(float4) * n, d2d, s), "segment result");
+        CK(cudaMemcpyAsync(out->v, f.v, sizeof(float4) * n, d2d, s), "segment result");
+        CK(cudaMemcpyAsync(out->C, f.C, 9 * sizeof(float) * n, d2d, s), "segment result");
+        CK(cudaMemcpyAsync(out->F, f.F, 9 * sizeof(float) * n, d2d, s), "segment result");
+        CK(cudaMemcpyAsync(mat->F_elastic, fe_last, 9 * sizeof(float) * n, d2d, s), "segment result");
+        CK(cudaMemcpyAsync(mat->mu, ab.work, sizeof(float) * n, d2d, s), "segment result");
+        CK(cudaMemcpyAsync(mat->lam, ab.work + np, sizeof(float) * n, d2d, s), "segment result");
+        CK(cudaMemcpyAsync(mat->yield_stress, ab.work + 2 * np, sizeof(float) * n, d2d, s), "segment result");
+    }
+    seg->ready = true;
+    return EMPM_OK;
+}
+
+extern "C" int empm_segment_reverse(EmpmCtx* ctx, EmpmSegment* seg, EmpmParticles* grad, EmpmMaterialGrad* gmat,
+                                    void* stream) {
+    int rc = check_segment(ctx, seg);
+    if (!rc) rc = check_particles(ctx, grad, "grad");
+    if (rc) return rc;
+    if (!gmat || !gmat->mu || !gmat->lam || !gmat->yield_stress || !gmat->mass)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "material gradient pointer is NULL");
+    if (!seg->ready) return empm_set_error(ctx, EMPM_ERR_INVALID, "segment has no completed forward pass");
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = upload_steps(ctx, seg->tables.data(), seg->n_steps, s);
+    if (rc) return rc;
+    const int n = seg->n;
+    if (n == 0) return EMPM_OK;
+    rc = ensure_adjoint_buffers(ctx, 0);
+    if (rc) return rc;
+    AdjointBuffers& ab = ctx->adj;
+    const size_t np = seg->np;
+    ParticleArrays Gp = particle_arrays(grad, n);
+    float* gm_mu = gmat->mu;
+    float* gm_lam = gmat->lam;
+    float* gm_ys = gmat->yield_stress;
+    float* gm_mass = gmat->mass;
+    if (seg->sorted) {
+        // incoming adjoint into the segment's cell order
+        const EmpmParticles gs = packed_particles(ab.gstate, n);
+        GradPermuteArgs perm;
+        perm.src = Gp;
+        perm.dst = particle_arrays(&gs, n);
+        perm.s_mu = gmat->mu; perm.s_lam = gmat->lam; perm.s_ys = gmat->yield_stress; perm.s_mass = gmat->mass;
+        gm_mu = ab.gmats;
+        gm_lam = ab.gmats + np;
+        gm_ys = ab.gmats + 2 * np;
+        gm_mass = ab.gmats + 3 * np;
+        perm.d_mu = gm_mu; perm.d_lam = gm_lam; perm.d_ys = gm_ys; perm.d_mass = gm_mass;
+        perm.pid = seg->pid;
+        perm.n = n;
+        perm.to_sorted = 1;
+        k_permute_grad<<<blocks_for(n, 256), 256, 0, s>>>(perm);
+        CK(cudaGetLastError(), "k_permute_grad");
+        Gp = perm.dst;
+    }
+    return segment_reverse(ctx, segment_data(seg), Gp, gm_mu, gm_lam, gm_ys, gm_mass, grad, gmat, s);
 }
 
 extern "C" int empm_restart_F(EmpmCtx* ctx, EmpmParticles* p, const float* target, const int* selection,

@@ -16,7 +16,7 @@ from __future__ import annotations
 
 import math
 import time as _time
-from typing import List, Optional
+from typing import Dict, List, Optional
 
 import numpy as np
 import torch
@@ -49,6 +49,25 @@ class _Context:
         with torch.cuda.device(device):
             N.check(self.L.empm_ctx_create(params, n_particles, max_steps, N.ctypes.byref(ptr)))
         self.ptr = ptr
+        # stored segments released by differentiable rollouts, by substep count,
+        # for the next rollout of this context (device memory kept allocated)
+        self.segment_pool: Dict[int, List[N.ctypes.c_void_p]] = {}
+
+    def take_segment(self, n_steps: int):
+        lst = self.segment_pool.get(n_steps)
+        return lst.pop() if lst else None
+
+    def give_segment(self, seg, n_steps: int) -> None:
+        self.segment_pool.setdefault(n_steps, []).append(seg)
+
+    def pooled(self, n_steps: int) -> int:
+        return len(self.segment_pool.get(n_steps, ()))
+
+    def free_segments(self) -> None:
+        for lst in self.segment_pool.values():
+            for seg in lst:
+                self.L.empm_segment_destroy(seg)
+        self.segment_pool = {}
 
     def set_params(self, params: N.EmpmModelParams):
         b = bytes(params)
@@ -71,6 +90,7 @@ class _Context:
     def __del__(self):
         try:
             if getattr(self, "ptr", None):
+                self.free_segments()
                 self.L.empm_ctx_destroy(self.ptr)
                 self.ptr = None
         except Exception:
@@ -312,6 +332,12 @@ class MPMWARPDiff(object):
 
     def read_status(self) -> int:
         return 0 if self._ctx is None else self._ctx.status()
+
+    def release_tape_memory(self) -> None:
+        """Free the device memory that differentiable rollouts left for reuse
+        (stored segments of finished tapes)."""
+        if self._ctx is not None:
+            self._ctx.free_segments()
 
     def kernel_timing(self, enable: bool, max_launches: int = 4096):
         """Start (enable) or stop per-kernel CUDA-event timing on the stream path."""

@@ -36,6 +36,8 @@
  *   empm_adjoint_segment <- the Warp tape replay of the substep kernels' adjoints
  *                          (MyTape / tape.backward, warp_utils.py:93-142;
  *                          interface.py:167-251,391-472,579-774,899-986)
+ *   empm_segment_*      <- the tape's record of the forward launches kept for the
+ *                          reverse pass (MyTape, warp_utils.py:93-127; interface.py:135-145)
  *   empm_prepare_adjoint <- the adjoints of compute_mu_lam_from_E_nu and of the mass
  *                          product on the same tape (mpm_utils.py:277-283,
  *                          mpm_data_structure.py:719-726)
@@ -339,6 +341,43 @@ typedef struct {
 int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* ckpt_mu, const float* ckpt_lam,
                           const float* ckpt_yield, const EmpmMaterial* mat, const EmpmStep* steps, int n_steps,
                           EmpmParticles* grad, EmpmMaterialGrad* gmat, void* stream);
+
+/* Stored segments: the forward pass of a differentiable rollout keeps, per
+ * segment, everything its reverse pass reads, so that the reverse pass does
+ * not recompute the segment from a checkpoint. This is what Warp's tape does
+ * for the reference (MyTape records every launch of p2g2p_differentiable,
+ * warp_utils.py:93-127, interface.py:135-145, and tape.backward replays the
+ * adjoints, interface.py:197); here a segment keeps about
+ * 152 B per particle and substep + 2 KiB per grid block and substep, and
+ * empm_segment_bytes gives the exact figure.
+ *
+ * empm_segment_create   allocates the store for n_steps substeps of the
+ *                       context's current particle count and grid blocks;
+ *                       EMPM_ERR_OOM (nothing left allocated) when it does not
+ *                       fit. Call it outside stream capture.
+ * empm_segment_forward  runs n_steps substeps from ckpt / ckpt_mu / ckpt_lam /
+ *                       ckpt_yield (not modified) as empm_rollout would, keeping
+ *                       the store. The state after the last substep goes to
+ *                       out (library layout); mat->mu, lam, yield_stress and
+ *                       F_elastic receive the updated values (they may alias the
+ *                       ckpt_* arrays); mat->vol and selection are read. Steps:
+ *                       n_steps tables of n_instances schedules.
+ * empm_segment_reverse  the adjoint of that forward pass: grad holds
+ *                       dL/d(out) on entry and dL/d(ckpt) on return; gmat as for
+ *                       empm_adjoint_segment. The context's model parameters
+ *                       must still be those of the forward pass. A segment may
+ *                       be reversed more than once.
+ * Gradients equal those of empm_adjoint_segment (which stores and reverses one
+ * segment inside one call) up to the order of floating-point reductions. */
+typedef struct EmpmSegment EmpmSegment;
+int  empm_segment_bytes(EmpmCtx* ctx, int n_steps, size_t* out);
+int  empm_segment_create(EmpmCtx* ctx, int n_steps, EmpmSegment** out);
+int  empm_segment_destroy(EmpmSegment* seg);
+int  empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmParticles* ckpt, const float* ckpt_mu,
+                          const float* ckpt_lam, const float* ckpt_yield, const EmpmMaterial* mat,
+                          const EmpmStep* steps, int n_steps, EmpmParticles* out, void* stream);
+int  empm_segment_reverse(EmpmCtx* ctx, EmpmSegment* seg, EmpmParticles* grad, EmpmMaterialGrad* gmat,
+                          void* stream);
 
 /* Chain rule through empm_prepare: dL/dE and dL/dnu from dL/dmu and dL/dlam
  * (compute_mu_lam_from_E_nu, mpm_utils.py:277-283), and dL/ddensity =

@@ -113,7 +113,8 @@ def _problem(material, n, G, seed, floor=False, deform=0.05, speed=0.3):
     return p
 
 
-def _gpu(p, dt, T, every, weights):
+def _setup(p, dt):
+    """State, model and solver of problem p on the GPU."""
     n, G = p["n"], p["G"]
     st = MPMStateStruct()
     st.init(n, device=DEV)
@@ -149,9 +150,17 @@ def _gpu(p, dt, T, every, weights):
             sv.set_particle_mover(velocity=m["velocity"], angular_velocity=m["angular_velocity"], center=m["center"],
                                   axis=m["axis"], selection_mask=_t(m["mask"], torch.int32), device=DEV)
     register_colliders(sv, p["colliders"])
+    return st, md, sv
+
+
+def _gpu(p, dt, T, every, weights):
+    n = p["n"]
+    st, md, sv = _setup(p, dt)
     mu0, lam0 = md.mu.double().cpu().numpy(), md.lam.double().cpu().numpy()
-    tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=every)
+    tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=every, store=p.get("tape_store"))
     tape.forward()
+    if p.get("tape_store") is not None:
+        assert tape.stored == p["tape_store"]
     wx, wv, wC, wF = weights
     res = tape.backward(g_x=_t(wx), g_v=_t(wv), g_C=_t(wC), g_F=_t(wF))
     torch.cuda.synchronize()
@@ -236,7 +245,7 @@ def test_segment_adjoint_plasticine_yielding(sort_every):
     p = _problem(5, n=800, G=16, seed=2, deform=0.25, speed=0.5)
     p["sort_every"] = sort_every
     tape = _check_directional(p, 2e-4, 6, 4, seed=12)
-    assert [c.step for c in tape.ckpts] == [0, 4]
+    assert tape.bounds == [0, 4, 6]
 
 
 def test_segment_adjoint_with_floor_contact():
@@ -270,11 +279,13 @@ def test_segment_adjoint_modifiers_selection_damping():
 
 @pytest.mark.parametrize("sort_every", [16, 0])
 def test_segment_adjoint_store_matches_recompute(sort_every):
-    """The reverse pass from the stored grids and elastic F gives the gradients
-    of the reverse pass that recomputes them. They agree up to the order of
-    the P2G's floating-point atomics, which the recomputed grid does not
-    repeat: a particle close to the yield surface can take the other branch,
-    so the bound is on the norm of each gradient."""
+    """The three ways to run the reverse pass give the same gradients:
+    - segments stored by the tape's forward pass (empm_segment_*);
+    - checkpoints whose segments are re-run with the grids and elastic F kept;
+    - checkpoints whose grids are recomputed in the reverse pass.
+    They agree up to the order of the P2G's floating-point atomics, which a
+    re-run does not repeat: a particle close to the yield surface can take the
+    other branch, so the bound is on the norm of each gradient."""
     dt = 2e-4
     p = _problem(5, n=1000, G=24, seed=7, floor=True, deform=0.25, speed=0.5)
     p["v"][:, 1] = np.float32(-1.5)
@@ -286,15 +297,54 @@ def test_segment_adjoint_store_matches_recompute(sort_every):
     weights = (rng.standard_normal((n, 3)), rng.standard_normal((n, 3)), 0.01 * rng.standard_normal((n, 9)),
                rng.standard_normal((n, 9)))
     outs = []
-    for store in (True, False):
-        p["adj_store"] = store
+    for tape_store, adj_store in ((False, False), (False, True), (True, True)):
+        p["tape_store"], p["adj_store"] = tape_store, adj_store
         res, _, _, _ = _gpu(p, dt, 12, 5, weights)
         outs.append(res)
-    for k in outs[0]:
-        a, b = outs[0][k], outs[1][k]
-        rel = float(np.linalg.norm(a - b)) / max(float(np.linalg.norm(b)), 1e-30)
-        print(f"  {k}: |store - recompute| / |recompute| = {rel:.2e}")
-        assert rel <= 2e-3, (k, rel)
+    for name, other in (("checkpoint + grid store", outs[1]), ("stored tape", outs[2])):
+        for k in outs[0]:
+            a, b = other[k], outs[0][k]
+            rel = float(np.linalg.norm(a - b)) / max(float(np.linalg.norm(b)), 1e-30)
+            print(f"  {name} {k}: |a - recompute| / |recompute| = {rel:.2e}")
+            assert rel <= 2e-3, (name, k, rel)
+
+
+@pytest.mark.parametrize("sort_every", [16, 0])
+def test_checkpointed_segments_fd(sort_every):
+    """Finite differences through checkpointed segments (re-run in the reverse
+    pass), the path taken when the stored rollout does not fit."""
+    p = _problem(5, n=800, G=16, seed=2, deform=0.25, speed=0.5)
+    p["sort_every"] = sort_every
+    p["tape_store"] = False
+    _check_directional(p, 2e-4, 6, 4, seed=12)
+
+
+def test_stored_forward_matches_rollout():
+    """The stored forward pass ends where the plain rollout ends, and the
+    budget decides between storing and checkpointing."""
+    dt, T = 2e-4, 12
+    p = _problem(5, n=1000, G=24, seed=9, floor=True, deform=0.25, speed=0.5)
+    finals = []
+    for store in (True, False):
+        p["tape_store"] = store
+        rng = np.random.default_rng(3)
+        n = p["n"]
+        w = (rng.standard_normal((n, 3)), rng.standard_normal((n, 3)), rng.standard_normal((n, 9)),
+             rng.standard_normal((n, 9)))
+        _, _, _, tape = _gpu(p, dt, T, 5, w)
+        finals.append((tape.final.particle_x.double().cpu().numpy(), tape.final.particle_v.double().cpu().numpy(),
+                       tape.model.mu.double().cpu().numpy()))
+    for a, b in zip(finals[0], finals[1]):
+        assert float(np.abs(a - b).max()) <= 1e-5 * max(1.0, float(np.abs(b).max()))
+    # a budget of one byte: automatic mode checkpoints, forced storing refuses
+    p["tape_store"] = None
+    st, md, sv = _setup(p, dt)
+    tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store_budget=1)
+    tape.forward()
+    assert not tape.stored and len(tape.ckpts) == 3
+    tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=True, store_budget=1)
+    with pytest.raises(MemoryError):
+        tape.forward()
 
 
 # ---------------------------------------------------------------------------
