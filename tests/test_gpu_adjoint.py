@@ -345,6 +345,20 @@ def test_stored_forward_matches_rollout():
     tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=True, store_budget=1)
     with pytest.raises(MemoryError):
         tape.forward()
+    # released segments go to the context's pool and the next rollout takes them
+    tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=True)
+    tape.forward()
+    ctx = sv._ctx
+    first = [sg.ptr.value for sg in tape.segments]
+    tape.release()
+    assert ctx.pooled(5) == 2 and ctx.pooled(2) == 1
+    tape2 = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=True)
+    tape2.forward()
+    assert sorted(sg.ptr.value for sg in tape2.segments) == sorted(first)
+    assert ctx.pooled(5) == 0 and ctx.pooled(2) == 0
+    del tape2
+    sv.release_tape_memory()
+    assert ctx.pooled(5) == 0
 
 
 # ---------------------------------------------------------------------------
