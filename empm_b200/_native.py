@@ -122,8 +122,9 @@ def lib():
         "empm_adjoint_segment": ([P, ctypes.POINTER(EmpmParticles), P, P, P, ctypes.POINTER(EmpmMaterial), P, I,
                                   ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterialGrad), P], I),
         "empm_prepare_adjoint": ([P, P, P, P, P, P, P, P, P, I, P], I),
-        "empm_segment_bytes": ([P, I, ctypes.POINTER(ctypes.c_size_t)], I),
-        "empm_segment_create": ([P, I, ctypes.POINTER(P)], I),
+        "empm_segment_bytes": ([P, I, I, ctypes.POINTER(ctypes.c_size_t)], I),
+        "empm_segment_create": ([P, I, I, ctypes.POINTER(P)], I),
+        "empm_segment_blocks": ([P, ctypes.POINTER(I), ctypes.POINTER(I), P], I),
         "empm_segment_destroy": ([P], I),
         "empm_segment_forward": ([P, P, ctypes.POINTER(EmpmParticles), P, P, P, ctypes.POINTER(EmpmMaterial), P, I,
                                   ctypes.POINTER(EmpmParticles), P], I),

@@ -90,15 +90,21 @@ class _StoredSegment:
     """A segment kept on the device by empm_segment_forward for its reverse
     pass. Released segments go back to their context's pool."""
 
-    def __init__(self, ctx, ptr: ctypes.c_void_p, step: int, n_steps: int):
+    def __init__(self, ctx, ptr: ctypes.c_void_p, step: int, n_steps: int, block_cap: int):
         self.ctx = ctx
         self.ptr = ptr
         self.step = step
         self.n_steps = n_steps
+        self.block_cap = block_cap
 
     def release(self) -> None:
         if self.ptr is not None:
-            self.ctx.give_segment(self.ptr, self.n_steps)
+            self.ctx.give_segment(self.ptr, self.n_steps, self.block_cap)
+        self.ptr = None
+
+    def destroy(self) -> None:
+        if self.ptr is not None:
+            N.lib().empm_segment_destroy(self.ptr)
         self.ptr = None
 
 
@@ -160,7 +166,15 @@ class CheckpointedRollout:
         except Exception:   # interpreter shutdown: the library may be gone
             pass
 
-    def _allocate_segments(self, ctx, dev) -> bool:
+    def _block_cap(self, ctx, n: int) -> int:
+        """Grid blocks per substep to keep: the largest count a stored forward
+        pass of this context touched, with a margin; before any, a guess from
+        the particle count (an overflow is detected and the pass repeated)."""
+        if ctx.touched_blocks is not None:
+            return int(ctx.touched_blocks * 1.25) + 16
+        return max(1024, n // 32)
+
+    def _allocate_segments(self, ctx, dev, block_cap: int) -> bool:
         """Stored segments for every segment of the rollout, or False (nothing
         kept) when they exceed the budget or do not fit."""
         if self.store is False:
@@ -170,9 +184,9 @@ class CheckpointedRollout:
         total = new = 0
         nb = ctypes.c_size_t()
         for n_seg in set(lengths):
-            N.check(L.empm_segment_bytes(ctx.ptr, n_seg, ctypes.byref(nb)), ctx.ptr)
+            N.check(L.empm_segment_bytes(ctx.ptr, n_seg, block_cap, ctypes.byref(nb)), ctx.ptr)
             total += nb.value * lengths.count(n_seg)
-            new += nb.value * max(0, lengths.count(n_seg) - ctx.pooled(n_seg))
+            new += nb.value * max(0, lengths.count(n_seg) - ctx.pooled(n_seg, block_cap))
         budget = self.store_budget
         if budget is None:
             # segments already in the pool count as available
@@ -183,22 +197,39 @@ class CheckpointedRollout:
             return False
         segs = []
         for s0, n_seg in zip(self.bounds[:-1], lengths):
-            p = ctx.take_segment(n_seg)
-            if p is None:
-                p = ctypes.c_void_p()
-                with torch.cuda.device(dev):
-                    rc = L.empm_segment_create(ctx.ptr, n_seg, ctypes.byref(p))
-                if rc != N.EMPM_OK:
-                    for sg in segs:
-                        sg.release()
-                    if rc == N.EMPM_ERR_OOM and not self.store:
-                        return False
-                    if rc == N.EMPM_ERR_OOM:
-                        raise MemoryError(N.last_error(ctx.ptr))
-                    N.check(rc, ctx.ptr)
-            segs.append(_StoredSegment(ctx, p, s0, n_seg))
+            pooled = ctx.take_segment(n_seg, block_cap)
+            if pooled is not None:
+                segs.append(_StoredSegment(ctx, pooled[0], s0, n_seg, pooled[1]))
+                continue
+            p = ctypes.c_void_p()
+            with torch.cuda.device(dev):
+                rc = L.empm_segment_create(ctx.ptr, n_seg, block_cap, ctypes.byref(p))
+            if rc != N.EMPM_OK:
+                for sg in segs:
+                    sg.release()
+                if rc == N.EMPM_ERR_OOM and not self.store:
+                    return False
+                if rc == N.EMPM_ERR_OOM:
+                    raise MemoryError(N.last_error(ctx.ptr))
+                N.check(rc, ctx.ptr)
+            segs.append(_StoredSegment(ctx, p, s0, n_seg, block_cap))
         self.segments = segs
         return True
+
+    def _blocks_overflowed(self, ctx, stream) -> bool:
+        """Read the touched-block maxima of the stored forward pass (one wait
+        for the stream) into the context's estimate; True when a segment could
+        not keep its grids."""
+        L = N.lib()
+        mx, cap = ctypes.c_int(), ctypes.c_int()
+        over = False
+        seen = 0
+        for sg in self.segments:
+            N.check(L.empm_segment_blocks(sg.ptr, ctypes.byref(mx), ctypes.byref(cap), stream), ctx.ptr)
+            seen = max(seen, mx.value)
+            over |= mx.value > cap.value
+        ctx.touched_blocks = seen if ctx.touched_blocks is None else max(ctx.touched_blocks, seen)
+        return over
 
     def _bounds(self) -> List[int]:
         b = set(range(0, self.n_steps, self.every))
@@ -217,16 +248,38 @@ class CheckpointedRollout:
             times.append(times[-1] + self.dt)
         self.bounds = self._bounds()
         self.release()
+        stream = _stream_ptr(st.device)
+        material0 = (model.mu.clone(), model.lam.clone(), model.yield_stress.clone())
+        for attempt in range(2):
+            store = self._allocate_segments(ctx, st.device, self._block_cap(ctx, n))
+            cur = self._run(ctx, store, times, stream)
+            if not store or not self._blocks_overflowed(ctx, stream):
+                break
+            # a substep touched more grid blocks than the segments hold: run the
+            # pass again from the start with room for the counts just observed
+            for sg in self.segments:
+                sg.destroy()
+            self.segments = []
+            for dst, src in zip((model.mu, model.lam, model.yield_stress), material0):
+                dst.copy_(src)
+            if attempt == 1:
+                raise RuntimeError("stored forward pass overflowed its grid store twice")
+        solver.time = t_end
+        self._ctx = ctx
+        self.final = cur
+        return cur
+
+    def _run(self, ctx, store: bool, times, stream) -> MPMStateStruct:
+        """The forward pass over all segments, stored or checkpointed."""
+        solver, model, st = self.solver, self.model, self.state
         self.ckpts = []
         self.records = []
-        store = self._allocate_segments(ctx, st.device)
         a = st.partial_clone(requires_grad=False)
         for src, dst in ((st._x4, a._x4), (st._v4, a._v4), (st._C, a._C), (st._F_trial, a._F_trial)):
             dst.copy_(src)
         b = st.partial_clone(requires_grad=False)
         cur, other = a, b
         record_set = set(self.record_steps)
-        stream = _stream_ptr(st.device)
         for i, (s0, s1) in enumerate(zip(self.bounds[:-1], self.bounds[1:])):
             L = s1 - s0
             seg = (N.EmpmStep * L).from_buffer(self.table, s0 * ctypes.sizeof(N.EmpmStep))
@@ -249,9 +302,6 @@ class CheckpointedRollout:
                     cur, other = other, cur
             if (s1 - 1) in record_set:
                 self.records.append(cur.particle_x.clone())
-        solver.time = t_end
-        self._ctx = ctx
-        self.final = cur
         return cur
 
     def backward(self, g_x: Optional[Tensor] = None, g_v: Optional[Tensor] = None, g_C: Optional[Tensor] = None,

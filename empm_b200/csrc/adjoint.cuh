@@ -428,14 +428,21 @@ __global__ void k_prepare_adjoint(const float* E, const float* nu, const float* 
 // stored substeps of a segment (EMPM_OPT_ADJ_STORE)
 // ---------------------------------------------------------------------------
 // The touched blocks of one substep, as listed by k_collect_blocks (count,
-// ids), into a store slot: per listed block its 64 node momenta (the P2G
-// accumulation) and 64 node velocities (after the boundary conditions), and
-// the list itself. One thread per node, grid-stride.
+// ids), into a store slot of cap blocks: per listed block its 64 node momenta
+// (the P2G accumulation) and 64 node velocities (after the boundary
+// conditions), and the list itself. One thread per node, grid-stride. The
+// count goes to dst_list[0] and, with max_count, into the running maximum; a
+// substep with more than cap touched blocks saves nothing else (its slot is
+// marked by count > cap, and the caller learns it from the maximum).
 __global__ void __launch_bounds__(256) k_save_grid(const float4* __restrict__ mom, const float4* __restrict__ vel,
                                                    const int* __restrict__ active, float4* __restrict__ dst,
-                                                   int* __restrict__ dst_list) {
+                                                   int* __restrict__ dst_list, int cap, int* max_count) {
     const int count = __ldg(active);
-    if (blockIdx.x == 0 && threadIdx.x == 0) dst_list[0] = count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        dst_list[0] = count;
+        if (max_count) atomicMax(max_count, count);
+    }
+    if (count > cap) return;
     const long long total = (long long)count * 64;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {

@@ -131,15 +131,19 @@ struct EmpmSegment {
     EmpmCtx* ctx = nullptr;
     int      n = 0, n_steps = 0, n_inst = 0;
     size_t   np = 0, cap_blocks = 0;
+    size_t   block_cap = 0;       // grid blocks each substep's store slot holds
     bool     sorted = false, has_sel = false, ready = false;
+    bool     checked = false;     // max_touched read back since the last forward pass
+    int      max_touched = 0;
     float*   states = nullptr;    // (n_steps + 1) packed states
     float*   mats = nullptr;      // n_steps x (mu | lam | yield)
-    float4*  gsave = nullptr;     // n_steps x cap_blocks x 128 float4
-    int*     glist = nullptr;     // n_steps x (1 + cap_blocks)
+    float4*  gsave = nullptr;     // n_steps x block_cap x 128 float4
+    int*     glist = nullptr;     // n_steps x (1 + block_cap)
     float*   fe = nullptr;        // n_steps x f9 planes
     float*   vol = nullptr;       // [np]
     int*     sel = nullptr;       // [np]
     int*     pid = nullptr;       // [np] caller index of each position (cell order)
+    int*     max_count = nullptr; // device: largest touched-block count of the forward pass
     std::vector<EmpmStep> tables;
 };
 

@@ -1120,7 +1120,8 @@ struct SegmentData {
     float4* gsave = nullptr;   // n_steps x cap_blocks x 128 float4
     int* glist = nullptr;      // n_steps x (1 + cap_blocks)
     float* fe = nullptr;       // n_steps x f9 planes
-    size_t cap_blocks = 0;
+    size_t cap_blocks = 0;     // grid blocks per substep slot
+    int* max_count = nullptr;  // running maximum of the touched-block counts, or NULL
     MaterialArrays base;
 };
 
@@ -1166,7 +1167,8 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
         if (rc) return rc;
         k_save_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active,
                                               d.gsave + (size_t)k * d.cap_blocks * 128,
-                                              d.glist + (size_t)k * (d.cap_blocks + 1));
+                                              d.glist + (size_t)k * (d.cap_blocks + 1), (int)d.cap_blocks,
+                                              d.max_count);
         CK(cudaGetLastError(), "k_save_grid");
         k_clear_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->flags, ctx->active);
         CK(cudaGetLastError(), "k_clear_grid");
@@ -1414,22 +1416,28 @@ static size_t segment_bytes(size_t np, size_t cap_blocks, int n_steps) {
 }
 
 static void segment_free(EmpmSegment* seg) {
-    void* ptrs[] = {seg->states, seg->mats, seg->gsave, seg->glist, seg->fe, seg->vol, seg->sel, seg->pid};
+    void* ptrs[] = {seg->states, seg->mats, seg->gsave, seg->glist, seg->fe, seg->vol, seg->sel, seg->pid,
+                    seg->max_count};
     for (void* q : ptrs) if (q) cudaFree(q);
     seg->states = seg->mats = seg->fe = seg->vol = nullptr;
     seg->gsave = nullptr;
-    seg->glist = seg->sel = seg->pid = nullptr;
+    seg->glist = seg->sel = seg->pid = seg->max_count = nullptr;
 }
 
-extern "C" int empm_segment_bytes(EmpmCtx* ctx, int n_steps, size_t* out) {
+// block slots per substep: 0 (or more than the context has) means all of them
+static size_t segment_block_cap(const EmpmCtx* ctx, int block_cap) {
+    return (block_cap <= 0 || block_cap > ctx->cap_blocks) ? (size_t)ctx->cap_blocks : (size_t)block_cap;
+}
+
+extern "C" int empm_segment_bytes(EmpmCtx* ctx, int n_steps, int block_cap, size_t* out) {
     if (!ctx || !out) return empm_set_error(ctx, EMPM_ERR_INVALID, "ctx or out is NULL");
     if (n_steps < 1 || n_steps > 100000)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
-    *out = segment_bytes(padded4(ctx->n_particles), (size_t)ctx->cap_blocks, n_steps);
+    *out = segment_bytes(padded4(ctx->n_particles), segment_block_cap(ctx, block_cap), n_steps);
     return EMPM_OK;
 }
 
-extern "C" int empm_segment_create(EmpmCtx* ctx, int n_steps, EmpmSegment** out) {
+extern "C" int empm_segment_create(EmpmCtx* ctx, int n_steps, int block_cap, EmpmSegment** out) {
     if (!ctx || !out) return empm_set_error(ctx, EMPM_ERR_INVALID, "ctx or out is NULL");
     *out = nullptr;
     if (n_steps < 1 || n_steps > 100000)
@@ -1441,7 +1449,8 @@ extern "C" int empm_segment_create(EmpmCtx* ctx, int n_steps, EmpmSegment** out)
     seg->n_inst = ctx->n_inst;
     seg->np = padded4(ctx->n_particles);
     seg->cap_blocks = (size_t)ctx->cap_blocks;
-    const size_t np = seg->np, k = (size_t)n_steps, nb = seg->cap_blocks;
+    seg->block_cap = segment_block_cap(ctx, block_cap);
+    const size_t np = seg->np, k = (size_t)n_steps, nb = seg->block_cap;
     cudaError_t e = cudaMalloc(&seg->states, (k + 1) * 26 * np * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&seg->mats, k * 3 * np * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&seg->fe, k * 9 * np * sizeof(float));
@@ -1450,6 +1459,7 @@ extern "C" int empm_segment_create(EmpmCtx* ctx, int n_steps, EmpmSegment** out)
     if (e == cudaSuccess) e = cudaMalloc(&seg->vol, np * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&seg->sel, np * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&seg->pid, np * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->max_count, sizeof(int));
     if (e != cudaSuccess) {
         segment_free(seg);
         delete seg;
@@ -1494,7 +1504,8 @@ static SegmentData segment_data(const EmpmSegment* seg) {
     d.gsave = seg->gsave;
     d.glist = seg->glist;
     d.fe = seg->fe;
-    d.cap_blocks = seg->cap_blocks;
+    d.cap_blocks = seg->block_cap;
+    d.max_count = seg->max_count;
     d.base.vol = seg->vol;
     d.base.mu = d.base.lam = d.base.ys = nullptr;
     d.base.sel = seg->has_sel ? seg->sel : nullptr;
@@ -1520,6 +1531,8 @@ extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmPa
         if (steps[e].hold) return empm_set_error(ctx, EMPM_ERR_UNSUPPORTED, "held substeps cannot be differentiated");
     cudaStream_t s = (cudaStream_t)stream;
     seg->ready = false;
+    seg->checked = false;
+    seg->max_touched = 0;
     seg->tables.assign(steps, steps + per);
     rc = upload_steps(ctx, seg->tables.data(), n_steps, s);
     if (rc) return rc;
@@ -1533,6 +1546,7 @@ extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmPa
     AdjointBuffers& ab = ctx->adj;
     const size_t np = seg->np;
     const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
+    CK(cudaMemsetAsync(seg->max_count, 0, sizeof(int), s), "reset touched-block maximum");
     seg->sorted = ctx->sort_every > 0;
     seg->has_sel = seg->sorted || mat->selection != nullptr;
     if (seg->sorted) {
@@ -1601,6 +1615,25 @@ extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmPa
     return EMPM_OK;
 }
 
+extern "C" int empm_segment_blocks(EmpmSegment* seg, int* max_touched, int* block_cap, void* stream) {
+    if (!seg) return empm_set_error(nullptr, EMPM_ERR_INVALID, "segment is NULL");
+    EmpmCtx* ctx = seg->ctx;
+    if (!seg->ready) return empm_set_error(ctx, EMPM_ERR_INVALID, "segment has no completed forward pass");
+    if (!seg->checked) {
+        int m = 0;
+        if (seg->n > 0) {
+            CK(cudaMemcpyAsync(&m, seg->max_count, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream),
+               "read touched-block maximum");
+            CK(cudaStreamSynchronize((cudaStream_t)stream), "read touched-block maximum");
+        }
+        seg->max_touched = m;
+        seg->checked = true;
+    }
+    if (max_touched) *max_touched = seg->max_touched;
+    if (block_cap) *block_cap = (int)seg->block_cap;
+    return EMPM_OK;
+}
+
 extern "C" int empm_segment_reverse(EmpmCtx* ctx, EmpmSegment* seg, EmpmParticles* grad, EmpmMaterialGrad* gmat,
                                     void* stream) {
     int rc = check_segment(ctx, seg);
@@ -1609,6 +1642,12 @@ extern "C" int empm_segment_reverse(EmpmCtx* ctx, EmpmSegment* seg, EmpmParticle
     if (!gmat || !gmat->mu || !gmat->lam || !gmat->yield_stress || !gmat->mass)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "material gradient pointer is NULL");
     if (!seg->ready) return empm_set_error(ctx, EMPM_ERR_INVALID, "segment has no completed forward pass");
+    rc = empm_segment_blocks(seg, nullptr, nullptr, stream);
+    if (rc) return rc;
+    if ((size_t)seg->max_touched > seg->block_cap)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "segment touched %d grid blocks in a substep, over its capacity "
+                              "of %zu: make it with block_cap >= %d and run the forward pass again",
+                              seg->max_touched, seg->block_cap, seg->max_touched);
     cudaStream_t s = (cudaStream_t)stream;
     rc = upload_steps(ctx, seg->tables.data(), seg->n_steps, s);
     if (rc) return rc;

@@ -49,23 +49,33 @@ class _Context:
         with torch.cuda.device(device):
             N.check(self.L.empm_ctx_create(params, n_particles, max_steps, N.ctypes.byref(ptr)))
         self.ptr = ptr
-        # stored segments released by differentiable rollouts, by substep count,
-        # for the next rollout of this context (device memory kept allocated)
-        self.segment_pool: Dict[int, List[N.ctypes.c_void_p]] = {}
+        # stored segments released by differentiable rollouts, as (segment,
+        # grid blocks per substep) by substep count, for the next rollout of this
+        # context (device memory kept allocated)
+        self.segment_pool: Dict[int, List[tuple]] = {}
+        # largest number of grid blocks a substep of a stored forward pass touched
+        self.touched_blocks: Optional[int] = None
 
-    def take_segment(self, n_steps: int):
-        lst = self.segment_pool.get(n_steps)
-        return lst.pop() if lst else None
+    def take_segment(self, n_steps: int, block_cap: int):
+        """A pooled segment of n_steps substeps with room for at least block_cap
+        blocks per substep (the smallest such), or None."""
+        lst = self.segment_pool.get(n_steps, [])
+        fit = [e for e in lst if e[1] >= block_cap]
+        if not fit:
+            return None
+        best = min(fit, key=lambda e: e[1])
+        lst.remove(best)
+        return best
 
-    def give_segment(self, seg, n_steps: int) -> None:
-        self.segment_pool.setdefault(n_steps, []).append(seg)
+    def give_segment(self, seg, n_steps: int, block_cap: int) -> None:
+        self.segment_pool.setdefault(n_steps, []).append((seg, block_cap))
 
-    def pooled(self, n_steps: int) -> int:
-        return len(self.segment_pool.get(n_steps, ()))
+    def pooled(self, n_steps: int, block_cap: int = 0) -> int:
+        return sum(1 for e in self.segment_pool.get(n_steps, ()) if e[1] >= block_cap)
 
     def free_segments(self) -> None:
         for lst in self.segment_pool.values():
-            for seg in lst:
+            for seg, _ in lst:
                 self.L.empm_segment_destroy(seg)
         self.segment_pool = {}
 

@@ -348,13 +348,15 @@ int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* 
  * for the reference (MyTape records every launch of p2g2p_differentiable,
  * warp_utils.py:93-127, interface.py:135-145, and tape.backward replays the
  * adjoints, interface.py:197); here a segment keeps about
- * 152 B per particle and substep + 2 KiB per grid block and substep, and
- * empm_segment_bytes gives the exact figure.
+ * 152 B per particle and substep + 2 KiB per touched grid block and substep,
+ * and empm_segment_bytes gives the exact figure.
  *
  * empm_segment_create   allocates the store for n_steps substeps of the
- *                       context's current particle count and grid blocks;
- *                       EMPM_ERR_OOM (nothing left allocated) when it does not
- *                       fit. Call it outside stream capture.
+ *                       context's current particle count, with room for
+ *                       block_cap touched grid blocks per substep (0: every
+ *                       block of the context's grids); EMPM_ERR_OOM (nothing
+ *                       left allocated) when it does not fit. Call it outside
+ *                       stream capture.
  * empm_segment_forward  runs n_steps substeps from ckpt / ckpt_mu / ckpt_lam /
  *                       ckpt_yield (not modified) as empm_rollout would, keeping
  *                       the store. The state after the last substep goes to
@@ -362,16 +364,24 @@ int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* 
  *                       F_elastic receive the updated values (they may alias the
  *                       ckpt_* arrays); mat->vol and selection are read. Steps:
  *                       n_steps tables of n_instances schedules.
+ * empm_segment_blocks   waits for the stream and gives the largest number of
+ *                       grid blocks any substep of the last forward pass
+ *                       touched, and the segment's block_cap. Over block_cap,
+ *                       that forward pass could not keep its grids: make a
+ *                       segment with a larger block_cap and run it again.
  * empm_segment_reverse  the adjoint of that forward pass: grad holds
  *                       dL/d(out) on entry and dL/d(ckpt) on return; gmat as for
  *                       empm_adjoint_segment. The context's model parameters
  *                       must still be those of the forward pass. A segment may
- *                       be reversed more than once.
+ *                       be reversed more than once. It checks the touched
+ *                       block count (empm_segment_blocks, once per forward
+ *                       pass) and returns EMPM_ERR_INVALID after an overflow.
  * Gradients equal those of empm_adjoint_segment (which stores and reverses one
  * segment inside one call) up to the order of floating-point reductions. */
 typedef struct EmpmSegment EmpmSegment;
-int  empm_segment_bytes(EmpmCtx* ctx, int n_steps, size_t* out);
-int  empm_segment_create(EmpmCtx* ctx, int n_steps, EmpmSegment** out);
+int  empm_segment_bytes(EmpmCtx* ctx, int n_steps, int block_cap, size_t* out);
+int  empm_segment_create(EmpmCtx* ctx, int n_steps, int block_cap, EmpmSegment** out);
+int  empm_segment_blocks(EmpmSegment* seg, int* max_touched, int* block_cap, void* stream);
 int  empm_segment_destroy(EmpmSegment* seg);
 int  empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmParticles* ckpt, const float* ckpt_mu,
                           const float* ckpt_lam, const float* ckpt_yield, const EmpmMaterial* mat,

@@ -359,6 +359,28 @@ def test_stored_forward_matches_rollout():
     del tape2
     sv.release_tape_memory()
     assert ctx.pooled(5) == 0
+    # a grid store too small for the touched blocks: the pass is repeated with
+    # room for the observed counts and ends where the checkpointed pass ends
+    q = _problem(5, n=2000, G=32, seed=9, deform=0.25, speed=0.5)   # ~64 touched blocks per substep
+    n = q["n"]
+    rng = np.random.default_rng(4)
+    g = torch.as_tensor(rng.standard_normal((n, 3)).astype(np.float32), device=DEV)
+    outs = []
+    for store, hint in ((True, 1), (False, None)):
+        st, md, sv = _setup(q, dt)
+        if hint is not None:
+            sv._context(md, n, st.device, max_steps=T).touched_blocks = hint
+        tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=store)
+        final = tape.forward()
+        assert tape.stored == store
+        if store:
+            assert sv._ctx.touched_blocks > int(hint * 1.25) + 16
+            assert all(sg.block_cap >= sv._ctx.touched_blocks for sg in tape.segments)
+        res = tape.backward(g_x=g)
+        outs.append((final.particle_x.double().cpu().numpy(), res["v"].double().cpu().numpy()))
+    assert float(np.abs(outs[0][0] - outs[1][0]).max()) <= 1e-5
+    rel = float(np.linalg.norm(outs[0][1] - outs[1][1])) / float(np.linalg.norm(outs[1][1]))
+    assert rel <= 2e-3, rel
 
 
 # ---------------------------------------------------------------------------
