@@ -664,6 +664,9 @@ def run_ours_c3(args):
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     from empm_b200 import workloads as W
+    import ctypes
+
+    from empm_b200 import _native as N
     from empm_b200.adjoint import CheckpointedRollout, prepare_adjoint
     from empm_b200.interface import MPMDifferentiableSimulation
 
@@ -696,12 +699,21 @@ def run_ours_c3(args):
 
     tape_store = None if args.tape_store is None else bool(args.tape_store)
     stored = []
+    store_info = {}
 
     def grad_step():
         reset()
         tape = CheckpointedRollout(solver, md, st, w.dt, w.T, checkpoint_every=every, store=tape_store)
         final = tape.forward()
         stored.append(tape.stored)
+        if tape.stored:
+            nb = ctypes.c_size_t()
+            total = 0
+            for sg in tape.segments:
+                N.check(N.lib().empm_segment_bytes(solver._ctx.ptr, sg.n_steps, sg.block_cap, ctypes.byref(nb)))
+                total += nb.value
+            store_info.update(bytes=total, touched_blocks=solver._ctx.touched_blocks,
+                              block_cap=tape.segments[0].block_cap)
         diff = final.particle_x - x_target
         res = tape.backward(g_x=2.0 * diff / n)
         g_E, g_nu, _ = prepare_adjoint(md.E, md.nu, res["mu"], res["lam"])
@@ -830,6 +842,9 @@ def run_ours_c3(args):
                    "particles": n, "grid": w.G, "substeps_per_step": w.T, "dt": w.dt,
                    "step": "checkpointed forward + adjoint of every substep (gradients in x0, v0, C0, F0, "
                            "mu, lam, yield, mass; E and nu through the prepare adjoint)",
+                   "store": ({"gb": store_info["bytes"] / 1e9, "touched_blocks_per_substep_max":
+                              store_info["touched_blocks"], "block_slots_per_substep": store_info["block_cap"]}
+                             if stored[-1] else None),
                    "reverse_pass": ("segments stored by the forward pass (no re-run)" if stored[-1] else
                                     "checkpoints, each segment re-run " +
                                     ("keeping its grids and elastic F" if solver.adj_store

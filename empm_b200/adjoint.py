@@ -99,6 +99,10 @@ class _StoredSegment:
 
     def release(self) -> None:
         if self.ptr is not None:
+            need = self.ctx.touched_blocks
+            if need is not None and self.block_cap > 2 * int(need * 1.25) + 64:
+                self.destroy()   # sized by a first guess far above what the rollouts touch
+                return
             self.ctx.give_segment(self.ptr, self.n_steps, self.block_cap)
         self.ptr = None
 
@@ -169,10 +173,12 @@ class CheckpointedRollout:
     def _block_cap(self, ctx, n: int) -> int:
         """Grid blocks per substep to keep: the largest count a stored forward
         pass of this context touched, with a margin; before any, a guess from
-        the particle count (an overflow is detected and the pass repeated)."""
+        the particle count (an overflow is detected and the pass repeated).
+        Segments sized by a guess far above the observed counts are freed when
+        released rather than pooled."""
         if ctx.touched_blocks is not None:
             return int(ctx.touched_blocks * 1.25) + 16
-        return max(1024, n // 32)
+        return max(512, n // 64)
 
     def _allocate_segments(self, ctx, dev, block_cap: int) -> bool:
         """Stored segments for every segment of the rollout, or False (nothing

@@ -345,7 +345,13 @@ def test_stored_forward_matches_rollout():
     tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=True, store_budget=1)
     with pytest.raises(MemoryError):
         tape.forward()
-    # released segments go to the context's pool and the next rollout takes them
+    # released segments go to the context's pool and the next rollout takes
+    # them (once a first pass has measured the touched blocks: segments sized
+    # by the first guess are freed instead)
+    tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=True)
+    tape.forward()
+    assert sv._ctx.touched_blocks is not None
+    tape.release()
     tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=5, store=True)
     tape.forward()
     ctx = sv._ctx
