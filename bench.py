@@ -440,6 +440,8 @@ def run_ours_c4(args):
     specs, dt, T = W.c4(T=args.substeps or 300)
     total = sum(s.n for s in specs)
     batch = BatchedMPM(specs, device=dev)
+    if args.resume_blocks is not None:
+        batch.resume_blocks = bool(args.resume_blocks)
     explicit = [o for o in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap") if getattr(args, o) is not None]
     for opt in explicit:
         setattr(batch, opt, getattr(args, opt))
@@ -618,7 +620,9 @@ def run_ours_c4(args):
                    "grids": sorted(set(s.n_grid for s in specs)), "substeps_per_step": T, "dt": dt,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (working set ~1 GB > 126 MB), no flush",
-                   "launch": "one CUDA graph per 50-substep block for the whole population",
+                   "launch": "one CUDA graph per 50-substep block for the whole population" +
+                             ("; blocks continue from the library's cell-sorted state, one write-back per rollout"
+                              if batch.resume_blocks else "; every block sorts and writes back"),
                    "options": {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode,
                                "g2p_tile": batch.g2p_tile, "tile_cap": batch.tile_cap,
                                "seg_cap": batch.seg_cap},
@@ -1286,6 +1290,9 @@ def main():
     ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
     ap.add_argument("--seg-cap", dest="seg_cap", type=int, default=None,
                     help="warp-aggregated P2G: longest same-cell run per reduction (4, 8, 16, 32)")
+    ap.add_argument("--resume-blocks", dest="resume_blocks", type=int, default=None,
+                    help="c4: 1 = graph blocks continue from the library's sorted state (default), 0 = each block "
+                         "sorts the caller's buffers and writes them back")
     ap.add_argument("--tape-store", dest="tape_store", type=int, default=None,
                     help="c3: 1 = the forward pass stores every segment, 0 = checkpoints (default: store when it fits)")
     ap.add_argument("--adj-store", dest="adj_store", type=int, default=None,

@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libempm_b200.so")
 
 EMPM_OK = 0
+ROLLOUT_GRAPH, ROLLOUT_RESUME, ROLLOUT_KEEP = 1, 2, 4
 EMPM_ERR_INVALID, EMPM_ERR_CUDA, EMPM_ERR_OOM, EMPM_ERR_UNSUPPORTED = -1, -2, -3, -4
 EMPM_MAX_COLLIDERS = 16
 EMPM_MAX_MODIFIERS = 8
@@ -107,6 +108,8 @@ def lib():
         "empm_substep": ([P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmParticles),
                           ctypes.POINTER(EmpmMaterial), ctypes.POINTER(EmpmStep), P], I),
         "empm_rollout": ([P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmParticles),
+                          ctypes.POINTER(EmpmMaterial), P, I, I, I, P], I),
+        "empm_rollout_ex": ([P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmParticles),
                           ctypes.POINTER(EmpmMaterial), P, I, I, I, P], I),
         "empm_batch_create": ([P, P, I, I, ctypes.POINTER(P)], I),
         "empm_batch_set_params": ([P, I, ctypes.POINTER(EmpmModelParams)], I),

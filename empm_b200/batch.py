@@ -119,6 +119,7 @@ class BatchedMPM:
         self.cur = 0
         self.time = 0.0
         self.use_graph = True
+        self.resume_blocks = True   # blocks continue from the library's sorted state (empm_rollout_ex)
         self.sort_every = 16
         self.p2g_mode = 2
         self.g2p_tile = False
@@ -249,7 +250,9 @@ class BatchedMPM:
 
     def rollout(self, dt: float, n_steps: int, block: int = 50):
         """Advance every instance by n_steps substeps, `block` substeps per
-        library call (one CUDA graph per block length)."""
+        library call (one CUDA graph per block). With ``resume_blocks`` the
+        blocks after the first continue from the library's cell-sorted state
+        and only the last writes the particles back in their own order."""
         self._apply_options()
         mat = N.EmpmMaterial(self.vol.data_ptr(), self.mu.data_ptr(), self.lam.data_ptr(),
                              self.yield_stress.data_ptr(), None, self._Fe.data_ptr())
@@ -259,9 +262,14 @@ class BatchedMPM:
             k = min(block, n_steps - done)
             table, n_tables = self._schedule(dt, k)
             a, b = self._views(self.cur), self._views(1 - self.cur)
+            flags = N.ROLLOUT_GRAPH if self.use_graph else 0
+            if self.resume_blocks:
+                if done > 0:
+                    flags |= N.ROLLOUT_RESUME
+                if done + k < n_steps:
+                    flags |= N.ROLLOUT_KEEP
             with torch.cuda.device(self.device):
-                N.check(self.L.empm_rollout(self.ptr, a, b, mat, table, n_tables, k, int(self.use_graph), stream),
-                        self.ptr)
+                N.check(self.L.empm_rollout_ex(self.ptr, a, b, mat, table, n_tables, k, flags, stream), self.ptr)
             if k % 2 == 1:
                 self.cur = 1 - self.cur
             for _ in range(k):

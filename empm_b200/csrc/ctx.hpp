@@ -19,6 +19,17 @@ struct GraphKey {
     int           tile_cap;
     int           seg_cap;
     unsigned long long params_version;
+    int           flags;                      // EMPM_ROLLOUT_RESUME / EMPM_ROLLOUT_KEEP
+    int           start_pc, start_mc, start_since;   // sorted state a resumed sequence starts in
+};
+
+// One captured rollout launch sequence and the sorted state it ends in.
+struct GraphEntry {
+    GraphKey        key{};
+    cudaGraphExec_t exec = nullptr;
+    bool            valid = false;
+    int             end_pc = 0, end_mc = 0, end_since = 0;
+    unsigned long long used = 0;
 };
 
 // Particle and material buffers of the sorted path (cell order).
@@ -100,9 +111,13 @@ struct EmpmCtx {
     cudaStream_t own_stream = nullptr;     // capture stream for the graph path
     cudaEvent_t  ev_a = nullptr;
     cudaEvent_t  ev_b = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    GraphKey     graph_key{};
-    bool         graph_valid = false;
+    static constexpr int kGraphs = 16;     // cached rollout graphs (LRU)
+    GraphEntry   graphs[kGraphs];
+    unsigned long long graph_clock = 0;
+    // the sorted state the last rollout ended in, which EMPM_ROLLOUT_RESUME
+    // continues from: particle / material buffer and substeps since its sort
+    bool         resident = false;
+    int          resident_pc = 0, resident_mc = 0, resident_since = 0;
     // launch options (empm_ctx_set_option)
     int          sort_every = 16;          // 0 = direct path for rollouts too
     int          p2g_mode = 2;             // 0 direct reductions, 1 shared-memory tile, 2 warp-aggregated

@@ -165,12 +165,26 @@ static InstanceConsts instance_consts(const EmpmModelParams& P, int n, int poff,
     return I;
 }
 
+// Captured rollout graphs no longer match the context (options, instance
+// tables, step-table storage): recapture on next use.
+static void invalidate_graphs(EmpmCtx* ctx) {
+    for (GraphEntry& g : ctx->graphs) g.valid = false;
+}
+
+static void destroy_graphs(EmpmCtx* ctx) {
+    for (GraphEntry& g : ctx->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        g.valid = false;
+    }
+}
+
 static int upload_instances(EmpmCtx* ctx) {
     std::vector<InstanceConsts> h(ctx->n_inst);
     for (int i = 0; i < ctx->n_inst; ++i) h[i] = instance_consts(ctx->params[i], ctx->counts[i], ctx->poff[i], ctx->boff[i]);
     CK(cudaMemcpy(ctx->d_inst, h.data(), sizeof(InstanceConsts) * h.size(), cudaMemcpyHostToDevice), "upload instances");
     ctx->params_version++;
-    ctx->graph_valid = false;
+    invalidate_graphs(ctx);
     return EMPM_OK;
 }
 
@@ -185,7 +199,7 @@ static int ensure_step_capacity(EmpmCtx* ctx, int n_tables) {
     }
     CK(cudaMalloc(&ctx->d_steps, sizeof(EmpmStep) * need), "step table");
     ctx->step_entries = need;
-    ctx->graph_valid = false;
+    invalidate_graphs(ctx);
     return EMPM_OK;
 }
 
@@ -260,7 +274,7 @@ extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, i
 
 extern "C" int empm_ctx_destroy(EmpmCtx* ctx) {
     if (!ctx) return EMPM_OK;
-    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    destroy_graphs(ctx);
     for (cudaEvent_t ev : ctx->timing_events) cudaEventDestroy(ev);
     free_sorted(ctx->sb);
     free_adjoint(ctx->adj);
@@ -297,7 +311,8 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
             break;
         default: return empm_set_error(ctx, EMPM_ERR_INVALID, "unknown option %d", option);
     }
-    ctx->graph_valid = false;
+    invalidate_graphs(ctx);
+    ctx->resident = false;
     return EMPM_OK;
 }
 
@@ -326,8 +341,8 @@ extern "C" int empm_batch_reserve(EmpmCtx* ctx, int max_particles, long long max
     const bool grow_i = max_instances > ctx->cap_inst;
     if (!grow_p && !grow_b && !grow_i) return EMPM_OK;
     CK(cudaDeviceSynchronize(), "sync before reserve");
-    if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
-    ctx->graph_valid = false;
+    destroy_graphs(ctx);
+    ctx->resident = false;
     if (grow_b) {
         const size_t grid_bytes = (size_t)max_blocks * 64 * sizeof(float4);
         cudaFree(ctx->grid_mom);
@@ -413,7 +428,8 @@ extern "C" int empm_batch_reconfigure(EmpmCtx* ctx, const EmpmModelParams* param
     CK(cudaMemcpyAsync(ctx->d_inst, h.data(), sizeof(InstanceConsts) * h.size(), cudaMemcpyHostToDevice,
                        (cudaStream_t)stream), "upload instances");
     ctx->params_version++;
-    ctx->graph_valid = false;
+    invalidate_graphs(ctx);
+    ctx->resident = false;
     return EMPM_OK;
 }
 
@@ -586,6 +602,7 @@ static int ensure_sorted_buffers(EmpmCtx* ctx) {
     SortedBuffers& sb = ctx->sb;
     if (sb.allocated && sb.n >= ctx->n_particles && sb.nb >= ctx->nblocks) return EMPM_OK;
     free_sorted(sb);
+    ctx->resident = false;
     // sized for the context's capacity, so that re-laid batches reuse them
     const int n = ctx->cap_particles;
     const size_t nblocks = (size_t)ctx->cap_blocks;
@@ -747,9 +764,14 @@ static bool use_sorted(EmpmCtx* ctx) {
     return ctx->sort_every > 0 && ctx->n_particles > 0;
 }
 
-// The whole launch sequence of a rollout (also what a graph captures).
+// The whole launch sequence of a rollout (also what a graph captures). On the
+// sorted path, ss / since carry the sorted state: with EMPM_ROLLOUT_RESUME the
+// sequence starts from them instead of sorting the caller's buffers, and on
+// return they hold the state it ends in. The cell sort repeats once since
+// reaches sort_every substeps, so the cadence continues across resumed calls.
+// With EMPM_ROLLOUT_KEEP the result stays in the sorted buffers only.
 static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat, int n_tables,
-                          int n_steps, cudaStream_t stream) {
+                          int n_steps, int flags, SortedState& ss, int& since, cudaStream_t stream) {
     int rc = EMPM_OK;
     if (!use_sorted(ctx)) {
         for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
@@ -760,14 +782,21 @@ static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, cons
         return rc;
     }
     const int n = ctx->n_particles;
-    SortedState ss;
-    const ParticleArrays ua = particle_arrays(a, n);
-    rc = launch_sort(ctx, ss, &ua, mat, stream);
-    for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
-        if (i > 0 && i % ctx->sort_every == 0) rc = launch_sort(ctx, ss, nullptr, nullptr, stream);
-        if (rc == EMPM_OK) rc = launch_substep_sorted(ctx, ss, n_tables == 1 ? 0 : i, stream);
+    if (!(flags & EMPM_ROLLOUT_RESUME)) {
+        ss = SortedState();
+        const ParticleArrays ua = particle_arrays(a, n);
+        rc = launch_sort(ctx, ss, &ua, mat, stream);
+        since = 0;
     }
-    if (rc) return rc;
+    for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
+        if (since >= ctx->sort_every) {
+            rc = launch_sort(ctx, ss, nullptr, nullptr, stream);
+            since = 0;
+        }
+        if (rc == EMPM_OK) rc = launch_substep_sorted(ctx, ss, n_tables == 1 ? 0 : i, stream);
+        ++since;
+    }
+    if (rc || (flags & EMPM_ROLLOUT_KEEP)) return rc;
     UnsortArgs u;
     u.src = particle_arrays(ctx->sb.part[ss.pc], n);
     u.dst = particle_arrays((n_steps & 1) ? b : a, n);
@@ -815,8 +844,8 @@ extern "C" int empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles
     return launch_substep_direct(ctx, in, out, mat, 0, s);
 }
 
-extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
-                            const EmpmStep* steps, int n_tables, int n_steps, int use_graph, void* stream) {
+extern "C" int empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
+                               const EmpmStep* steps, int n_tables, int n_steps, int flags, void* stream) {
     if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
     int rc = check_particles(ctx, a, "a");
     if (!rc) rc = check_particles(ctx, b, "b");
@@ -826,54 +855,106 @@ extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, co
     if (n_steps < 1 || n_steps > 100000) return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
     if (n_tables != 1 && n_tables != n_steps)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "n_tables must be 1 or n_steps (%d, %d)", n_tables, n_steps);
+    if (flags & ~(EMPM_ROLLOUT_GRAPH | EMPM_ROLLOUT_RESUME | EMPM_ROLLOUT_KEEP))
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "unknown rollout flags %#x", flags);
     cudaStream_t s = (cudaStream_t)stream;
+    const bool sorted = use_sorted(ctx);
+    if (!sorted) flags &= EMPM_ROLLOUT_GRAPH;   // the direct path always writes the caller's buffers
     rc = upload_steps(ctx, steps, n_tables, s);
     if (rc) return rc;
-    if (use_sorted(ctx)) {
+    if (sorted) {
         rc = ensure_sorted_buffers(ctx);
         if (rc) return rc;
     }
-    if (!use_graph) return launch_rollout(ctx, a, b, mat, n_tables, n_steps, s);
-    // CUDA graph path: capture on the context's own stream (legacy stream 0
-    // cannot be captured), joined to the caller's stream by events.
-    GraphKey key;
-    memset(&key, 0, sizeof(key));
-    key.a = *a;
-    key.b = *b;
-    key.mat = *mat;
-    key.n_steps = n_steps;
-    key.n_tables = n_tables;
-    key.sort_every = ctx->sort_every;
-    key.p2g_mode = ctx->p2g_mode;
-    key.g2p_tile = ctx->g2p_tile;
-    key.tile_cap = ctx->tile_cap;
-    key.seg_cap = ctx->seg_cap;
-    key.params_version = ctx->params_version;
-    if (!ctx->graph_valid || memcmp(&key, &ctx->graph_key, sizeof(key)) != 0) {
-        if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
-        ctx->graph_valid = false;
-        const bool timing_was = ctx->timing;
-        ctx->timing = false;
-        cudaError_t cap = cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal);
-        if (cap != cudaSuccess) { ctx->timing = timing_was; CK(cap, "begin capture"); }
-        rc = launch_rollout(ctx, a, b, mat, n_tables, n_steps, ctx->own_stream);
-        cudaGraph_t graph = nullptr;
-        cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
-        ctx->timing = timing_was;
-        if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
-        CK(e, "end capture");
-        e = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
-        cudaGraphDestroy(graph);
-        CK(e, "graph instantiate");
-        ctx->graph_key = key;
-        ctx->graph_valid = true;
+    if ((flags & EMPM_ROLLOUT_RESUME) && !ctx->resident)
+        return empm_set_error(ctx, EMPM_ERR_INVALID, "EMPM_ROLLOUT_RESUME: no sorted state to continue from");
+    SortedState ss;
+    int since = 0;
+    if (flags & EMPM_ROLLOUT_RESUME) {
+        ss.pc = ctx->resident_pc;
+        ss.mc = ctx->resident_mc;
+        since = ctx->resident_since;
     }
-    CK(cudaEventRecord(ctx->ev_a, s), "record");
-    CK(cudaStreamWaitEvent(ctx->own_stream, ctx->ev_a, 0), "wait");
-    CK(cudaGraphLaunch(ctx->graph_exec, ctx->own_stream), "graph launch");
-    CK(cudaEventRecord(ctx->ev_b, ctx->own_stream), "record");
-    CK(cudaStreamWaitEvent(s, ctx->ev_b, 0), "wait");
+    ctx->resident = false;
+    if (!(flags & EMPM_ROLLOUT_GRAPH)) {
+        rc = launch_rollout(ctx, a, b, mat, n_tables, n_steps, flags, ss, since, s);
+        if (rc) return rc;
+    } else {
+        // CUDA graph path: capture on the context's own stream (legacy stream 0
+        // cannot be captured), joined to the caller's stream by events. The
+        // graphs are cached by launch key, which includes the sorted state a
+        // resumed sequence starts in.
+        GraphKey key;
+        memset(&key, 0, sizeof(key));
+        key.a = *a;
+        key.b = *b;
+        key.mat = *mat;
+        key.n_steps = n_steps;
+        key.n_tables = n_tables;
+        key.sort_every = ctx->sort_every;
+        key.p2g_mode = ctx->p2g_mode;
+        key.g2p_tile = ctx->g2p_tile;
+        key.tile_cap = ctx->tile_cap;
+        key.seg_cap = ctx->seg_cap;
+        key.params_version = ctx->params_version;
+        key.flags = flags & (EMPM_ROLLOUT_RESUME | EMPM_ROLLOUT_KEEP);
+        if (flags & EMPM_ROLLOUT_RESUME) {
+            key.start_pc = ss.pc;
+            key.start_mc = ss.mc;
+            key.start_since = since;
+        }
+        GraphEntry* g = nullptr;
+        for (GraphEntry& e : ctx->graphs)
+            if (e.valid && memcmp(&key, &e.key, sizeof(key)) == 0) { g = &e; break; }
+        if (!g) {
+            g = &ctx->graphs[0];
+            for (GraphEntry& e : ctx->graphs) {
+                if (!e.valid) { g = &e; break; }
+                if (e.used < g->used) g = &e;
+            }
+            if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
+            g->valid = false;
+            const bool timing_was = ctx->timing;
+            ctx->timing = false;
+            cudaError_t cap = cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal);
+            if (cap != cudaSuccess) { ctx->timing = timing_was; CK(cap, "begin capture"); }
+            rc = launch_rollout(ctx, a, b, mat, n_tables, n_steps, flags, ss, since, ctx->own_stream);
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
+            ctx->timing = timing_was;
+            if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+            CK(e, "end capture");
+            e = cudaGraphInstantiate(&g->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(e, "graph instantiate");
+            g->key = key;
+            g->valid = true;
+            g->end_pc = ss.pc;
+            g->end_mc = ss.mc;
+            g->end_since = since;
+        }
+        g->used = ++ctx->graph_clock;
+        ss.pc = g->end_pc;
+        ss.mc = g->end_mc;
+        since = g->end_since;
+        CK(cudaEventRecord(ctx->ev_a, s), "record");
+        CK(cudaStreamWaitEvent(ctx->own_stream, ctx->ev_a, 0), "wait");
+        CK(cudaGraphLaunch(g->exec, ctx->own_stream), "graph launch");
+        CK(cudaEventRecord(ctx->ev_b, ctx->own_stream), "record");
+        CK(cudaStreamWaitEvent(s, ctx->ev_b, 0), "wait");
+    }
+    if (sorted) {
+        ctx->resident = true;
+        ctx->resident_pc = ss.pc;
+        ctx->resident_mc = ss.mc;
+        ctx->resident_since = since;
+    }
     return EMPM_OK;
+}
+
+extern "C" int empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
+                            const EmpmStep* steps, int n_tables, int n_steps, int use_graph, void* stream) {
+    return empm_rollout_ex(ctx, a, b, mat, steps, n_tables, n_steps, use_graph ? EMPM_ROLLOUT_GRAPH : 0, stream);
 }
 
 extern "C" int empm_read_status(EmpmCtx* ctx, uint32_t* status, void* stream) {
@@ -1322,6 +1403,7 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
     rc = ensure_adjoint_buffers(ctx, n_steps);
     if (rc) return rc;
 
+    ctx->resident = false;   // the sort below reuses the rollout's sorted buffers
     const size_t np = padded4(n);
     const size_t state_floats = 26 * np;
     float* mu_w = ab.work;
@@ -1547,6 +1629,7 @@ extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmPa
     const size_t np = seg->np;
     const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
     CK(cudaMemsetAsync(seg->max_count, 0, sizeof(int), s), "reset touched-block maximum");
+    ctx->resident = false;   // a sort here reuses the rollout's sorted buffers
     seg->sorted = ctx->sort_every > 0;
     seg->has_sel = seg->sorted || mat->selection != nullptr;
     if (seg->sorted) {

@@ -260,6 +260,27 @@ int  empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out,
 int  empm_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
                   const EmpmStep* steps, int n_tables, int n_steps, int use_graph, void* stream);
 
+/* empm_rollout with flags, for a rollout run as several calls (e.g. one CUDA
+ * graph per block of substeps):
+ *   EMPM_ROLLOUT_GRAPH   capture / replay a CUDA graph (use_graph above);
+ *   EMPM_ROLLOUT_RESUME  continue from the cell-sorted state the previous
+ *                        rollout on this context ended in, instead of sorting
+ *                        a: the caller promises that a holds that rollout's
+ *                        result, unchanged. The sort cadence continues too.
+ *                        EMPM_ERR_INVALID when there is no such state (another
+ *                        call re-laid, re-sorted or re-configured the context);
+ *   EMPM_ROLLOUT_KEEP    leave the result in the library's sorted buffers
+ *                        only: a, b and the mat arrays are not written, and a
+ *                        later EMPM_ROLLOUT_RESUME call continues from it.
+ * Without sorting (EMPM_OPT_SORT_EVERY 0) RESUME and KEEP have no effect.
+ * Graphs are cached per launch key (buffers, n_steps, options, flags, and the
+ * sorted state a resumed sequence starts in), 16 at most. */
+#define EMPM_ROLLOUT_GRAPH   1
+#define EMPM_ROLLOUT_RESUME  2
+#define EMPM_ROLLOUT_KEEP    4
+int  empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
+                     const EmpmStep* steps, int n_tables, int n_steps, int flags, void* stream);
+
 /* Launch options of a context (empm_ctx_set_option). */
 #define EMPM_OPT_SORT_EVERY  1   /* rollouts re-sort particles by 4^3 cell block every N substeps; 0 = no sorting (default 16) */
 #define EMPM_OPT_P2G_MODE    2   /* sorted-path P2G: 0 = one 16-byte reduction per particle and node,

@@ -123,3 +123,44 @@ def test_batch_launch_options_agree(sort_every, p2g_mode, seg_cap):
     b.rollout(2e-4, 24, block=12)
     torch.cuda.synchronize()
     assert max_abs(b.positions(), ref.positions()) <= 1e-5
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_resumed_blocks_match_written_back_blocks(use_graph):
+    """Blocks that continue from the library's sorted state (one write-back at
+    the end) end where blocks that write back and re-sort every time end."""
+    specs = _specs(dynamic=True)
+    runs = []
+    for resume in (False, True):
+        b = BatchedMPM(specs, device=DEV)
+        b.use_graph = use_graph
+        b.resume_blocks = resume
+        b.sort_every = 16
+        b.rollout(2e-4, 130, block=50)
+        b.rollout(2e-4, 20, block=50)        # a second call starts from the caller's buffers again
+        torch.cuda.synchronize()
+        runs.append((b.positions().clone(), b.mu.clone(), b.yield_stress.clone(), b._Fe.clone()))
+    for a, c in zip(runs[0], runs[1]):
+        assert max_abs(a, c) <= 1e-5 * max(1.0, float(c.abs().max()))
+
+
+def test_rollout_resume_needs_a_sorted_state():
+    from empm_b200 import _native as N
+    from empm_b200.mpm_data_structure import _stream_ptr
+
+    specs = _specs()
+    b = BatchedMPM(specs, device=DEV)
+    b._apply_options()
+    mat = N.EmpmMaterial(b.vol.data_ptr(), b.mu.data_ptr(), b.lam.data_ptr(), b.yield_stress.data_ptr(), None,
+                         b._Fe.data_ptr())
+    table, n_tables = b._schedule(2e-4, 4)
+    rc = b.L.empm_rollout_ex(b.ptr, b._views(0), b._views(1), mat, table, n_tables, 4, N.ROLLOUT_RESUME,
+                             _stream_ptr(b.device))
+    assert rc == N.EMPM_ERR_INVALID
+    assert "no sorted state" in N.last_error(b.ptr)
+    # after a rollout that kept its state, resuming works
+    b.rollout(2e-4, 4, block=4)
+    rc = b.L.empm_rollout_ex(b.ptr, b._views(b.cur), b._views(1 - b.cur), mat, table, n_tables, 4,
+                             N.ROLLOUT_RESUME, _stream_ptr(b.device))
+    assert rc == N.EMPM_OK
+    torch.cuda.synchronize()
