@@ -454,7 +454,7 @@ def run_ours_c4(args):
         res = A.tune_batch(batch, dt, substeps=50)
         tuned = {"options": res["options"], "candidates": len(res["ms"]), "seconds": time.perf_counter() - t_tune,
                  "best_ms_per_substep": min(res["ms"].values()),
-                 "default_ms_per_substep": res["ms"].get(json.dumps(dict(sort_every=16, p2g_mode=2, tile_cap=1024,
+                 "default_ms_per_substep": res["ms"].get(json.dumps(dict(sort_every=32, p2g_mode=2, tile_cap=1024,
                                                                          seg_cap=4, g2p_tile=0), sort_keys=True))}
     init = [t.clone() for t in (batch._x4[0], batch._v4[0], batch._C[0], batch._F[0], batch.mu, batch.lam,
                                 batch.yield_stress)]

@@ -120,7 +120,7 @@ class BatchedMPM:
         self.time = 0.0
         self.use_graph = True
         self.resume_blocks = True   # blocks continue from the library's sorted state (empm_rollout_ex)
-        self.sort_every = 16
+        self.sort_every = 32
         self.p2g_mode = 2
         self.g2p_tile = False
         self.tile_cap = 1024

@@ -119,7 +119,7 @@ struct EmpmCtx {
     bool         resident = false;
     int          resident_pc = 0, resident_mc = 0, resident_since = 0;
     // launch options (empm_ctx_set_option)
-    int          sort_every = 16;          // 0 = direct path for rollouts too
+    int          sort_every = 32;          // 0 = direct path for rollouts too
     int          p2g_mode = 2;             // 0 direct reductions, 1 shared-memory tile, 2 warp-aggregated
     int          g2p_tile = 0;
     int          tile_cap = 1024;          // nodes per shared-memory tile (16 B each)

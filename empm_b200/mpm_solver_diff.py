@@ -114,7 +114,7 @@ class MPMWARPDiff(object):
         self._ctx: Optional[_Context] = None
         self.use_graph = True
         # launch options of the library (see EMPM_OPT_* in include/empm_b200.h)
-        self.sort_every = 16
+        self.sort_every = 32
         self.p2g_mode = 2          # 0 direct, 1 shared-memory tile, 2 warp-aggregated
         self.g2p_tile = False
         self.tile_cap = 1024

@@ -319,7 +319,7 @@ class GpuExecutor:
     """Device state of the server: the batch context and its particle arena,
     the per-request checkpoints and the adjoint engine."""
 
-    def __init__(self, cap: Capacity, device="cuda:0", sort_every: int = 16):
+    def __init__(self, cap: Capacity, device="cuda:0", sort_every: int = 32):
         import torch
 
         from . import _native as N
@@ -657,7 +657,7 @@ class MPMServer:
     """Continuous-batching request loop on one GPU (see the module docstring)."""
 
     def __init__(self, hbm_budget: int = 40 << 30, device="cuda:0", block: int = 50, max_instances: int = 64,
-                 capacity: Optional[Capacity] = None, sort_every: int = 16, max_blocks_in_flight: int = 2):
+                 capacity: Optional[Capacity] = None, sort_every: int = 32, max_blocks_in_flight: int = 2):
         self.cap = capacity or capacity_for_budget(hbm_budget, max_instances=max_instances, every=block)
         self.sched = Scheduler(self.cap, block=block)
         self.exec = GpuExecutor(self.cap, device=device, sort_every=sort_every)

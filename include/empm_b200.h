@@ -282,7 +282,7 @@ int  empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const Emp
                      const EmpmStep* steps, int n_tables, int n_steps, int flags, void* stream);
 
 /* Launch options of a context (empm_ctx_set_option). */
-#define EMPM_OPT_SORT_EVERY  1   /* rollouts re-sort particles by 4^3 cell block every N substeps; 0 = no sorting (default 16) */
+#define EMPM_OPT_SORT_EVERY  1   /* rollouts re-sort particles by 4^3 cell block every N substeps; 0 = no sorting (default 32) */
 #define EMPM_OPT_P2G_MODE    2   /* sorted-path P2G: 0 = one 16-byte reduction per particle and node,
                                     1 = shared-memory node tile per chunk, 2 = warp-aggregated reductions
                                     over same-cell particles (default) */
