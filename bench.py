@@ -932,6 +932,13 @@ def run_ours_c5(args):
     clk = clocks.stop()
     stats = dict(srv.stats)
     srv.stop(timeout=600)
+    # the plain sample below runs as a user alone on the GPU would: the
+    # server's arenas and checkpoints are released first
+    del srv
+    import gc
+
+    gc.collect()
+    torch.cuda.empty_cache()
     ok = [r for r in rows if r[0] == "ok"]
     t_first = min(r[4] for r in rows)
     t_last = max(r[5] for r in rows)

@@ -178,7 +178,7 @@ class CheckpointedRollout:
         released rather than pooled."""
         if ctx.touched_blocks is not None:
             return int(ctx.touched_blocks * 1.25) + 16
-        return max(512, n // 64)
+        return max(512, n // 256)
 
     def _allocate_segments(self, ctx, dev, block_cap: int) -> bool:
         """Stored segments for every segment of the rollout, or False (nothing
