@@ -955,6 +955,7 @@ def run_ours_c5(args):
     prng = np.random.default_rng(55)
     sample = [arrivals[i] for i in prng.choice(len(arrivals), size=min(args.c5_plain, len(arrivals)), replace=False)]
     plain_ps, plain_ms, kernel_ms = 0, 0.0, 0.0
+    plain_rows = []
     for (_, grad, n, G, T, sd) in sample:
         req = W.c5_request(grad, n, G, T, sd)
         solver, md, st = single_instance(req.spec, device=dev)
@@ -968,6 +969,7 @@ def run_ours_c5(args):
             solver.time = 0.0
             torch.cuda.synchronize()
 
+        stored = None
         for rep in range(2):   # the first run creates the context, captures graphs and allocates buffers
             restore()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -976,11 +978,16 @@ def run_ours_c5(args):
                 tape = CheckpointedRollout(solver, md, st, req.dt, T, checkpoint_every=50)
                 diff = tape.forward().particle_x - target
                 tape.backward(g_x=2.0 * diff / n)
+                stored = tape.stored
+                tape.release()
+                del tape, diff
             else:
                 solver.rollout(md, st, other, req.dt, T)
             e1.record()
             torch.cuda.synchronize()
         t_rollout = e0.elapsed_time(e1)
+        plain_rows.append({"grad": bool(grad), "particles": int(n), "grid": int(G), "substeps": int(T),
+                           "ms": round(t_rollout, 2), "stored_tape": stored})
         plain_ms += t_rollout
         plain_ps += n * T
         if grad:
@@ -998,7 +1005,9 @@ def run_ours_c5(args):
             e1.record()
             torch.cuda.synchronize()
             kernel_ms += e0.elapsed_time(e1)
+        solver.release_tape_memory()
         del solver, md, st, other, init
+        gc.collect()
     plain_value = plain_ps / (plain_ms / 1e3)
     plain_kernel_value = plain_ps / (kernel_ms / 1e3)
 
@@ -1038,6 +1047,7 @@ def run_ours_c5(args):
                    "engine": {k: stats[k] for k in ("blocks", "substeps", "relayouts")},
                    "plain_value": plain_value, "served_vs_plain": value / plain_value,
                    "plain_kernel_value": plain_kernel_value, "served_vs_plain_kernel": value / plain_kernel_value,
+                   "plain_requests": plain_rows,
                    "plain_kernel": "the same sampled requests with the rollouts driven one p2g2p_differentiable call "
                                    "per substep (the plain single-instance kernel path, as the reference's "
                                    "advance_to drives its kernels); gradient requests as in plain",
