@@ -1,8 +1,8 @@
 """Generate golden vectors by running the reference's own simulator source.
 
-Run in a container that has the reference checkout (read-only) at
-/root/reference; the GPU test box does not, so the outputs are committed as
-tests/golden/*.npz:
+Run where the reference checkout is available (read-only) at
+/root/reference. The machines that run the GPU tests do not have it, so the
+outputs are committed as tests/golden/*.npz:
 
     python tests/golden/make_golden.py [--reference /root/reference]
 
