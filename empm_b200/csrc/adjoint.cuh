@@ -427,49 +427,6 @@ __global__ void k_prepare_adjoint(const float* E, const float* nu, const float* 
 // ---------------------------------------------------------------------------
 // stored substeps of a segment (EMPM_OPT_ADJ_STORE)
 // ---------------------------------------------------------------------------
-// The touched blocks of one substep, as listed by k_collect_blocks (count,
-// ids), into a store slot of cap blocks: per listed block its 64 node momenta
-// (the P2G accumulation) and 64 node velocities (after the boundary
-// conditions), and the list itself. One thread per node, grid-stride. The
-// count goes to dst_list[0] and, with max_count, into the running maximum; a
-// substep with more than cap touched blocks saves nothing else (its slot is
-// marked by count > cap, and the caller learns it from the maximum).
-__global__ void __launch_bounds__(256) k_save_grid(const float4* __restrict__ mom, const float4* __restrict__ vel,
-                                                   const int* __restrict__ active, float4* __restrict__ dst,
-                                                   int* __restrict__ dst_list, int cap, int* max_count) {
-    const int count = __ldg(active);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        dst_list[0] = count;
-        if (max_count) atomicMax(max_count, count);
-    }
-    if (count > cap) return;
-    const long long total = (long long)count * 64;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const long long slot = idx >> 6;
-        const int in_block = (int)(idx & 63);
-        const int b = __ldg(active + 1 + slot);
-        const long long node = ((long long)b << 6) | in_block;
-        dst[slot * 128 + in_block] = mom[node];
-        dst[slot * 128 + 64 + in_block] = vel[node];
-        if (in_block == 0) dst_list[1 + slot] = b;
-    }
-}
-
-// What the grid update's non-keep variant does inline, for the listed
-// blocks: zero the accumulation and clear the touched flags.
-__global__ void __launch_bounds__(256) k_clear_grid(float4* __restrict__ mom, unsigned char* __restrict__ flags,
-                                                    const int* __restrict__ active) {
-    const long long total = (long long)__ldg(active) * 64;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const int b = __ldg(active + 1 + (idx >> 6));
-        const int in_block = (int)(idx & 63);
-        mom[((long long)b << 6) | in_block] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (in_block == 0) flags[b] = 0;
-    }
-}
-
 // A store slot back into the grid: node momenta and velocities of its
 // blocks, and their touched flags set, as the recomputed P2G and grid update
 // would leave them for the adjoint kernels.

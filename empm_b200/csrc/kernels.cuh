@@ -231,6 +231,14 @@ struct GridUpdateArgs {
     float4*        vel;      // node velocity after the boundary conditions (w = node mass)
     unsigned char* flags;    // touched blocks; cleared here
     Launch         L;
+    // optional store slot of the listed blocks (stored segments): per listed
+    // block its 64 node momenta, then its 64 node velocities; the list count
+    // and ids; a running maximum of the counts. A substep with more than
+    // store_cap listed blocks stores only its count.
+    float4*        store = nullptr;
+    int*           store_list = nullptr;
+    int            store_cap = 0;
+    int*           max_count = nullptr;
 };
 
 // One touched 4^3 block (64 nodes, two per lane of the calling warp):
@@ -314,7 +322,13 @@ __global__ void __launch_bounds__(256) k_collect_blocks(unsigned char* flags, in
 // Grid update over the listed blocks, one thread per node (grid-stride).
 template <bool kKeep>
 __global__ void __launch_bounds__(256) k_grid_update_list(const GridUpdateArgs a, const int* active) {
-    const long long total = (long long)__ldg(active) * 64;
+    const int count = __ldg(active);
+    const long long total = (long long)count * 64;
+    if (a.store && blockIdx.x == 0 && threadIdx.x == 0) {
+        a.store_list[0] = count;
+        if (a.max_count) atomicMax(a.max_count, count);
+    }
+    const bool save = a.store && count <= a.store_cap;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const int b = __ldg(active + 1 + (idx >> 6));
@@ -335,7 +349,14 @@ __global__ void __launch_bounds__(256) k_grid_update_list(const GridUpdateArgs a
                 apply_colliders(st, i, j, k, G, __ldg(&I->dx), dense, v);
             }
         }
-        a.vel[node] = make_float4(v.x, v.y, v.z, m.w);
+        const float4 v4 = make_float4(v.x, v.y, v.z, m.w);
+        a.vel[node] = v4;
+        if (save) {
+            const long long slot = idx >> 6;
+            a.store[slot * 128 + in_block] = m;
+            a.store[slot * 128 + 64 + in_block] = v4;
+            if (in_block == 0) a.store_list[1 + slot] = b;
+        }
     }
 }
 

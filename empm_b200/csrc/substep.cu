@@ -542,13 +542,28 @@ static int particle_threads(const EmpmCtx* ctx, long long n, int usual) {
     return blocks_for(n, usual) >= 2LL * ctx->sm_count ? usual : 64;
 }
 
+// Optional store slot for launch_grid_update_list (stored segments).
+struct GridStoreSlot {
+    float4* blocks;
+    int*    list;
+    int     cap;
+    int*    max_count;
+};
+
 template <bool kKeep>
-static int launch_grid_update_list(EmpmCtx* ctx, const Launch& L, cudaStream_t stream) {
+static int launch_grid_update_list(EmpmCtx* ctx, const Launch& L, cudaStream_t stream,
+                                   const GridStoreSlot* store = nullptr) {
     GridUpdateArgs g;
     g.mom = ctx->grid_mom;
     g.vel = ctx->grid_vel;
     g.flags = ctx->flags;
     g.L = L;
+    if (store) {
+        g.store = store->blocks;
+        g.store_list = store->list;
+        g.store_cap = store->cap;
+        g.max_count = store->max_count;
+    }
     CK(cudaMemsetAsync(ctx->active, 0, sizeof(int), stream), "reset touched-block count");
     k_collect_blocks<kKeep><<<blocks_for(ctx->nblocks, 256), 256, 0, stream>>>(ctx->flags, (int)ctx->nblocks,
                                                                                ctx->active, L);
@@ -1212,8 +1227,7 @@ struct SegmentData {
 // the state after it is only needed by the caller: its P2G writes the
 // velocity modifiers into that substep's stored velocities, which the reverse
 // pass reads. With the store, P2G writes each substep's elastic F straight
-// into its store slot and the touched grid blocks are saved after the grid
-// update.
+// into its store slot and the grid update saves the touched grid blocks.
 static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
     AdjointBuffers& ab = ctx->adj;
     const int n = d.n;
@@ -1224,7 +1238,6 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
     Mw.lam = ab.work + np;
     Mw.ys = ab.work + 2 * np;
     const F9Planes Fe = f9_planes(ab.fe, n);
-    const int grid_ctas = ctx->sm_count * 8;
     for (int k = 0; k < d.n_steps; ++k) {
         CK(cudaMemcpyAsync(d.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, s),
            "snapshot");
@@ -1243,16 +1256,16 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
         else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
         timing_mark(ctx, 0, 1, s);
         CK(cudaGetLastError(), "adjoint segment P2G");
+        // the grid update stores the touched blocks as it goes, and clears the
+        // accumulator and the touched flags as for a plain substep
         timing_mark(ctx, 1, 0, s);
-        const int rc = launch_grid_update_list<true>(ctx, Lk, s);
+        GridStoreSlot slot;
+        slot.blocks = d.gsave + (size_t)k * d.cap_blocks * 128;
+        slot.list = d.glist + (size_t)k * (d.cap_blocks + 1);
+        slot.cap = (int)d.cap_blocks;
+        slot.max_count = d.max_count;
+        const int rc = launch_grid_update_list<false>(ctx, Lk, s, &slot);
         if (rc) return rc;
-        k_save_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->active,
-                                              d.gsave + (size_t)k * d.cap_blocks * 128,
-                                              d.glist + (size_t)k * (d.cap_blocks + 1), (int)d.cap_blocks,
-                                              d.max_count);
-        CK(cudaGetLastError(), "k_save_grid");
-        k_clear_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->flags, ctx->active);
-        CK(cudaGetLastError(), "k_clear_grid");
         timing_mark(ctx, 1, 1, s);
         timing_mark(ctx, 2, 0, s);
         k_g2p_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Fk, Mw, Pout, Lk, ctx->grid_vel);
