@@ -869,10 +869,10 @@ def run_ours_c3(args):
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n * (12 + 12 + 4 + 4),
                 "d2h_bytes_per_step": n * 12 + 12,
                 "path": "MPMDifferentiableSimulation.apply + loss.backward() with pinned host inputs"},
-        # per substep, not counting the cell sorts and permutations: with stored segments the forward's 6 (P2G,
-        # block list, grid update, grid save, grid clear, G2P) and the reverse pass's 4 (grid restore, the 3
-        # adjoint kernels); with checkpoints also the plain forward's 4 before them
-        "gpu_launches": (10 if stored[-1] else 14) * w.T * args.steps,
+        # per substep, not counting the cell sorts and permutations: with stored segments the forward's 4 (P2G,
+        # block list, grid update writing the store, G2P) and the reverse pass's 4 (grid restore, the 3 adjoint
+        # kernels); with checkpoints also the plain forward's 4 before them
+        "gpu_launches": (8 if stored[-1] else 12) * w.T * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
