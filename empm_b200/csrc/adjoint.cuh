@@ -203,6 +203,48 @@ struct AdjGridArgs {
     Launch         L;
 };
 
+// The grid adjoint of one node of block b (instance inst) whose accumulated
+// momentum and mass are m: the forward update is replayed to learn which
+// collider projections applied, then their transposes, the damping and the
+// normalisation are applied to the node velocity adjoint (gacc, zeroed here).
+__device__ __forceinline__ void adj_grid_node(const AdjGridArgs& a, int b, int inst, int lane, float4 m) {
+    const InstanceConsts* I = a.L.inst + inst;
+    const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
+    const float damping = __ldg(&I->damping);
+    const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
+    const long long node = ((long long)b << 6) | lane;
+    const float4 g4 = a.gacc[node];
+    a.gacc[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    V3 v = grid_velocity(m, st.dt, v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2])), damping);
+    unsigned long long codes = 0;
+    if (st.n_colliders > 0) {
+        int i, j, k;
+        node_coords(((long long)(b - boff) << 6) | lane, NB, i, j, k);
+        if (i < G && j < G && k < G) {
+            const long long dense = ((long long)i * G + j) * G + k;
+            apply_colliders_rec(st, i, j, k, G, __ldg(&I->dx), dense, v,
+                                [&](int cidx, unsigned code) { codes |= (unsigned long long)code << (4 * cidx); });
+        }
+    }
+    V3 g = v3(g4.x, g4.y, g4.z);
+    for (int cidx = st.n_colliders - 1; codes != 0 && cidx >= 0; --cidx) {
+        const unsigned code = (unsigned)(codes >> (4 * cidx)) & 15u;
+        if (code & 1u) g.x = 0.f;
+        if (code & 2u) g.y = 0.f;
+        if (code & 4u) g.z = 0.f;
+        if (code & 8u) g = g * 0.3f;
+    }
+    if (damping < 1.f) g = g - (1.f - damping) * g;
+    float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (m.w > 1e-15f) {
+        const float inv = 1.f / m.w;
+        out = make_float4(g.x * inv, g.y * inv, g.z * inv, -(g.x * m.x + g.y * m.y + g.z * m.z) * inv * inv);
+    }
+    a.gmom[node] = out;
+}
+
+// Over the blocks flagged in the grid (the recomputed substep): the kept
+// momentum is read from the grid and zeroed there, and the flags cleared.
 __global__ void __launch_bounds__(256) k_adj_grid(const AdjGridArgs a) {
     const int nblocks = a.L.nblocks;
     const int group = threadIdx.x >> 6;
@@ -212,44 +254,26 @@ __global__ void __launch_bounds__(256) k_adj_grid(const AdjGridArgs a) {
         const bool active = b < nblocks && a.flags[b] != 0;
         __syncthreads();   // every group has read its flag before any is cleared
         if (!active) continue;
-        const int inst = find_instance_block(a.L, b);
-        const InstanceConsts* I = a.L.inst + inst;
-        const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
-        const float damping = __ldg(&I->damping);
-        const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
         const long long node = ((long long)b << 6) | lane;
         const float4 m = a.mom[node];
-        const float4 g4 = a.gacc[node];
         a.mom[node] = make_float4(0.f, 0.f, 0.f, 0.f);
-        a.gacc[node] = make_float4(0.f, 0.f, 0.f, 0.f);
-        // replay the forward update to learn which projections applied
-        V3 v = grid_velocity(m, st.dt, v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2])), damping);
-        unsigned long long codes = 0;
-        if (st.n_colliders > 0) {
-            int i, j, k;
-            node_coords(((long long)(b - boff) << 6) | lane, NB, i, j, k);
-            if (i < G && j < G && k < G) {
-                const long long dense = ((long long)i * G + j) * G + k;
-                apply_colliders_rec(st, i, j, k, G, __ldg(&I->dx), dense, v,
-                                    [&](int cidx, unsigned code) { codes |= (unsigned long long)code << (4 * cidx); });
-            }
-        }
-        V3 g = v3(g4.x, g4.y, g4.z);
-        for (int cidx = st.n_colliders - 1; codes != 0 && cidx >= 0; --cidx) {
-            const unsigned code = (unsigned)(codes >> (4 * cidx)) & 15u;
-            if (code & 1u) g.x = 0.f;
-            if (code & 2u) g.y = 0.f;
-            if (code & 4u) g.z = 0.f;
-            if (code & 8u) g = g * 0.3f;
-        }
-        if (damping < 1.f) g = g - (1.f - damping) * g;
-        float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (m.w > 1e-15f) {
-            const float inv = 1.f / m.w;
-            out = make_float4(g.x * inv, g.y * inv, g.z * inv, -(g.x * m.x + g.y * m.y + g.z * m.z) * inv * inv);
-        }
-        a.gmom[node] = out;
+        adj_grid_node(a, b, find_instance_block(a.L, b), lane, m);
         if (lane == 0) a.flags[b] = 0;
+    }
+}
+
+// Over the blocks of a store slot (a stored substep): the momentum is read
+// from the slot, so the grid's accumulator and flags are not used. One thread
+// per node, grid-stride.
+__global__ void __launch_bounds__(256) k_adj_grid_stored(const AdjGridArgs a, const float4* __restrict__ slot,
+                                                         const int* __restrict__ slot_list) {
+    const long long total = (long long)__ldg(slot_list) * 64;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long k = idx >> 6;
+        const int lane = (int)(idx & 63);
+        const int b = __ldg(slot_list + 1 + k);
+        adj_grid_node(a, b, find_instance_block(a.L, b), lane, __ldg(slot + k * 128 + lane));
     }
 }
 
@@ -427,22 +451,17 @@ __global__ void k_prepare_adjoint(const float* E, const float* nu, const float* 
 // ---------------------------------------------------------------------------
 // stored substeps of a segment (EMPM_OPT_ADJ_STORE)
 // ---------------------------------------------------------------------------
-// A store slot back into the grid: node momenta and velocities of its
-// blocks, and their touched flags set, as the recomputed P2G and grid update
-// would leave them for the adjoint kernels.
-__global__ void __launch_bounds__(256) k_restore_grid(float4* __restrict__ mom, float4* __restrict__ vel,
-                                                      unsigned char* __restrict__ flags,
-                                                      const float4* __restrict__ src, const int* __restrict__ src_list) {
+// The node velocities of a store slot back into the grid, where the G2P
+// adjoint gathers them (the grid adjoint reads the momenta from the slot).
+__global__ void __launch_bounds__(256) k_restore_grid(float4* __restrict__ vel, const float4* __restrict__ src,
+                                                      const int* __restrict__ src_list) {
     const long long total = (long long)__ldg(src_list) * 64;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const long long slot = idx >> 6;
         const int in_block = (int)(idx & 63);
         const int b = __ldg(src_list + 1 + slot);
-        const long long node = ((long long)b << 6) | in_block;
-        mom[node] = __ldg(src + slot * 128 + in_block);
-        vel[node] = __ldg(src + slot * 128 + 64 + in_block);
-        if (in_block == 0) flags[b] = 1;
+        vel[((long long)b << 6) | in_block] = __ldg(src + slot * 128 + 64 + in_block);
     }
 }
 

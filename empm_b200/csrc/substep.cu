@@ -1301,11 +1301,11 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         const ParticleArrays Pk = particle_arrays(d.states + (size_t)k * state_floats, n);
         const Launch Lk = make_launch(ctx, k);
         F9Planes Fk = Fe;
+        const float4* slot = d.store ? d.gsave + (size_t)k * d.cap_blocks * 128 : nullptr;
+        const int* slot_list = d.store ? d.glist + (size_t)k * (d.cap_blocks + 1) : nullptr;
         if (d.store) {
             Fk = f9_planes(d.fe + (size_t)k * 9 * np, n);
-            k_restore_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_mom, ctx->grid_vel, ctx->flags,
-                                                     d.gsave + (size_t)k * d.cap_blocks * 128,
-                                                     d.glist + (size_t)k * (d.cap_blocks + 1));
+            k_restore_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_vel, slot, slot_list);
             CK(cudaGetLastError(), "k_restore_grid");
         } else {
             CK(cudaMemcpyAsync(ab.work, snap, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, s),
@@ -1344,7 +1344,8 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         gg.flags = ctx->flags;
         gg.L = Lk;
         timing_mark(ctx, 4, 0, s);
-        k_adj_grid<<<(int)nb, 256, 0, s>>>(gg);
+        if (d.store) k_adj_grid_stored<<<grid_ctas, 256, 0, s>>>(gg, slot, slot_list);
+        else k_adj_grid<<<(int)nb, 256, 0, s>>>(gg);
         timing_mark(ctx, 4, 1, s);
         CK(cudaGetLastError(), "k_adj_grid");
         AdjP2GArgs ap;
