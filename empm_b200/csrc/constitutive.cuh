@@ -131,6 +131,9 @@ EMPM_HD bool viscoplastic(const M3& U, V3& s, const M3& V, float mu, float ys, f
 
 // Return map + stress for one particle. mu, lam, ys are read and, for the
 // von Mises models, updated in place.
+// MAT >= 0 compiles the update for that material only (a batch whose
+// instances all use it); -1 switches on ms.material.
+template <int MAT = -1>
 EMPM_HD ConstitutiveOut constitutive(const M3& Ft, float& mu, float& lam, float& ys, float dt,
                                      const MaterialScalars& ms) {
     ConstitutiveOut out;
@@ -139,7 +142,8 @@ EMPM_HD ConstitutiveOut constitutive(const M3& Ft, float& mu, float& lam, float&
     V3 s;
     svd3(Ft, U, s, V);
     M3 F = Ft;
-    switch (ms.material) {
+    const int material = MAT >= 0 ? MAT : ms.material;
+    switch (material) {
         case 1: von_mises(U, s, V, mu, lam, ys, ms, false, out.mat_changed, F); break;
         case 2: sand(U, s, V, mu, lam, ms, F); break;
         case 3: viscoplastic(U, s, V, mu, ys, dt, ms, F); break;
@@ -149,7 +153,7 @@ EMPM_HD ConstitutiveOut constitutive(const M3& Ft, float& mu, float& lam, float&
     // F = U diag(s) V^T (after the return maps too), so det F = s.x s.y s.z
     const float J = s.x * s.y * s.z;
     M3 tau = m3_zero();
-    switch (ms.material) {
+    switch (material) {
         case 0:
         case 5: {  // fixed-corotated (mpm_utils.py:8-15): 2 mu (F - R) F^T + lam J (J - 1) I, R = U V^T
             const float d = lam * J * (J - 1.f);

@@ -162,6 +162,7 @@ struct MaterialArrays {
 
 // Stress + everything P2G needs for particle p (modifiers applied, material
 // write-back, elastic F handed to G2P). Returns false for unsimulated particles.
+template <int MAT = -1>
 __device__ __forceinline__ bool prepare_particle(const ParticleArrays& P, const MaterialArrays& M, F9Planes Fe,
                                                  const StepConsts& c, int p, P2GParticle& q) {
     if (M.sel && __ldg(M.sel + p) != 0) return false;
@@ -176,7 +177,7 @@ __device__ __forceinline__ bool prepare_particle(const ParticleArrays& P, const 
         if (apply_modifiers(st, mi, x, xm.w, v)) P.v[p] = make_float4(v.x, v.y, v.z, vv.w);
     }
     float mu = __ldg(M.mu + p), lam = __ldg(M.lam + p), ys = __ldg(M.ys + p);
-    const ConstitutiveOut co = constitutive(f9_load(P.F, p), mu, lam, ys, st.dt, c.ms);
+    const ConstitutiveOut co = constitutive<MAT>(f9_load(P.F, p), mu, lam, ys, st.dt, c.ms);
     f9_store(Fe, p, co.F);
     if (co.mat_changed) { M.mu[p] = mu; M.lam[p] = lam; M.ys[p] = ys; }
     q.st = make_stencil(x, c.inv_dx);
@@ -566,7 +567,7 @@ __global__ void k_unsort(const UnsortArgs a) {
 // Same-cell runs are split every seg_cap = 2^ROUNDS lanes, so a segment sums
 // in at most ROUNDS shuffle rounds; the rounds a run cap never needs are not
 // compiled in (smaller code for the instruction cache).
-template <int ROUNDS>
+template <int ROUNDS, int MAT = -1>
 __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
                                                      float4* grid, unsigned char* flags) {
     constexpr int seg_cap = 1 << ROUNDS;
@@ -576,7 +577,7 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
     const StepConsts c = consts_of(L, inst);
     P2GParticle q;
     bool valid = false;
-    if (p < L.n_total) valid = prepare_particle(P, M, Fe, c, p, q);
+    if (p < L.n_total) valid = prepare_particle<MAT>(P, M, Fe, c, p, q);
     // a segment is a run of lanes with the same validity, instance and base
     // cell; lanes without a particle contribute zeros and never write
     const int b0 = valid ? q.st.b[0] : lane, b1 = valid ? q.st.b[1] : 0, b2 = valid ? q.st.b[2] : 0;
@@ -634,10 +635,17 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
     if (head && valid) mark_stencil_blocks(flags, q.st, c);
 }
 
-// k_p2g_warpagg for a run cap seg_cap (a power of two in 1..32)
+// k_p2g_warpagg for a run cap seg_cap (a power of two in 1..32). material:
+// the material id every instance of the launch uses, or -1 when they differ;
+// plasticine (5) and jelly (0) at run caps 4 and 8 have kernels compiled for
+// that material alone.
 static inline void launch_p2g_warpagg(int grid_ctas, int threads, cudaStream_t s, const ParticleArrays& P,
                                       const MaterialArrays& M, const F9Planes& Fe, const Launch& L, float4* mom,
-                                      unsigned char* flags, int seg_cap) {
+                                      unsigned char* flags, int seg_cap, int material = -1) {
+    if (material == 5 && seg_cap == 4) { k_p2g_warpagg<2, 5><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); return; }
+    if (material == 5 && seg_cap == 8) { k_p2g_warpagg<3, 5><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); return; }
+    if (material == 0 && seg_cap == 4) { k_p2g_warpagg<2, 0><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); return; }
+    if (material == 0 && seg_cap == 8) { k_p2g_warpagg<3, 0><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); return; }
     switch (seg_cap) {
         case 1: k_p2g_warpagg<0><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;
         case 2: k_p2g_warpagg<1><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, mom, flags); break;

@@ -542,6 +542,15 @@ static int particle_threads(const EmpmCtx* ctx, long long n, int usual) {
     return blocks_for(n, usual) >= 2LL * ctx->sm_count ? usual : 64;
 }
 
+// The material id all instances share, or -1 when they differ.
+static int uniform_material(const EmpmCtx* ctx) {
+    if (ctx->n_inst < 1) return -1;
+    const int m = ctx->params[0].material;
+    for (int i = 1; i < ctx->n_inst; ++i)
+        if (ctx->params[i].material != m) return -1;
+    return m;
+}
+
 // Optional store slot for launch_grid_update_list (stored segments).
 struct GridStoreSlot {
     float4* blocks;
@@ -753,7 +762,7 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaS
     if (ctx->p2g_mode == 2) {
         const int tp = particle_threads(ctx, n, 256);
         launch_p2g_warpagg(blocks_for(n, tp), tp, stream, t.P, t.M, t.Fe, t.L, ctx->grid_mom, ctx->flags,
-                           ctx->seg_cap);
+                           ctx->seg_cap, uniform_material(ctx));
     } else {
         k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
     }
@@ -1189,7 +1198,8 @@ static int launch_substep_arrays(EmpmCtx* ctx, const ParticleArrays& Pin, const 
     const int n = ctx->n_particles;
     const Launch L = make_launch(ctx, table);
     timing_mark(ctx, 0, 0, s);
-    if (warpagg) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, M, Fe, L, ctx->grid_mom, ctx->flags, ctx->seg_cap);
+    if (warpagg) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, M, Fe, L, ctx->grid_mom, ctx->flags, ctx->seg_cap,
+                                    uniform_material(ctx));
     else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, M, Fe, L, ctx->grid_mom, ctx->flags);
     timing_mark(ctx, 0, 1, s);
     CK(cudaGetLastError(), "adjoint segment P2G");
@@ -1252,7 +1262,7 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
         const Launch Lk = make_launch(ctx, k);
         timing_mark(ctx, 0, 0, s);
         if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
-                                         ctx->seg_cap);
+                                         ctx->seg_cap, uniform_material(ctx));
         else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
         timing_mark(ctx, 0, 1, s);
         CK(cudaGetLastError(), "adjoint segment P2G");
@@ -1313,7 +1323,7 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
             const Launch Lrec = make_launch(ctx, n_steps + k);
             timing_mark(ctx, 0, 0, s);
             if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pk, Mw, Fe, Lrec, ctx->grid_mom,
-                                             ctx->flags, ctx->seg_cap);
+                                             ctx->flags, ctx->seg_cap, uniform_material(ctx));
             else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pk, Mw, Fe, Lrec, ctx->grid_mom, ctx->flags);
             timing_mark(ctx, 0, 1, s);
             CK(cudaGetLastError(), "P2G (adjoint recompute)");
