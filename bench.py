@@ -57,7 +57,7 @@ def load_peaks():
 # the dominant kernel, from one ncu capture of exactly this workload and
 # particle count on a B200: (workload, kernel, particles) -> bytes per launch.
 NCU_DRAM_BYTES = {
-    ("c4", "stress_p2g", 3172508): 403.2064e6 + 111.232e6,
+    ("c4", "stress_p2g", 3172508): 403.197184e6 + 110.350592e6,
     ("lbs", "blend", 2000000): 196.818688e6 + 41.4976e6,
 }
 
