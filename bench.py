@@ -67,6 +67,29 @@ def measured_traffic(workload: str, kernel: str, particles: int):
     return NCU_DRAM_BYTES.get((workload, kernel, int(particles)))
 
 
+def rollout_launches(n_steps: int, block: int, sort_every: int, resume: bool) -> int:
+    """This library's kernel launches in one sorted rollout of n_steps
+    substeps run as graph blocks of `block` substeps: 4 per substep (P2G,
+    block list, grid update, G2P), 4 per cell sort (keys, chunk counts, cell
+    scan, scatter; its two CUB scans are not counted) and 1 per write-back."""
+    if sort_every <= 0:
+        return 4 * n_steps   # the direct path: no sort, the caller's buffers throughout
+    sorts = unsorts = 0
+    done, since = 0, 0
+    while done < n_steps:
+        k = min(block, n_steps - done)
+        if not (resume and done > 0):
+            sorts, since = sorts + 1, 0
+        for _ in range(k):
+            if since >= sort_every:
+                sorts, since = sorts + 1, 0
+            since += 1
+        if not resume or done + k >= n_steps:
+            unsorts += 1
+        done += k
+    return 4 * n_steps + 4 * sorts + unsorts
+
+
 def bytes_per_particle(material: str):
     """Algorithmic bytes per particle-substep: x, v, C, F read + written
     (192 B) and mass, vol, mu, lam read (16 B); plasticine adds the yield read
@@ -368,7 +391,7 @@ def run_ours(args):
                                f"rollout in this run ({stream_ms:.2f} ms vs {ms / args.steps:.2f} ms graph)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": 3 * w.T * args.steps,
+        "gpu_launches": rollout_launches(w.T, w.T, solver.sort_every, False) * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -648,7 +671,7 @@ def run_ours_c4(args):
                                f"population rollout in this run ({stream_ms:.2f} ms vs {ms / args.steps:.2f} ms graph)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": total * 36, "d2h_bytes_per_step": total * 12},
-        "gpu_launches": 3 * T * args.steps,
+        "gpu_launches": rollout_launches(T, 50, batch.sort_every, batch.resume_blocks) * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -1062,7 +1085,10 @@ def run_ours_c5(args):
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d[0], "d2h_bytes_per_step":
                 sum(r[2] * (24 if not r[1] else 24) for r in ok),
                 "path": "MPMServer.submit with host (numpy) requests -> results on the host"},
-        "gpu_launches": 3 * stats["substeps"] + 8 * n_grad_substeps,
+        # 4 per forward substep of a block (P2G, block list, grid update, G2P) and 8 per substep of a
+        # gradient request's adjoint (its segment re-run and reverse pass); cell sorts and write-backs
+        # are not counted
+        "gpu_launches": 4 * stats["substeps"] + 8 * n_grad_substeps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
