@@ -160,3 +160,25 @@ def test_malformed_requests_raise():
     with pytest.raises(ValueError):
         r.validate()
     _req().validate()
+
+
+def test_capacity_budget_charges_the_adjoint_store():
+    """The adjoint engine's share of the budget includes its per-substep store
+    (touched grid blocks, 2 KiB + 4 B each, and elastic F, 36 B per particle,
+    for every substep of a segment); the rest is split between arena, grids
+    and checkpoints."""
+    from empm_b200.serving import capacity_for_budget
+
+    budget = 60 << 30
+    a = capacity_for_budget(budget, every=50, adjoint_particles=1_000_000, adjoint_grid=160)
+    b = capacity_for_budget(budget, every=25, adjoint_particles=1_000_000, adjoint_grid=160)
+    blocks = grid_blocks(160)
+    store_50 = 50 * (blocks * (128 * 16 + 4) + 1_000_000 * 36)
+    store_25 = 25 * (blocks * (128 * 16 + 4) + 1_000_000 * 36)
+    # halving the segment length frees the store difference (and the segment states) for the other shares
+    assert b.ckpt_bytes > a.ckpt_bytes
+    freed = (b.ckpt_bytes - a.ckpt_bytes) / 0.35
+    assert freed >= store_50 - store_25
+    assert a.adjoint_blocks == blocks and a.adjoint_particles == 1_000_000
+    with pytest.raises(ValueError):
+        capacity_for_budget(store_50 // 2, every=50, adjoint_particles=1_000_000, adjoint_grid=160)
