@@ -355,10 +355,12 @@ typedef struct {
  * The segment is recomputed from the checkpoint and the state of every
  * substep is kept in context-owned memory: about 120 bytes per particle and
  * substep, allocated on first use and grown as needed (so call it outside
- * stream capture). The adjoint of each substep then recomputes that substep's
- * grid and runs the three adjoint kernels. The result is the gradient of the
- * FP32 forward map, up to FP32 rounding. The velocity written by a rotation
- * modifier is treated as independent of x. */
+ * stream capture). With EMPM_OPT_ADJ_STORE (the default) the re-run also
+ * keeps each substep's touched grid blocks and elastic F, and the reverse pass
+ * reads them; otherwise it recomputes each substep's grid first. Then the
+ * three adjoint kernels run. The result is the gradient of the FP32 forward
+ * map, up to FP32 rounding. The velocity written by a rotation modifier is
+ * treated as independent of x. */
 int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* ckpt_mu, const float* ckpt_lam,
                           const float* ckpt_yield, const EmpmMaterial* mat, const EmpmStep* steps, int n_steps,
                           EmpmParticles* grad, EmpmMaterialGrad* gmat, void* stream);
