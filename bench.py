@@ -153,7 +153,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(args):
+def dist_setup(args, backend: str = "nccl"):
+    """(world, rank, local rank) from the launcher's environment; with more
+    than one rank, the process group (NCCL on this rank's GPU, or gloo)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -163,10 +165,34 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device(f"cuda:{local}"))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device(f"cuda:{local}"))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def rank_barrier(world: int) -> None:
+    """Barrier over the job's ranks (nothing with one rank)."""
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def rank_max(x: float, world: int, device) -> float:
+    """The maximum of x over the job's ranks, reduced on `device` (the
+    backend's: this rank's GPU for NCCL, "cpu" for gloo)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def get_workload(name, particles=None, grid=None, substeps=None):
@@ -279,19 +305,10 @@ def run_ours(args):
         solver.rollout(md, st, other, w.dt, w.T, schedule=schedule)
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x):
-        if world > 1:
-            import torch.distributed as dist
-
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return rank_max(x, world, dev)
 
     for _ in range(args.warmup):
         step()
@@ -494,19 +511,10 @@ def run_ours_c4(args):
         batch.rollout(dt, T, block=50)
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x):
-        if world > 1:
-            import torch.distributed as dist
-
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return rank_max(x, world, dev)
 
     for _ in range(args.warmup):
         step()
@@ -747,19 +755,10 @@ def run_ours_c3(args):
         return (diff * diff).sum(1).mean(), g_E.sum(), g_nu.sum(), res["yield_stress"].sum()
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x):
-        if world > 1:
-            import torch.distributed as dist
-
-            tt = torch.tensor([x], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            return float(tt.item())
-        return x
+        return rank_max(x, world, dev)
 
     for _ in range(args.warmup):
         out = grad_step()
@@ -1152,19 +1151,10 @@ def run_ours_lbs(args):
         return mi(prev, cur, xyz, quat)
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
+        rank_barrier(world)
 
     def max_over_ranks(x):
-        if world > 1:
-            import torch.distributed as dist
-
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return rank_max(x, world, dev)
 
     for _ in range(args.warmup):
         step()

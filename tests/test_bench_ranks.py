@@ -1,0 +1,58 @@
+"""The multi-rank plumbing of bench.py on CPU: two gloo ranks set up from the
+launcher's environment, meet at the barrier, and agree on the maximum of
+their timings (the bench reports the slowest rank). The same helpers run
+over NCCL when bench.py is launched on GPUs."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port() -> int:
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, out_dir: str) -> None:
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+
+    import bench
+
+    w, r, local = bench.dist_setup(None, backend="gloo")
+    try:
+        bench.rank_barrier(w)
+        slowest = bench.rank_max(1.5 * (r + 1), w, "cpu")
+        with open(os.path.join(out_dir, f"rank{r}.txt"), "w") as f:
+            f.write(f"{w} {r} {local} {slowest}")
+        bench.rank_barrier(w)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_agree_on_the_slowest(tmp_path):
+    world = 2
+    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for r in range(world):
+        w, rank, local, slowest = open(tmp_path / f"rank{r}.txt").read().split()
+        assert (int(w), int(rank), int(local)) == (world, r, r)
+        assert float(slowest) == pytest.approx(3.0)
+
+
+def test_one_rank_needs_no_process_group(monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    assert bench.dist_setup(None) == (1, 0, 0)
+    bench.rank_barrier(1)
+    assert bench.rank_max(2.5, 1, "cpu") == 2.5
