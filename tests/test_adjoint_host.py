@@ -155,3 +155,32 @@ def test_block_capacity_estimate_and_oversized_segments(fake_lib):
     assert t._allocate_segments(ctx, "cpu", t._block_cap(ctx, 200_000))
     t.release()                                          # right-sized: pooled
     assert ctx.pooled(4, 141) == 2
+
+
+def test_overflow_check_updates_the_estimate(fake_lib):
+    """_blocks_overflowed reads each segment's touched-block maximum once,
+    keeps the largest as the context's estimate and reports a segment whose
+    slots were too few."""
+    maxima = {}
+
+    def blocks(seg, max_touched, block_cap, stream):
+        touched, cap = maxima[seg.value]
+        max_touched._obj.value = touched
+        block_cap._obj.value = cap
+        return N.EMPM_OK
+
+    fake_lib.empm_segment_blocks = blocks
+    ctx = _fake_ctx(fake_lib)
+    t = _tape(10, 4, budget=10 ** 9)
+    assert t._allocate_segments(ctx, "cpu", 100)
+    ids = [sg.ptr.value for sg in t.segments]
+    maxima.update({ids[0]: (60, 100), ids[1]: (90, 100), ids[2]: (40, 100)})
+    assert not t._blocks_overflowed(ctx, None)
+    assert ctx.touched_blocks == 90
+    maxima[ids[1]] = (130, 100)
+    assert t._blocks_overflowed(ctx, None)
+    assert ctx.touched_blocks == 130
+    assert t._block_cap(ctx, 10 ** 6) == int(130 * 1.25) + 16
+    maxima[ids[1]] = (20, 100)                 # a smaller pass keeps the larger estimate
+    assert not t._blocks_overflowed(ctx, None)
+    assert ctx.touched_blocks == 130
