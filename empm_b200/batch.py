@@ -262,12 +262,7 @@ class BatchedMPM:
             k = min(block, n_steps - done)
             table, n_tables = self._schedule(dt, k)
             a, b = self._views(self.cur), self._views(1 - self.cur)
-            flags = N.ROLLOUT_GRAPH if self.use_graph else 0
-            if self.resume_blocks:
-                if done > 0:
-                    flags |= N.ROLLOUT_RESUME
-                if done + k < n_steps:
-                    flags |= N.ROLLOUT_KEEP
+            flags = block_flags(done, k, n_steps, self.use_graph, self.resume_blocks)
             with torch.cuda.device(self.device):
                 N.check(self.L.empm_rollout_ex(self.ptr, a, b, mat, table, n_tables, k, flags, stream), self.ptr)
             if k % 2 == 1:
@@ -297,6 +292,20 @@ class BatchedMPM:
                 self.ptr = None
         except Exception:
             pass
+
+
+def block_flags(done: int, k: int, n_steps: int, use_graph: bool, resume: bool) -> int:
+    """empm_rollout_ex flags of the block of k substeps that starts after
+    `done` of a rollout of n_steps: a graph when asked; with `resume`, every
+    block but the first continues from the library's sorted state and every
+    block but the last keeps its result there."""
+    flags = N.ROLLOUT_GRAPH if use_graph else 0
+    if resume:
+        if done > 0:
+            flags |= N.ROLLOUT_RESUME
+        if done + k < n_steps:
+            flags |= N.ROLLOUT_KEEP
+    return flags
 
 
 def single_instance(spec: InstanceSpec, device="cuda:0"):
