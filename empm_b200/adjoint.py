@@ -128,7 +128,9 @@ class CheckpointedRollout:
     stores every segment and raises MemoryError when they do not fit; False
     checkpoints. None stores when the whole rollout fits ``store_budget`` bytes
     (default: half of the device memory free at the forward pass) and the
-    allocation succeeds, and checkpoints otherwise.
+    allocation succeeds, and checkpoints otherwise. Released segments return
+    to the solver context's pool and are reused in stream order, so one
+    solver's rollouts should run on one CUDA stream.
     """
 
     def __init__(self, solver, model: MPMModelStruct, state: MPMStateStruct, dt: float, n_steps: int,
@@ -316,6 +318,9 @@ class CheckpointedRollout:
         """Adjoint of the whole rollout. g_* are dL/d(final state); g_records[r]
         is dL/d(record r). Returns dL/d(initial x, v, C, F_trial, mu, lam,
         yield_stress, mass)."""
+        if not self.segments and not self.ckpts:
+            raise RuntimeError("nothing to differentiate: forward() has not run, or its stored segments were "
+                               "released (release(), or a backward through the autograd Functions)")
         st, model = self.state, self.model
         n = st.n_particles
         dev = st.device

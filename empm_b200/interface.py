@@ -143,6 +143,7 @@ class MPMDifferentiableSimulationTrail(autograd.Function):
         # interface.py:178-197: the record gradients are summed over time and
         # injected at the final state
         res = ctx.tape.backward(g_x=out_pos_grad.sum(dim=0))
+        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         velo_grad = res["v"] if ctx.on_tape else torch.zeros_like(res["v"])
         density_grad = _masked_density(density_grad if ctx.on_tape else torch.zeros_like(density_grad),
@@ -184,6 +185,7 @@ class MPMDifferentiableSimulation(autograd.Function):
     @staticmethod
     def backward(ctx, out_pos_grad):
         res = ctx.tape.backward(g_x=out_pos_grad)
+        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         velo_grad = res["v"] if ctx.on_tape else torch.zeros_like(res["v"])
         density_grad = _masked_density(density_grad if ctx.on_tape else torch.zeros_like(density_grad),
@@ -217,6 +219,7 @@ class MPMDifferentiableSimulationWCheckpoint(autograd.Function):
     @staticmethod
     def backward(ctx, out_pos_grad, out_velo_grad, out_F_grad, out_C_grad):
         res = ctx.tape.backward(g_x=out_pos_grad, g_v=out_velo_grad, g_C=out_C_grad, g_F=out_F_grad)
+        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         return (None, None, None, None, None, res["x"], res["v"], res["F"], res["C"], E_grad, nu_grad, density_grad,
                 None, None, None, None)
@@ -251,6 +254,7 @@ class MPMDifferentiableSimulationClean(autograd.Function):
         # the covariance output is a pass-through (its update is disabled in the
         # reference, mpm_utils.py:578), so its gradient does not reach the inputs
         res = ctx.tape.backward(g_x=out_pos_grad, g_v=out_velo_grad, g_C=out_C_grad, g_F=out_F_grad)
+        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         return (None, None, None, None, None, res["x"], res["v"], res["F"], res["C"], E_grad, nu_grad, density_grad,
                 None, None, None, None)

@@ -184,3 +184,9 @@ def test_overflow_check_updates_the_estimate(fake_lib):
     maxima[ids[1]] = (20, 100)                 # a smaller pass keeps the larger estimate
     assert not t._blocks_overflowed(ctx, None)
     assert ctx.touched_blocks == 130
+
+
+def test_backward_without_forward_data_raises():
+    t = CheckpointedRollout(None, None, None, 1e-4, 10, checkpoint_every=4)
+    with pytest.raises(RuntimeError, match="nothing to differentiate"):
+        t.backward()
