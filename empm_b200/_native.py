@@ -118,7 +118,7 @@ def lib():
         "empm_batch_reconfigure": ([P, P, P, I, P], I),
         "empm_substep_noalloc": ([ctypes.POINTER(EmpmModelParams), ctypes.POINTER(EmpmParticles),
                                   ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterial),
-                                  ctypes.POINTER(EmpmStep), I, P], I),
+                                  ctypes.POINTER(EmpmStep), I, P, P], I),
         "empm_read_status": ([P, ctypes.POINTER(ctypes.c_uint32), P], I),
         "empm_last_error": ([P, ctypes.c_char_p, I], I),
         "empm_debug_stress": ([ctypes.POINTER(EmpmModelParams), P, P, P, P, ctypes.c_float, P, P, I, P], I),

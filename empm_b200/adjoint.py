@@ -161,10 +161,12 @@ class CheckpointedRollout:
         return bool(self.segments)
 
     def release(self) -> None:
-        """Free the stored segments (a later backward is then impossible)."""
+        """Hand the stored segments back to the pool and drop the checkpoints
+        (a later backward then raises)."""
         for sg in self.segments:
             sg.release()
         self.segments = []
+        self.ckpts = []
 
     def __del__(self):
         try:
@@ -319,8 +321,8 @@ class CheckpointedRollout:
         is dL/d(record r). Returns dL/d(initial x, v, C, F_trial, mu, lam,
         yield_stress, mass)."""
         if not self.segments and not self.ckpts:
-            raise RuntimeError("nothing to differentiate: forward() has not run, or its stored segments were "
-                               "released (release(), or a backward through the autograd Functions)")
+            raise RuntimeError("nothing to differentiate: forward() has not run, or its tape was released "
+                               "(release(), or a later differentiable forward pass on the same solver)")
         st, model = self.state, self.model
         n = st.n_particles
         dev = st.device

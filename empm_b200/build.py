@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import argparse
 import glob
+import hashlib
 import os
 import shutil
 import subprocess
@@ -30,11 +31,34 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _stale(target: str, sources) -> bool:
-    if not os.path.exists(target):
-        return True
-    t = os.path.getmtime(target)
-    return any(os.path.getmtime(s) > t for s in sources)
+def _digest(paths, extra) -> str:
+    h = hashlib.sha256()
+    for p in paths:
+        h.update(os.path.basename(p).encode())
+        with open(p, "rb") as f:
+            h.update(f.read())
+    h.update(" ".join(extra).encode())
+    return h.hexdigest()
+
+
+def _stamp_path(target: str) -> str:
+    return target + ".sha256"
+
+
+def _up_to_date(target: str, digest: str) -> bool:
+    """True when target exists and was built from sources with this digest
+    (content hashes, not modification times: a stale object copied in with a
+    newer time stamp is rebuilt all the same)."""
+    stamp = _stamp_path(target)
+    if not (os.path.exists(target) and os.path.exists(stamp)):
+        return False
+    with open(stamp) as f:
+        return f.read().strip() == digest
+
+
+def _write_stamp(target: str, digest: str) -> None:
+    with open(_stamp_path(target), "w") as f:
+        f.write(digest + "\n")
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
@@ -43,20 +67,25 @@ def build(verbose: bool = False, force: bool = False) -> str:
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     headers = sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) +
                      glob.glob(os.path.join(os.path.dirname(HERE), "include", "*.h")))
-    objs = []
+    objs, obj_digests = [], []
     for src in sources:
         obj = os.path.join(BUILD_DIR, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
-        if force or _stale(obj, [src] + headers):
+        digest = _digest([src] + headers, NVCC_FLAGS)
+        obj_digests.append(digest)
+        if force or not _up_to_date(obj, digest):
             cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
             if verbose:
                 cmd += ["-Xptxas", "-v"]
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
+            _write_stamp(obj, digest)
     target = os.path.join(OUT_DIR, "libempm_b200.so")
-    if force or _stale(target, objs):
+    link_digest = hashlib.sha256("".join(obj_digests).encode()).hexdigest()
+    if force or not _up_to_date(target, link_digest):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", target] + objs + ["-cudart", "static"]
         subprocess.run(cmd, check=True)
+        _write_stamp(target, link_digest)
     return target
 
 

@@ -480,6 +480,18 @@ static int check_particles(EmpmCtx* ctx, const EmpmParticles* p, const char* nam
     return EMPM_OK;
 }
 
+// True when a and b share any particle buffer (x, v, C or F_trial in either
+// role): the G2P of one substep would overwrite state that other threads of
+// the same launch still read.
+static bool particles_alias(const EmpmParticles* a, const EmpmParticles* b) {
+    const void* pa[4] = {a->x, a->v, a->C, a->F};
+    const void* pb[4] = {b->x, b->v, b->C, b->F};
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+            if (pa[i] == pb[j]) return true;
+    return false;
+}
+
 static int check_material(EmpmCtx* ctx, const EmpmMaterial* m) {
     if (!m || !m->vol || !m->mu || !m->lam || !m->yield_stress || !m->F_elastic)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "material pointer is NULL");
@@ -861,7 +873,7 @@ extern "C" int empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles
     if (!rc) rc = check_particles(ctx, out, "out");
     if (!rc) rc = check_material(ctx, mat);
     if (rc) return rc;
-    if (in->x == out->x) return empm_set_error(ctx, EMPM_ERR_INVALID, "in and out must be distinct buffers");
+    if (particles_alias(in, out)) return empm_set_error(ctx, EMPM_ERR_INVALID, "in and out must be distinct buffers");
     cudaStream_t s = (cudaStream_t)stream;
     rc = upload_steps(ctx, step, 1, s);
     if (rc) return rc;
@@ -875,7 +887,7 @@ extern "C" int empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b,
     if (!rc) rc = check_particles(ctx, b, "b");
     if (!rc) rc = check_material(ctx, mat);
     if (rc) return rc;
-    if (a->x == b->x) return empm_set_error(ctx, EMPM_ERR_INVALID, "a and b must be distinct buffers");
+    if (particles_alias(a, b)) return empm_set_error(ctx, EMPM_ERR_INVALID, "a and b must be distinct buffers");
     if (n_steps < 1 || n_steps > 100000) return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
     if (n_tables != 1 && n_tables != n_steps)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "n_tables must be 1 or n_steps (%d, %d)", n_tables, n_steps);
@@ -1881,6 +1893,17 @@ __device__ __align__(256) InstanceConsts g_noalloc_inst[1];
 __device__ __align__(256) EmpmStep g_noalloc_step[1];
 __device__ __align__(256) unsigned g_noalloc_status[1];
 
+// Writes the call's instance constants and schedule into the file-scope
+// arrays (device code names them directly) and clears the status word it
+// was given. Kernel arguments are copied when the launch is issued, so the
+// host's structs may go out of scope at once and no pageable host-to-device
+// copy (which would wait for the stream) is needed.
+__global__ void k_noalloc_setup(const InstanceConsts ic, const EmpmStep st, unsigned* status, int clear_status) {
+    g_noalloc_inst[0] = ic;
+    g_noalloc_step[0] = st;
+    if (clear_status) *status = 0u;
+}
+
 // Device addresses of the arrays above. In host code their names are host-side
 // stand-ins, not device addresses, so the addresses are looked up once per
 // device with cudaGetSymbolAddress while that device is current.
@@ -1916,7 +1939,8 @@ int noalloc_setup(int device, NoallocPtrs** out) {
 }  // namespace
 
 extern "C" int empm_substep_noalloc(const EmpmModelParams* params, const EmpmParticles* in, EmpmParticles* out,
-                                    const EmpmMaterial* mat, const EmpmStep* step, int n_particles, void* stream) {
+                                    const EmpmMaterial* mat, const EmpmStep* step, int n_particles,
+                                    uint32_t* status, void* stream) {
     EmpmCtx* ctx = nullptr;
     int rc = validate_params(nullptr, params);
     if (rc) return rc;
@@ -1932,7 +1956,7 @@ extern "C" int empm_substep_noalloc(const EmpmModelParams* params, const EmpmPar
     if (!rc) rc = check_particles(nullptr, out, "out");
     if (!rc) rc = check_material(nullptr, mat);
     if (rc) return rc;
-    if (in->x == out->x) return empm_set_error(nullptr, EMPM_ERR_INVALID, "in and out must be distinct buffers");
+    if (particles_alias(in, out)) return empm_set_error(nullptr, EMPM_ERR_INVALID, "in and out must be distinct buffers");
     int device = 0;
     CK(cudaGetDevice(&device), "cudaGetDevice");
     NoallocPtrs* P = nullptr;
@@ -1945,10 +1969,11 @@ extern "C" int empm_substep_noalloc(const EmpmModelParams* params, const EmpmPar
     // the arrays keep the previous call's contents: reset what must start at zero
     CK(cudaMemsetAsync(P->grid, 0, sizeof(float4) * (size_t)nblocks * 64, s), "clear grid scratch");
     CK(cudaMemsetAsync(P->flags, 0, (size_t)nblocks, s), "clear block flags");
-    CK(cudaMemsetAsync(P->status, 0, sizeof(unsigned), s), "clear status");
-    // pageable sources: the runtime stages them before returning
-    CK(cudaMemcpyAsync(P->inst, &ic, sizeof(InstanceConsts), cudaMemcpyHostToDevice, s), "upload instance");
-    CK(cudaMemcpyAsync(P->step, step, sizeof(EmpmStep), cudaMemcpyHostToDevice, s), "upload step");
+    // the caller's status word accumulates across calls (the caller clears it);
+    // the internal one is cleared every call
+    unsigned* status_word = status ? reinterpret_cast<unsigned*>(status) : P->status;
+    k_noalloc_setup<<<1, 1, 0, s>>>(ic, *step, status_word, status ? 0 : 1);
+    CK(cudaGetLastError(), "k_noalloc_setup");
     Launch L;
     L.inst = P->inst;
     L.n_inst = 1;
@@ -1956,7 +1981,7 @@ extern "C" int empm_substep_noalloc(const EmpmModelParams* params, const EmpmPar
     L.nblocks = (int)nblocks;
     L.steps = P->step;
     L.table = 0;
-    L.status = P->status;
+    L.status = status_word;
     const ParticleArrays Pin = particle_arrays(in, n_particles);
     const ParticleArrays Pout = particle_arrays(out, n_particles);
     MaterialArrays M;

@@ -25,9 +25,17 @@ and their quirks, follow the reference's backward passes:
   extra_no_grad_steps > 0, Simulation and Trail therefore return zero velocity
   and density gradients (their inputs are not on the tape), while
   WCheckpoint / Clean return the gradients at the state after the extra steps.
+
+A forward pass keeps its tape (stored segments or checkpoints) until the next
+differentiable forward pass on the same solver, or until its graph is freed.
+So a graph may be backpropagated more than once (retain_graph=True) until
+then, as the reference's Warp tape allows; the next forward hands the tape's
+segments back to the solver's pool before it allocates its own, so two sets
+are never held at once, and a backward through the older graph then raises.
 """
 from __future__ import annotations
 
+import weakref
 from typing import Optional
 
 import torch
@@ -68,10 +76,23 @@ def _run(mpm_solver, mpm_model, state, n_steps, dt, record_every=None, step_call
     return cur, recorded
 
 
+def _new_tape(mpm_solver, *args, **kw) -> CheckpointedRollout:
+    """A tape for a differentiable forward pass. The solver's previous tape
+    (if its graph is still alive) is released first: its segments go back to
+    the pool and this pass reuses them."""
+    prev = getattr(mpm_solver, "_live_tape", None)
+    prev = prev() if prev is not None else None
+    if prev is not None:
+        prev.release()
+    tape = CheckpointedRollout(mpm_solver, *args, **kw)
+    mpm_solver._live_tape = weakref.ref(tape)
+    return tape
+
+
 def _taped_run(mpm_solver, mpm_model, state, n_steps, dt, step_callback=None):
-    tape = CheckpointedRollout(mpm_solver, mpm_model, state, dt, n_steps,
-                               checkpoint_every=int(getattr(mpm_solver, "checkpoint_every", CHECKPOINT_EVERY)),
-                               step_callback=step_callback)
+    tape = _new_tape(mpm_solver, mpm_model, state, dt, n_steps,
+                     checkpoint_every=int(getattr(mpm_solver, "checkpoint_every", CHECKPOINT_EVERY)),
+                     step_callback=step_callback)
     return tape, tape.forward()
 
 
@@ -129,9 +150,9 @@ class MPMDifferentiableSimulationTrail(autograd.Function):
                                    step_callback=mpm_solver.step_callback)
             ctx.final_state = final
             return torch.stack(recorded, dim=0)
-        tape = CheckpointedRollout(mpm_solver, mpm_model, prev, substep_size, num_substeps,
-                                   checkpoint_every=int(getattr(mpm_solver, "checkpoint_every", CHECKPOINT_EVERY)),
-                                   record_every=substep, step_callback=mpm_solver.step_callback)
+        tape = _new_tape(mpm_solver, mpm_model, prev, substep_size, num_substeps,
+                         checkpoint_every=int(getattr(mpm_solver, "checkpoint_every", CHECKPOINT_EVERY)),
+                         record_every=substep, step_callback=mpm_solver.step_callback)
         ctx.final_state = tape.forward()
         ctx.tape, ctx.tape_state, ctx.mpm_model = tape, prev, mpm_model
         ctx.on_tape = extra_no_grad_steps == 0
@@ -143,7 +164,6 @@ class MPMDifferentiableSimulationTrail(autograd.Function):
         # interface.py:178-197: the record gradients are summed over time and
         # injected at the final state
         res = ctx.tape.backward(g_x=out_pos_grad.sum(dim=0))
-        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         velo_grad = res["v"] if ctx.on_tape else torch.zeros_like(res["v"])
         density_grad = _masked_density(density_grad if ctx.on_tape else torch.zeros_like(density_grad),
@@ -185,7 +205,6 @@ class MPMDifferentiableSimulation(autograd.Function):
     @staticmethod
     def backward(ctx, out_pos_grad):
         res = ctx.tape.backward(g_x=out_pos_grad)
-        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         velo_grad = res["v"] if ctx.on_tape else torch.zeros_like(res["v"])
         density_grad = _masked_density(density_grad if ctx.on_tape else torch.zeros_like(density_grad),
@@ -219,7 +238,6 @@ class MPMDifferentiableSimulationWCheckpoint(autograd.Function):
     @staticmethod
     def backward(ctx, out_pos_grad, out_velo_grad, out_F_grad, out_C_grad):
         res = ctx.tape.backward(g_x=out_pos_grad, g_v=out_velo_grad, g_C=out_C_grad, g_F=out_F_grad)
-        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         return (None, None, None, None, None, res["x"], res["v"], res["F"], res["C"], E_grad, nu_grad, density_grad,
                 None, None, None, None)
@@ -254,7 +272,6 @@ class MPMDifferentiableSimulationClean(autograd.Function):
         # the covariance output is a pass-through (its update is disabled in the
         # reference, mpm_utils.py:578), so its gradient does not reach the inputs
         res = ctx.tape.backward(g_x=out_pos_grad, g_v=out_velo_grad, g_C=out_C_grad, g_F=out_F_grad)
-        ctx.tape.release()   # the stored segments return to the pool for the next rollout
         E_grad, nu_grad, density_grad = _param_grads(ctx, res)
         return (None, None, None, None, None, res["x"], res["v"], res["F"], res["C"], E_grad, nu_grad, density_grad,
                 None, None, None, None)

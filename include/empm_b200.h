@@ -312,18 +312,25 @@ int  empm_last_error(EmpmCtx* ctx, char* buf, int len);
  * rendering loop, where a cudaMalloc could stall or fail, or code running
  * while another framework's memory pool must not grow. The caller passes the
  * inputs and outputs as for empm_substep (particles in the caller's order,
- * one schedule for the single instance described by params). The grid scratch
- * lives in file-scope device arrays sized for grids of at most
- * EMPM_NOALLOC_MAX_GRID^3 nodes (8 MiB, held by every GPU that loads the
- * library until the process exits); larger n_grid is rejected with
- * EMPM_ERR_INVALID. The first call on a device looks the arrays' device
+ * one schedule for the single instance described by params; in and out share
+ * no buffer). The grid scratch lives in file-scope device arrays sized for
+ * grids of at most EMPM_NOALLOC_MAX_GRID^3 nodes (8 MiB, held by every GPU
+ * that loads the library until the process exits); larger n_grid is rejected
+ * with EMPM_ERR_INVALID. The first call on a device looks the arrays' device
  * addresses up (cudaGetSymbolAddress), so make it before any stream capture.
- * Every call shares the arrays and clears them at its start: calls that
- * overlap on the GPU (different streams, threads or processes sharing the
- * library on one device) race and must be serialised by the caller. */
+ * The schedule and the instance constants reach the device as kernel
+ * arguments, so the call does not wait for the stream.
+ * status: NULL, or a device uint32 into which the kernels OR their
+ * EMPM_STATUS_* bits (NaN/Inf, CFL breach, stencil outside the grid); it is
+ * not cleared by the call, so it accumulates until the caller resets it.
+ * Every call in one process shares the arrays (each process that loads the
+ * library has its own copy) and clears them at its start: calls that overlap
+ * on the GPU (different streams or host threads of one process) race and
+ * must be serialised by the caller. */
 #define EMPM_NOALLOC_MAX_GRID 64
 int  empm_substep_noalloc(const EmpmModelParams* params, const EmpmParticles* in, EmpmParticles* out,
-                          const EmpmMaterial* mat, const EmpmStep* step, int n_particles, void* stream);
+                          const EmpmMaterial* mat, const EmpmStep* step, int n_particles, uint32_t* status,
+                          void* stream);
 
 /* ---- reverse mode ----------------------------------------------------------- */
 

@@ -47,6 +47,12 @@ typedef struct {
     real gravity[3];
     real rpic_damping, grid_v_damping_scale;
     real softening, hardening, xi, plastic_viscosity, alpha;
+    /* 1: the colliders' inside tests are evaluated as the reference's Warp
+     * kernels evaluate them, on float32 offsets float(i) * dx - point and
+     * float32 extents (mpm_solver_diff.py:612-672, 756-793, 835-858). A node
+     * plane can lie exactly on a collider face (x = 0.25 for a face at
+     * 0.30 - 0.05), and there the float32 and float64 tests disagree. */
+    int  pred32;
 } OrModel;
 
 /* gate: 0 off, 1 apply, 2 zero every node (same meaning as the library) */
@@ -396,6 +402,27 @@ static int inside_shape(int shape, const real* off, const OrCollider* c) {
     return 0;
 }
 
+/* inside_shape on float32 offsets and extents (OrModel.pred32) */
+static int inside_shape_f32(int shape, const float* off, const OrCollider* c) {
+    if (shape == 1)
+        return fabsf(off[0]) < (float)c->size[0] && fabsf(off[1]) < (float)c->size[1] &&
+               fabsf(off[2]) < (float)c->size[2];
+    const float nrm[3] = {(float)c->normal[0], (float)c->normal[1], (float)c->normal[2]};
+    if (shape == 2) return sqrtf(off[0] * off[0] + off[1] * off[1] + off[2] * off[2]) < (float)c->radius;
+    if (shape == 3) {
+        const float proj = off[0] * nrm[0] + off[1] * nrm[1] + off[2] * nrm[2];
+        const float rad[3] = {off[0] - proj * nrm[0], off[1] - proj * nrm[1], off[2] - proj * nrm[2]};
+        return fabsf(proj) < (float)c->half_height &&
+               sqrtf(rad[0] * rad[0] + rad[1] * rad[1] + rad[2] * rad[2]) < (float)c->radius;
+    }
+    if (shape == 4) return off[0] * nrm[0] + off[1] * nrm[1] + off[2] * nrm[2] < 0.0f;
+    return 0;
+}
+
+static int collider_inside(const OrModel* m, int shape, const real* off, const float* off32, const OrCollider* c) {
+    return m->pred32 ? inside_shape_f32(shape, off32, c) : inside_shape(shape, off, c);
+}
+
 /* grid_normalization_and_gravity + damping + colliders; grid_v_out is zeroed by the caller */
 void or_grid_update(const OrModel* m, const real* grid_m, const real* grid_v_in, real* grid_v_out,
                     const OrCollider* coll, int nc, real dt) {
@@ -416,10 +443,13 @@ void or_grid_update(const OrModel* m, const real* grid_m, const real* grid_v_in,
             if (cl->gate == 0) continue;
             if (cl->gate == 2) { vo[0] = vo[1] = vo[2] = 0; continue; }
             const real off[3] = {(real)i * m->dx - cl->point[0], (real)j * m->dx - cl->point[1], (real)k * m->dx - cl->point[2]};
+            const float dx32 = (float)m->dx;
+            const float off32[3] = {(float)i * dx32 - (float)cl->point[0], (float)j * dx32 - (float)cl->point[1],
+                                    (float)k * dx32 - (float)cl->point[2]};
             if (cl->kind == 1 || cl->kind == 2) {
                 const int shape = cl->kind == 1 ? 4 : cl->shape;
                 if (shape == 4) {
-                    if (dot3(off, cl->normal) < 0) {
+                    if (collider_inside(m, 4, off, off32, cl)) {
                         if (cl->surface_type == 11) {
                             const real z = (real)k * m->dx;
                             if (z < 0.4 || z > 0.53) { vo[0] = vo[1] = vo[2] = 0; }
@@ -428,17 +458,17 @@ void or_grid_update(const OrModel* m, const real* grid_m, const real* grid_v_in,
                             vo[0] = vo[1] = vo[2] = 0;
                         }
                     }
-                } else if (inside_shape(shape, off, cl)) {
+                } else if (collider_inside(m, shape, off, off32, cl)) {
                     vo[0] = vo[1] = vo[2] = 0;
                 }
             } else if (cl->kind == 3) {
-                if (inside_shape(cl->shape, off, cl)) {
+                if (collider_inside(m, cl->shape, off, off32, cl)) {
                     real c3[3];
                     cross3(cl->rot_axis, off, c3);
                     for (int r = 0; r < 3; ++r) vo[r] = cl->velocity[r] + cl->angular_velocity * c3[r];
                 }
             } else if (cl->kind == 4) {
-                if (fabs(off[0]) < cl->size[0] && fabs(off[1]) < cl->size[1] && fabs(off[2]) < cl->size[2])
+                if (collider_inside(m, 1, off, off32, cl))
                     for (int r = 0; r < 3; ++r) vo[r] = cl->velocity[r];
             } else if (cl->kind == 5) {
                 const int pad = 3;

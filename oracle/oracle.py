@@ -50,7 +50,7 @@ def _lib_struct(real):
             ("material", ctypes.c_int), ("gravity", real * 3),
             ("rpic_damping", real), ("grid_v_damping_scale", real),
             ("softening", real), ("hardening", real), ("xi", real),
-            ("plastic_viscosity", real), ("alpha", real),
+            ("plastic_viscosity", real), ("alpha", real), ("pred32", ctypes.c_int),
         ]
 
     class OrCollider(ctypes.Structure):
@@ -105,6 +105,8 @@ def lib(precision: str = "fp64") -> _Lib:
             _LIBS[precision] = _Lib(os.path.join(_BUILD, "liboracle64.so"), ctypes.c_double, np.float64)
         elif precision == "fp32_omp":
             _LIBS[precision] = _Lib(os.path.join(_BUILD, "liboracle32_omp.so"), ctypes.c_float, np.float32)
+        elif precision == "fp64_omp":
+            _LIBS[precision] = _Lib(os.path.join(_BUILD, "liboracle64_omp.so"), ctypes.c_double, np.float64)
         else:
             raise ValueError(precision)
     return _LIBS[precision]
@@ -211,7 +213,12 @@ class OracleSim:
     def __init__(self, x, v, vol, mass, E, nu, *, n_grid, grid_lim=1.0, material=0, gravity=(0.0, 0.0, 0.0),
                  yield_stress=None, softening=0.1, hardening=0.0, xi=0.0, plastic_viscosity=0.0,
                  friction_angle=25.0, rpic_damping=0.0, grid_v_damping_scale=1.1, selection=None,
-                 precision="fp64"):
+                 precision="fp64", collider_f32=False):
+        """collider_f32: keep the collider state as the reference's Warp
+        structs keep it, in float32 (kinematic collider points are rounded to
+        float32 after every move, mpm_solver_diff.py:795-801, 860-866), and
+        evaluate the inside tests on float32 offsets (OrModel.pred32). The
+        default keeps both in the oracle's precision."""
         self.L = lib(precision)
         R = self.L.np_real
         n = x.shape[0]
@@ -248,6 +255,8 @@ class OracleSim:
         m.xi = xi
         m.plastic_viscosity = plastic_viscosity
         m.alpha = alpha
+        m.pred32 = 1 if collider_f32 else 0
+        self.collider_f32 = bool(collider_f32)
         self.model = m
         g3 = self.G ** 3
         self.grid_m = np.zeros(g3, R)
@@ -309,6 +318,8 @@ class OracleSim:
         for c in self.colliders:
             if c.kind in (GRID_VELOCITY, CUBOID_VELOCITY) and c.start_time <= self.time < c.end_time:
                 c.point = tuple(p + dt * vv for p, vv in zip(c.point, c.velocity))
+                if self.collider_f32:
+                    c.point = tuple(float(np.float32(p)) for p in c.point)
         self.x, self.v, self.C, self.F_trial = x1, v1, C1, F1
         self.time = self.time + dt
 

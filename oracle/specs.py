@@ -65,10 +65,11 @@ def oracle_colliders(specs, mask=None):
 MATERIAL_IDS = {"jelly": 0, "metal": 1, "sand": 2, "foam": 3, "snow": 4, "plasticine": 5, "neo-hookean": 6}
 
 
-def sim_from_workload(w, precision="fp64"):
+def sim_from_workload(w, precision="fp64", collider_f32=False):
     """OracleSim for an empm_b200.workloads.Workload."""
     sim = O.OracleSim(w.x, w.v, w.vol, w.rho.astype(np.float64) * w.vol, w.E, w.nu, n_grid=w.G,
-                      material=MATERIAL_IDS[w.material], gravity=w.gravity, yield_stress=w.ys, precision=precision)
+                      material=MATERIAL_IDS[w.material], gravity=w.gravity, yield_stress=w.ys, precision=precision,
+                      collider_f32=collider_f32)
     sim.colliders = oracle_colliders(w.colliders)
     return sim
 
