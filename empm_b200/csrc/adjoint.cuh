@@ -397,6 +397,9 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
                 case EMPM_MOD_ROTATION:
                     if (mk == 1) gv = v3(0.f, 0.f, 0.f);
                     break;
+                case EMPM_MOD_SET_VELOCITY_LAYERED:
+                    if (mk >= (int)md.scale[0]) gv = v3(0.f, 0.f, 0.f);
+                    break;
                 case EMPM_MOD_MOVER:
                     if (mk == 1) gxa = gxa + md.scale[0] * cross(gv, v3(md.normal[0], md.normal[1], md.normal[2]));
                     break;

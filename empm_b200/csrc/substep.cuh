@@ -57,7 +57,8 @@ EMPM_HD bool stencil_in_grid(const Stencil& st, int G) {
 }
 
 // Pre-P2G particle velocity modifiers (mpm_solver_diff.py:977-991, 1022-1036,
-// 1098-1142, 1198-1212, 1332-1348, 1391-1410). Returns true when v changed.
+// 1098-1142, 1146-1171, 1198-1212, 1332-1348, 1391-1410). Returns true when v
+// changed.
 __device__ __forceinline__ bool apply_modifiers(const EmpmStep& st, int mask_index, V3 x, float mass, V3& v) {
     bool changed = false;
     const float dt = st.dt;
@@ -79,6 +80,9 @@ __device__ __forceinline__ bool apply_modifiers(const EmpmStep& st, int mask_ind
                 break;
             case EMPM_MOD_SET_VELOCITY:
                 if (mk == 1) { v = vec; changed = true; }
+                break;
+            case EMPM_MOD_SET_VELOCITY_LAYERED:
+                if (mk >= (int)md.scale[0]) { v = vec; changed = true; }
                 break;
             case EMPM_MOD_ROTATION:
                 if (mk == 1) {

@@ -251,6 +251,12 @@ class MPMWARPDiff(object):
             m.kind = p._kind
             m.gate = N.GATE_APPLY if self._window(t32, p) else N.GATE_OFF
             m.mask = p.mask.data_ptr() if p.mask is not None else None
+            if p._kind == N.MOD_SET_VELOCITY_LAYERED:
+                layer = self._outermost_layer(t32, p)
+                m.gate = N.GATE_APPLY if layer >= 0 else N.GATE_OFF
+                m.vec = N.F3(*_vec3(p.velocity))
+                m.scale = (N.ctypes.c_float * 2)(float(layer + 1), 0.0)
+                continue
             if p._kind in (N.MOD_IMPULSE, N.MOD_IMPULSE_MASK):
                 m.vec = N.F3(*_vec3(p.force))
             elif p._kind == N.MOD_SET_VELOCITY:
@@ -544,28 +550,51 @@ class MPMWARPDiff(object):
 
     def release_particles_sequentially(self, normal, start_position, end_position, num_layers, start_time, end_time,
                                        mpm_state=None):
-        """Layered release (mpm_solver_diff.py:1146-1171). The reference calls
-        enforce_particle_velocity_translation without a state (a TypeError
-        there); here the state must be passed as mpm_state."""
+        """Layered release (mpm_solver_diff.py:1146-1171): 50 nested boxes along
+        the axis of `normal` (num_layers is overridden by 50, as there), box i of
+        half length |start - end| / 50 * (50 - i) about end_position, each
+        holding its particles at zero velocity from start_time until
+        end_time / 50 * (i + 1). The reference registers one translation
+        modifier per box (and calls it without a state, a TypeError there);
+        here mpm_state must be passed. The 50 boxes are nested and all set
+        v = 0, so at any time the held particles are those of the outermost
+        box still active: they are registered as one modifier whose mask
+        counts the boxes holding each particle."""
         if mpm_state is None:
             raise TypeError("release_particles_sequentially needs mpm_state")
         num_layers = 50
-        point = [0, 0, 0]
-        size = [0, 0, 0]
-        axis = -1
-        for i in range(3):
-            if normal[i] == 0:
-                point[i] = 1
-                size[i] = 1
-            else:
-                axis = i
-                point[i] = end_position
+        axis = next((i for i in range(3) if normal[i] != 0), -1)
+        point = [float(end_position) if i == axis else 1.0 for i in range(3)]
+        base = [0.0 if i == axis else 1.0 for i in range(3)]
         half_length_portion = abs(start_position - end_position) / num_layers
         end_time_portion = end_time / num_layers
+        counts = torch.zeros(self.n_particles, dtype=torch.int32, device=mpm_state.device)
         for i in range(num_layers):
-            size[axis] = half_length_portion * (num_layers - i)
-            self.enforce_particle_velocity_translation(mpm_state, point=point, size=size, velocity=[0, 0, 0],
-                                                       start_time=start_time, end_time=end_time_portion * (i + 1))
+            size = list(base)
+            if axis >= 0:
+                size[axis] = half_length_portion * (num_layers - i)
+            counts += self._box_mask(mpm_state, point, size)
+        p = ParticleVelocityModifier()
+        p.point, p.size = _vec3(point), _vec3(base)
+        p.velocity = (0.0, 0.0, 0.0)
+        p.start_time = start_time
+        p.end_time = end_time_portion * num_layers
+        p.layer_end_times = [end_time_portion * (i + 1) for i in range(num_layers)]
+        p.mask = counts.contiguous()
+        p._kind = N.MOD_SET_VELOCITY_LAYERED
+        self.particle_velocity_modifier_params.append(p)
+        self.particle_velocity_modifiers.append(N.MOD_SET_VELOCITY_LAYERED)
+
+    @staticmethod
+    def _outermost_layer(t32, p) -> int:
+        """Index of the outermost release box active at t32, or -1 (each box's
+        own window, evaluated as the reference evaluates one modifier's)."""
+        if not bool(t32 >= _f32(p.start_time)):
+            return -1
+        for i, end in enumerate(p.layer_end_times):
+            if bool(t32 < _f32(end)):
+                return i
+        return -1
 
     def enforce_particle_velocity_by_mask(self, mpm_state, selection_mask: torch.Tensor, velocity, start_time,
                                           end_time):

@@ -137,6 +137,9 @@ typedef struct {
 #define EMPM_MOD_SET_VELOCITY     3  /* enforce_particle_velocity_translation/_by_mask: v = velocity (mask==1) :993-1036,1173-1212 */
 #define EMPM_MOD_ROTATION         4  /* enforce_particle_velocity_rotation  :1041-1142 */
 #define EMPM_MOD_MOVER            5  /* set_particle_mover: v += velocity + w * axis x (x - center) :1291-1348 */
+#define EMPM_MOD_SET_VELOCITY_LAYERED 6  /* release_particles_sequentially :1146-1171: v = velocity where
+                                           mask >= (int)scale[0]; mask counts the nested release boxes that
+                                           hold the particle, scale[0] = 1 + the outermost box still held */
 
 typedef struct {
     int   kind;            /* EMPM_MOD_* */

@@ -1,0 +1,150 @@
+"""Accuracy at the benchmarked sizes, against the FP64 oracle.
+
+The fixtures (tests/golden/fullsize_*.npz, made by
+tests/golden/make_fullsize.py with the FP64 OpenMP build of the oracle) hold
+seeded particle subsets of the full workloads and finite differences of the
+differentiable rollout's loss. Bars: final positions within 1e-4 of the
+domain (unit cube) of the FP64 oracle; gradients within 1e-3 relative of
+central finite differences (h = 1e-3 relative). Each test prints its
+measured error.
+
+  * large single rollout: 500,000 plasticine particles, 128^3 grid, moving
+    cuboid collider, dt=1e-4 x 1000 substeps, through the graph rollout the
+    bench times, plus the error every 100 substeps;
+  * batched population: 32 members (3.17M particles, grids 48..128^3),
+    dt=2e-4 x 300, through the batched graph path with the autotuned launch
+    options;
+  * differentiable rollout: 200,000 particles, 96^3, dt=2e-4 x 400,
+    checkpoints every 20 substeps; dL/dE, dL/dnu, dL/dyield and the
+    derivative along a direction of the initial velocities.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from empm_b200 import workloads as W
+from empm_b200.adjoint import CheckpointedRollout, prepare_adjoint
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+POS_BAR = 1e-4
+GRAD_BAR = 1e-3
+
+
+def _fixture(name):
+    return np.load(os.path.join(GOLDEN, f"fullsize_{name}.npz"))
+
+
+def _dist(x_gpu: torch.Tensor, idx: np.ndarray, ref: np.ndarray) -> np.ndarray:
+    got = x_gpu[torch.as_tensor(idx, device=x_gpu.device)].double().cpu().numpy()
+    return np.linalg.norm(got - ref.astype(np.float64), axis=1)
+
+
+def _c2_product():
+    w = W.c2()
+    solver, md, st, other = W.build_product(w, device=DEV)
+    cb = W.cuboid_callback(w, solver)
+    table, t_end = solver.build_schedule(0.0, w.dt, w.T, cb)
+    return w, solver, md, st, other, table, t_end
+
+
+def test_c2_large_rollout_final_positions_vs_fp64_oracle():
+    f = _fixture("c2")
+    w, solver, md, st, other, table, t_end = _c2_product()
+    res = solver.rollout(md, st, other, w.dt, w.T, schedule=(table, t_end))
+    torch.cuda.synchronize()
+    d = _dist(res.particle_x, f["final_idx"], f["final_x"])
+    fp32 = f["fp32_vs_fp64"][-1]
+    print(f"c2 after {w.T} substeps, {len(d)} particles: max {d.max():.3e} mean {d.mean():.3e} "
+          f"p99 {np.percentile(d, 99):.3e} (FP32 oracle vs FP64 over all particles: max {fp32[0]:.3e} "
+          f"mean {fp32[1]:.3e})")
+    assert solver.read_status() & 1 == 0
+    assert d.max() <= POS_BAR
+
+
+def test_c2_error_growth_every_100_substeps():
+    f = _fixture("c2")
+    w, solver, md, st, other, table, t_end = _c2_product()
+    marks = [int(m) for m in f["marks"]]
+    step = ctypes.sizeof(type(table[0]))
+    cur, prev = st, other
+    s0, t = 0, 0.0
+    worst = []
+    for k, s1 in enumerate(marks):
+        L = s1 - s0
+        seg = (type(table[0]) * L).from_buffer(table, s0 * step)
+        t1 = t + L * w.dt
+        res = solver.rollout(md, cur, prev, w.dt, L, schedule=(seg, t1))
+        if res is not cur:
+            cur, prev = prev, cur
+        d = _dist(cur.particle_x, f["curve_idx"], f["curve_x"][k])
+        fp32 = f["fp32_vs_fp64"][k]
+        worst.append(d.max())
+        print(f"c2 substep {s1}: max {d.max():.3e} mean {d.mean():.3e} "
+              f"(FP32 oracle vs FP64, all particles: max {fp32[0]:.3e} mean {fp32[1]:.3e})")
+        s0, t = s1, t1
+    assert max(worst) <= POS_BAR
+
+
+def test_c4_population_vs_fp64_oracle():
+    from empm_b200 import autotune as A
+    from empm_b200.batch import BatchedMPM
+
+    f = _fixture("c4")
+    specs, dt, T = W.c4()
+    batch = BatchedMPM(specs, device=DEV)
+    tuned = A.tune_batch(batch, dt, substeps=50)
+    batch.rollout(dt, T, block=50)
+    torch.cuda.synchronize()
+    assert batch.read_status() & 1 == 0
+    offs = f["offsets"]
+    worst = 0.0
+    for i, s in enumerate(specs):
+        idx = f["idx"][offs[i]:offs[i + 1]]
+        d = _dist(batch.positions(i), idx, f["x"][offs[i]:offs[i + 1]])
+        worst = max(worst, float(d.max()))
+        print(f"c4 member {i:2d} (n={s.n:6d}, G={s.n_grid:3d}): max {d.max():.3e} mean {d.mean():.3e}")
+    print(f"c4 worst member max {worst:.3e} with options {tuned['options']}")
+    assert worst <= POS_BAR
+
+
+def test_c3_gradients_vs_central_differences():
+    f = _fixture("c3")
+    names = [str(s) for s in f["names"]]
+    fd = dict(zip(names, f["fd"]))
+    w = W.c3()
+    tw = W.c3(guess=False)
+    solver, md, st, other = W.build_product(tw, device=DEV)
+    x_target = solver.rollout(md, st, other, tw.dt, tw.T).particle_x.clone()
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=DEV)  # noqa: E731
+    st._x4.copy_(t(np.concatenate([w.x, (w.vol * w.rho)[:, None]], 1).astype(np.float32)))
+    st._v4.copy_(t(np.concatenate([w.v, np.zeros((w.n, 1), np.float32)], 1)))
+    st._C.zero_()
+    st.particle_F_trial = torch.eye(3, device=DEV).expand(w.n, 3, 3)
+    md.E.copy_(t(w.E))
+    md.nu.copy_(t(w.nu))
+    md.finalize_mu_lam(w.n)
+    md.yield_stress.copy_(t(w.ys))
+    solver.time = 0.0
+    tape = CheckpointedRollout(solver, md, st, w.dt, w.T, checkpoint_every=20)
+    final = tape.forward()
+    diff = final.particle_x - x_target
+    loss = float((diff * diff).sum(1).mean())
+    res = tape.backward(g_x=2.0 * diff / w.n)
+    g_E, g_nu, _ = prepare_adjoint(md.E, md.nu, res["mu"], res["lam"])
+    direction = t((np.random.default_rng(int(f["dir_seed"])).standard_normal((w.n, 3)) * 0.05).astype(np.float32))
+    got = {"E": float(g_E.double().sum()), "nu": float(g_nu.double().sum()),
+           "yield_stress": float(res["yield_stress"].double().sum()),
+           "v0_dir": float((res["v"].double() * direction.double()).sum())}
+    print(f"c3 loss {loss:.6e} (FP64 oracle {float(f['loss']):.6e}); stored tape: {tape.stored}")
+    worst = 0.0
+    for k in names:
+        rel = abs(got[k] - fd[k]) / abs(fd[k])
+        worst = max(worst, rel)
+        print(f"c3 dL/d{k}: adjoint {got[k]:.6e} central difference {fd[k]:.6e} relative error {rel:.2e}")
+    assert abs(loss - float(f["loss"])) <= 1e-3 * float(f["loss"])
+    assert worst <= GRAD_BAR
