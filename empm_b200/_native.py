@@ -22,6 +22,7 @@ COLL_SURFACE, COLL_GEOMETRY, COLL_GRID_VELOCITY, COLL_CUBOID_VELOCITY, COLL_BOUN
 SHAPE_CUBE, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_HALFSPACE = 1, 2, 3, 4
 GATE_OFF, GATE_APPLY, GATE_ZERO_ALL = 0, 1, 2
 OPT_SORT_EVERY, OPT_P2G_MODE, OPT_G2P_TILE, OPT_TILE_CAP, OPT_SEG_CAP, OPT_ADJ_STORE = 1, 2, 3, 4, 5, 6
+OPT_FUSE = 7
 MOD_IMPULSE, MOD_IMPULSE_MASK, MOD_SET_VELOCITY, MOD_ROTATION, MOD_MOVER = 1, 2, 3, 4, 5
 MOD_SET_VELOCITY_LAYERED = 6
 
@@ -108,6 +109,8 @@ def lib():
         "empm_unpack_particles": ([ctypes.POINTER(EmpmParticles), P, P, P, P, I, P], I),
         "empm_substep": ([P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmParticles),
                           ctypes.POINTER(EmpmMaterial), ctypes.POINTER(EmpmStep), P], I),
+        "empm_substep_inplace": ([P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmMaterial),
+                                  ctypes.POINTER(EmpmStep), P, P], I),
         "empm_rollout": ([P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmParticles),
                           ctypes.POINTER(EmpmMaterial), P, I, I, I, P], I),
         "empm_rollout_ex": ([P, ctypes.POINTER(EmpmParticles), ctypes.POINTER(EmpmParticles),
@@ -149,6 +152,7 @@ def lib():
         "empm_ctx_set_option": ([P, I, I], I),
         "empm_ctx_kernel_times": ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
         "empm_ctx_adjoint_kernel_times": ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
+        "empm_ctx_fused_kernel_times": ([P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(I)], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -156,6 +160,20 @@ def lib():
         f.restype = res
     _lib = L
     return L
+
+
+def kernel_times(L, ctx) -> dict:
+    """Per-kernel CUDA-event times of a context's stream-path launches:
+    {kernel: (total_ms, launches)} for stress_p2g, grid_update, g2p and the
+    fused g2p2g."""
+    ms = (ctypes.c_float * 3)()
+    cnt = (ctypes.c_int * 3)()
+    check(L.empm_ctx_kernel_times(ctx, ms, cnt), ctx)
+    out = {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("stress_p2g", "grid_update", "g2p"))}
+    fms, fcnt = ctypes.c_float(), ctypes.c_int()
+    check(L.empm_ctx_fused_kernel_times(ctx, ctypes.byref(fms), ctypes.byref(fcnt)), ctx)
+    out["g2p2g"] = (float(fms.value), int(fcnt.value))
+    return out
 
 
 def last_error(ctx=None) -> str:

@@ -125,6 +125,7 @@ class BatchedMPM:
         self.g2p_tile = False
         self.tile_cap = 1024
         self.seg_cap = 4           # warp-aggregated P2G: longest same-cell run per reduction
+        self.fuse = True           # fused G2P + stress + P2G between cell sorts
         self._opts = {}
         # per-instance collider lists / schedule builders
         self.solvers = []
@@ -238,7 +239,7 @@ class BatchedMPM:
     def _apply_options(self):
         opts = {N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_MODE: int(self.p2g_mode),
                 N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap),
-                N.OPT_SEG_CAP: int(self.seg_cap)}
+                N.OPT_SEG_CAP: int(self.seg_cap), N.OPT_FUSE: int(bool(self.fuse))}
         for k, v in opts.items():
             if self._opts.get(k) != v:
                 N.check(self.L.empm_ctx_set_option(self.ptr, k, v), self.ptr)
@@ -280,10 +281,8 @@ class BatchedMPM:
         N.check(self.L.empm_ctx_timing(self.ptr, int(enable), int(max_launches)), self.ptr)
 
     def kernel_times(self):
-        ms = (ctypes.c_float * 3)()
-        cnt = (ctypes.c_int * 3)()
-        N.check(self.L.empm_ctx_kernel_times(self.ptr, ms, cnt), self.ptr)
-        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("stress_p2g", "grid_update", "g2p"))}
+        """{kernel: (total_ms, launches)} for [stress_p2g, grid_update, g2p, g2p2g]."""
+        return N.kernel_times(self.L, self.ptr)
 
     def __del__(self):
         try:

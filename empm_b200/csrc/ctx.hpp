@@ -18,6 +18,7 @@ struct GraphKey {
     int           g2p_tile;
     int           tile_cap;
     int           seg_cap;
+    int           fuse;                       // fused G2P + P2G runs in use (option and hold pattern)
     unsigned long long params_version;
     int           flags;                      // EMPM_ROLLOUT_RESUME / EMPM_ROLLOUT_KEEP
     int           start_pc, start_mc, start_since;   // sorted state a resumed sequence starts in
@@ -125,14 +126,17 @@ struct EmpmCtx {
     int          tile_cap = 1024;          // nodes per shared-memory tile (16 B each)
     int          seg_cap = 4;              // warp-aggregated P2G: longest same-cell run per head
     int          adj_store = 1;            // adjoint segments store substep grids instead of recomputing
+    int          fuse = 1;                 // sorted rollouts fuse the G2P of one substep with the P2G of the next
+    bool         fuse_ok = true;           // the uploaded step tables allow it (holds never released)
     SortedBuffers sb;
     AdjointBuffers adj;
     // per-kernel event timing (stream path only)
     bool         timing = false;
     int          timing_capacity = 0;
-    // timed kernels: 0 stress+P2G, 1 grid update, 2 G2P, 3 adjoint G2P, 4 adjoint grid, 5 adjoint P2G
-    static constexpr int kTimedKernels = 6;
-    int          timing_count[kTimedKernels] = {0, 0, 0, 0, 0, 0};
+    // timed kernels: 0 stress+P2G, 1 grid update, 2 G2P, 3 adjoint G2P, 4 adjoint grid, 5 adjoint P2G,
+    // 6 fused G2P + stress + P2G
+    static constexpr int kTimedKernels = 7;
+    int          timing_count[kTimedKernels] = {0, 0, 0, 0, 0, 0, 0};
     std::vector<cudaEvent_t> timing_events;   // [kTimedKernels][capacity][2]
     char         err[512] = {0};
 };

@@ -567,17 +567,14 @@ __global__ void k_unsort(const UnsortArgs a) {
 // Same-cell runs are split every seg_cap = 2^ROUNDS lanes, so a segment sums
 // in at most ROUNDS shuffle rounds; the rounds a run cap never needs are not
 // compiled in (smaller code for the instruction cache).
-template <int ROUNDS, int MAT = -1>
-__global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
-                                                     float4* grid, unsigned char* flags) {
+// The warp-aggregated scatter of one prepared particle per lane (all 32
+// lanes of the warp take part; lanes with valid == false contribute zeros and
+// never write). c: the lane's instance constants for this substep.
+template <int ROUNDS>
+__device__ __forceinline__ void warpagg_scatter(bool valid, int inst, const P2GParticle& q, const StepConsts& c,
+                                                float4* grid, unsigned char* flags) {
     constexpr int seg_cap = 1 << ROUNDS;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const int inst = p < L.n_total ? find_instance_particle(L, p) : 0;
-    const StepConsts c = consts_of(L, inst);
-    P2GParticle q;
-    bool valid = false;
-    if (p < L.n_total) valid = prepare_particle<MAT>(P, M, Fe, c, p, q);
     // a segment is a run of lanes with the same validity, instance and base
     // cell; lanes without a particle contribute zeros and never write
     const int b0 = valid ? q.st.b[0] : lane, b1 = valid ? q.st.b[1] : 0, b2 = valid ? q.st.b[2] : 0;
@@ -633,6 +630,114 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
             red_add_v4(grid + gaddr(c, q.st.b[0] + i, q.st.b[1] + j, q.st.b[2] + k), v);
     });
     if (head && valid) mark_stencil_blocks(flags, q.st, c);
+}
+
+// Same-cell runs are split every seg_cap = 2^ROUNDS lanes, so a segment sums
+// in at most ROUNDS shuffle rounds; the rounds a run cap never needs are not
+// compiled in (smaller code for the instruction cache).
+template <int ROUNDS, int MAT = -1>
+__global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(ParticleArrays P, MaterialArrays M, F9Planes Fe, Launch L,
+                                                     float4* grid, unsigned char* flags) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int inst = p < L.n_total ? find_instance_particle(L, p) : 0;
+    const StepConsts c = consts_of(L, inst);
+    P2GParticle q;
+    bool valid = false;
+    if (p < L.n_total) valid = prepare_particle<MAT>(P, M, Fe, c, p, q);
+    warpagg_scatter<ROUNDS>(valid, inst, q, c, grid, flags);
+}
+
+// -------------------------------------------------------------------------
+// sorted path, fused: the G2P of substep s-1 and the stress + P2G of substep s
+// in one pass over the particles
+// -------------------------------------------------------------------------
+// Between two such kernels a particle's persistent state is its position and
+// its elastic F (plus the material scalars); its velocity, affine matrix and
+// trial F are consumed by the P2G in the same thread, so they are not written
+// back. Position and elastic F are updated in place: a thread reads and writes
+// only its own particle. The grid velocities of substep s-1 (vel) are read,
+// the accumulator of substep s (mom, cleared by the grid update of s-1) is
+// written: the two are separate buffers. A run of fused substeps starts with
+// the separate stress + P2G and ends with the separate G2P, which writes the
+// full state. Held instances (step-table hold) must stay held once held within
+// the run: when a particle's instance becomes held at substep s, its state
+// after the G2P of s-1 is written in full, then left alone.
+template <int ROUNDS, int MAT = -1>
+__global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_g2p2g(ParticleArrays P, MaterialArrays M, F9Planes Fe,
+                                                                  Launch L, int g2p_table, const float4* vel,
+                                                                  float4* mom, unsigned char* flags) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int inst = p < L.n_total ? find_instance_particle(L, p) : 0;
+    const StepConsts c = consts_of(L, inst);   // substep s: stress + P2G
+    P2GParticle q;
+    bool valid = false;
+    if (p < L.n_total && !(M.sel && __ldg(M.sel + p) != 0)) {
+        const EmpmStep& sg = L.steps[(size_t)g2p_table * L.n_inst + inst];   // substep s-1: G2P
+        if (!sg.hold) {
+            const float dt = sg.dt;
+            const float4 xm = __ldg(P.x + p);
+            const V3 x = v3(xm.x, xm.y, xm.z);
+            const Stencil st = make_stencil(x, c.inv_dx);
+            const bool in_grid = stencil_in_grid(st, c.G);
+            GlobalFetch fetch{vel, &c};
+            const G2POut o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
+            const float dx = 1.f / c.inv_dx;   // as g2p_particle computes it
+            const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
+            V3 nx = x + dt * o.v;
+            nx = v3(fminf(fmaxf(nx.x, lo), hi), fminf(fmaxf(nx.y, lo), hi), fminf(fmaxf(nx.z, lo), hi));
+            const M3 Fn = (m3_identity() + dt * o.gradv) * f9_load(Fe, p);
+            P.x[p] = make_float4(nx.x, nx.y, nx.z, xm.w);
+            unsigned bad = 0;
+            if (!finite3(o.v) || !finite3(nx) || !isfinite(Fn.m[0] + Fn.m[4] + Fn.m[8])) bad |= EMPM_STATUS_NAN;
+            if (fmaxf(fmaxf(fabsf(o.v.x), fabsf(o.v.y)), fabsf(o.v.z)) * dt > dx) bad |= EMPM_STATUS_CFL;
+            if (!in_grid) bad |= EMPM_STATUS_OUT_OF_BAND;
+            if (bad) atomicOr(c.status, bad);
+            const EmpmStep& sp = *c.step;
+            if (sp.hold) {
+                // held from substep s on: keep the state after this G2P
+                P.v[p] = make_float4(o.v.x, o.v.y, o.v.z, 0.f);
+                f9_store(P.C, p, o.C);
+                f9_store(P.F, p, Fn);
+            } else {
+                V3 v = o.v;
+                if (sp.n_modifiers > 0) {
+                    const int mi = M.pid ? __ldg(M.pid + p) : p;
+                    apply_modifiers(sp, mi, nx, xm.w, v);
+                }
+                float mu = __ldg(M.mu + p), lam = __ldg(M.lam + p), ys = __ldg(M.ys + p);
+                const ConstitutiveOut co = constitutive<MAT>(Fn, mu, lam, ys, sp.dt, c.ms);
+                f9_store(Fe, p, co.F);
+                if (co.mat_changed) { M.mu[p] = mu; M.lam[p] = lam; M.ys[p] = ys; }
+                q.st = make_stencil(nx, c.inv_dx);
+                q.wm_scale = xm.w;
+                q.v = v;
+                q.Cd = damp_affine(o.C, c.rpic);
+                q.Sv = (-__ldg(M.vol + p)) * co.tau;
+                valid = true;
+            }
+        }
+    }
+    warpagg_scatter<ROUNDS>(valid, inst, q, c, mom, flags);
+}
+
+static inline void launch_g2p2g(int grid_ctas, int threads, cudaStream_t s, const ParticleArrays& P,
+                                const MaterialArrays& M, const F9Planes& Fe, const Launch& L, int g2p_table,
+                                const float4* vel, float4* mom, unsigned char* flags, int seg_cap,
+                                int material = -1) {
+#define EMPM_G2P2G(R, MAT) k_g2p2g<R, MAT><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, g2p_table, vel, mom, flags)
+    if (material == 5 && seg_cap == 4) { EMPM_G2P2G(2, 5); return; }
+    if (material == 5 && seg_cap == 8) { EMPM_G2P2G(3, 5); return; }
+    if (material == 0 && seg_cap == 4) { EMPM_G2P2G(2, 0); return; }
+    if (material == 0 && seg_cap == 8) { EMPM_G2P2G(3, 0); return; }
+    switch (seg_cap) {
+        case 1: EMPM_G2P2G(0, -1); break;
+        case 2: EMPM_G2P2G(1, -1); break;
+        case 4: EMPM_G2P2G(2, -1); break;
+        case 8: EMPM_G2P2G(3, -1); break;
+        case 16: EMPM_G2P2G(4, -1); break;
+        default: EMPM_G2P2G(5, -1); break;
+    }
+#undef EMPM_G2P2G
 }
 
 // k_p2g_warpagg for a run cap seg_cap (a power of two in 1..32). material:

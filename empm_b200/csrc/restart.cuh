@@ -95,4 +95,44 @@ __global__ void __launch_bounds__(128) k_restart_g2p(ParticleArrays P, const flo
     P.x[p] = make_float4(__ldg(target + 3 * p), __ldg(target + 3 * p + 1), __ldg(target + 3 * p + 2), xm.w);
 }
 
+// -------------------------------------------------------------------------
+// in-place G2P of MPMWARPDiff.p2g2p (mpm_solver_diff.py:293-429)
+// -------------------------------------------------------------------------
+// g2p (mpm_utils.py:441-499) followed by clip_particle_x (:582-599), written
+// back into the particle's own arrays: v, C, F_trial = (I + dt grad v) F_e,
+// x += dt v (the atomic_add of :486) clamped to [2 dx, grid_lim - 2 dx], and,
+// when cov is given (update_cov_with_F), cov += dt (G cov + cov G^T) with
+// G = grad v. Unsimulated particles (selection != 0) are left as they are.
+// Each thread reads and writes only its own particle, so in place is safe.
+__global__ void __launch_bounds__(128) k_g2p_inplace(ParticleArrays P, F9Planes Fe, MaterialArrays M, Launch L,
+                                                     const float4* vel, float* cov) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= L.n_total) return;
+    if (M.sel && __ldg(M.sel + p) != 0) return;
+    const StepConsts c = consts_of(L, find_instance_particle(L, p));
+    if (c.step->hold) return;
+    const float dt = c.step->dt;
+    const float4 xm = P.x[p];
+    const V3 x = v3(xm.x, xm.y, xm.z);
+    const Stencil st = make_stencil(x, c.inv_dx);
+    const bool in_grid = stencil_in_grid(st, c.G);
+    const GlobalFetch fetch{vel, &c};
+    const G2POut o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
+    const float dx = 1.f / c.inv_dx;
+    const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
+    V3 nx = x + dt * o.v;
+    nx = v3(fminf(fmaxf(nx.x, lo), hi), fminf(fmaxf(nx.y, lo), hi), fminf(fmaxf(nx.z, lo), hi));
+    const M3 Fn = (m3_identity() + dt * o.gradv) * f9_load(Fe, p);
+    P.x[p] = make_float4(nx.x, nx.y, nx.z, xm.w);
+    P.v[p] = make_float4(o.v.x, o.v.y, o.v.z, 0.f);
+    f9_store(P.C, p, o.C);
+    f9_store(P.F, p, Fn);
+    if (cov) update_cov(cov, p, o.gradv, dt);
+    unsigned flags = 0;
+    if (!finite3(o.v) || !finite3(nx) || !isfinite(Fn.m[0] + Fn.m[4] + Fn.m[8])) flags |= EMPM_STATUS_NAN;
+    if (fmaxf(fmaxf(fabsf(o.v.x), fabsf(o.v.y)), fabsf(o.v.z)) * dt > dx) flags |= EMPM_STATUS_CFL;
+    if (!in_grid) flags |= EMPM_STATUS_OUT_OF_BAND;
+    if (flags) atomicOr(c.status, flags);
+}
+
 }  // namespace empm

@@ -5,6 +5,7 @@
 #include <string.h>
 #include <stdarg.h>
 #include <mutex>
+#include <algorithm>
 #include "../../include/empm_b200.h"
 #include <cub/device/device_scan.cuh>
 #include "kernels.cuh"
@@ -304,6 +305,7 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
             ctx->tile_cap = value;
             break;
         case EMPM_OPT_ADJ_STORE: ctx->adj_store = value != 0; break;
+        case EMPM_OPT_FUSE: ctx->fuse = value != 0; break;
         case EMPM_OPT_SEG_CAP:
             if (value < 1 || value > 32 || (value & (value - 1)) != 0)
                 return empm_set_error(ctx, EMPM_ERR_INVALID, "seg_cap %d not a power of two in 1..32", value);
@@ -754,7 +756,7 @@ static int launch_sort(EmpmCtx* ctx, SortedState& ss, const ParticleArrays* user
     return EMPM_OK;
 }
 
-static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaStream_t stream) {
+static TiledArgs sorted_args(EmpmCtx* ctx, const SortedState& ss, int table) {
     SortedBuffers& sb = ctx->sb;
     const int n = ctx->n_particles;
     TiledArgs t;
@@ -767,8 +769,15 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaS
     t.grid = ctx->grid_mom;
     t.flags = ctx->flags;
     t.out = particle_arrays(sb.part[1 - ss.pc], n);
+    t.tile_cap = 0;
+    return t;
+}
+
+// stress + P2G of one substep on the sorted state
+static int launch_p2g_sorted(EmpmCtx* ctx, const SortedState& ss, int table, cudaStream_t stream) {
+    const int n = ctx->n_particles;
+    TiledArgs t = sorted_args(ctx, ss, table);
     t.tile_cap = ctx->p2g_mode == 1 ? ctx->tile_cap : 0;
-    const int persistent = ctx->sm_count * 2;
     const size_t smem = sizeof(float4) * (size_t)ctx->tile_cap;
     timing_mark(ctx, 0, 0, stream);
     if (ctx->p2g_mode == 2) {
@@ -776,17 +785,23 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaS
         launch_p2g_warpagg(blocks_for(n, tp), tp, stream, t.P, t.M, t.Fe, t.L, ctx->grid_mom, ctx->flags,
                            ctx->seg_cap, uniform_material(ctx));
     } else {
-        k_p2g_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+        k_p2g_tiled<<<ctx->sm_count * 2, TILE_THREADS, smem, stream>>>(t);
     }
     timing_mark(ctx, 0, 1, stream);
     CK(cudaGetLastError(), "k_p2g_sorted");
-    int rc = launch_grid_update(ctx, table, stream);
-    if (rc) return rc;
+    return EMPM_OK;
+}
+
+// G2P of one substep: the sorted state -> the other particle buffer
+static int launch_g2p_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaStream_t stream) {
+    const int n = ctx->n_particles;
+    TiledArgs t = sorted_args(ctx, ss, table);
     t.grid = ctx->grid_vel;
     t.tile_cap = ctx->g2p_tile ? ctx->tile_cap : 0;
+    const size_t smem = sizeof(float4) * (size_t)ctx->tile_cap;
     timing_mark(ctx, 2, 0, stream);
     if (ctx->g2p_tile) {
-        k_g2p_tiled<<<persistent, TILE_THREADS, smem, stream>>>(t);
+        k_g2p_tiled<<<ctx->sm_count * 2, TILE_THREADS, smem, stream>>>(t);
     } else {
         k_g2p_direct<<<blocks_for(n, 128), 128, 0, stream>>>(t.P, t.Fe, t.M, t.out, t.L, ctx->grid_vel);
     }
@@ -794,6 +809,52 @@ static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaS
     CK(cudaGetLastError(), "k_g2p_sorted");
     ss.pc = 1 - ss.pc;
     return EMPM_OK;
+}
+
+static int launch_substep_sorted(EmpmCtx* ctx, SortedState& ss, int table, cudaStream_t stream) {
+    int rc = launch_p2g_sorted(ctx, ss, table, stream);
+    if (!rc) rc = launch_grid_update(ctx, table, stream);
+    if (!rc) rc = launch_g2p_sorted(ctx, ss, table, stream);
+    return rc;
+}
+
+// Fused G2P of substep g2p_table and stress + P2G of substep `table`, in
+// place on the sorted state's positions and the elastic F buffer.
+static int launch_g2p2g_sorted(EmpmCtx* ctx, const SortedState& ss, int g2p_table, int table, cudaStream_t stream) {
+    const int n = ctx->n_particles;
+    const TiledArgs t = sorted_args(ctx, ss, table);
+    const int tp = particle_threads(ctx, n, 256);
+    timing_mark(ctx, 6, 0, stream);
+    launch_g2p2g(blocks_for(n, tp), tp, stream, t.P, t.M, t.Fe, t.L, g2p_table, ctx->grid_vel, ctx->grid_mom,
+                 ctx->flags, ctx->seg_cap, uniform_material(ctx));
+    timing_mark(ctx, 6, 1, stream);
+    CK(cudaGetLastError(), "k_g2p2g");
+    return EMPM_OK;
+}
+
+static bool use_fused(const EmpmCtx* ctx) {
+    return ctx->fuse && ctx->fuse_ok && ctx->p2g_mode == 2 && !ctx->g2p_tile;
+}
+
+// Substeps [first, first + count) of a rollout on the sorted state, with no
+// cell sort among them: separately, or as one run of fused kernels (the
+// run's first stress + P2G and last G2P separate).
+static int launch_sorted_run(EmpmCtx* ctx, SortedState& ss, int first, int count, int n_tables,
+                             cudaStream_t stream) {
+    auto table = [&](int i) { return n_tables == 1 ? 0 : i; };
+    int rc = EMPM_OK;
+    if (count < 2 || !use_fused(ctx)) {
+        for (int i = first; i < first + count && rc == EMPM_OK; ++i) rc = launch_substep_sorted(ctx, ss, table(i), stream);
+        return rc;
+    }
+    rc = launch_p2g_sorted(ctx, ss, table(first), stream);
+    if (!rc) rc = launch_grid_update(ctx, table(first), stream);
+    for (int i = first + 1; i < first + count && rc == EMPM_OK; ++i) {
+        rc = launch_g2p2g_sorted(ctx, ss, table(i - 1), table(i), stream);
+        if (!rc) rc = launch_grid_update(ctx, table(i), stream);
+    }
+    if (!rc) rc = launch_g2p_sorted(ctx, ss, table(first + count - 1), stream);
+    return rc;
 }
 
 static bool use_sorted(EmpmCtx* ctx) {
@@ -824,13 +885,16 @@ static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, cons
         rc = launch_sort(ctx, ss, &ua, mat, stream);
         since = 0;
     }
-    for (int i = 0; i < n_steps && rc == EMPM_OK; ++i) {
+    for (int i = 0; i < n_steps && rc == EMPM_OK;) {
         if (since >= ctx->sort_every) {
             rc = launch_sort(ctx, ss, nullptr, nullptr, stream);
             since = 0;
         }
-        if (rc == EMPM_OK) rc = launch_substep_sorted(ctx, ss, n_tables == 1 ? 0 : i, stream);
-        ++since;
+        // the substeps up to the next cell sort
+        const int count = std::min(n_steps - i, ctx->sort_every - since);
+        if (rc == EMPM_OK) rc = launch_sorted_run(ctx, ss, i, count, n_tables, stream);
+        since += count;
+        i += count;
     }
     if (rc || (flags & EMPM_ROLLOUT_KEEP)) return rc;
     UnsortArgs u;
@@ -880,6 +944,40 @@ extern "C" int empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles
     return launch_substep_direct(ctx, in, out, mat, 0, s);
 }
 
+extern "C" int empm_substep_inplace(EmpmCtx* ctx, EmpmParticles* state, const EmpmMaterial* mat,
+                                    const EmpmStep* step, float* cov, void* stream) {
+    if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
+    int rc = check_particles(ctx, state, "state");
+    if (!rc) rc = check_material(ctx, mat);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = upload_steps(ctx, step, 1, s);
+    if (rc) return rc;
+    const int n = ctx->n_particles;
+    const Launch L = make_launch(ctx, 0);
+    const ParticleArrays P = particle_arrays(state, n);
+    MaterialArrays M;
+    M.vol = mat->vol;
+    M.mu = mat->mu;
+    M.lam = mat->lam;
+    M.ys = mat->yield_stress;
+    M.sel = mat->selection;
+    M.pid = nullptr;
+    const F9Planes Fe = f9_planes(mat->F_elastic, n);
+    if (n > 0) {
+        const int tp = particle_threads(ctx, n, 128);
+        k_p2g_direct<<<blocks_for(n, tp), tp, 0, s>>>(P, M, Fe, L, ctx->grid_mom, ctx->flags);
+        CK(cudaGetLastError(), "k_p2g_direct (in place)");
+    }
+    rc = launch_grid_update(ctx, 0, s);
+    if (rc) return rc;
+    if (n > 0) {
+        k_g2p_inplace<<<blocks_for(n, 128), 128, 0, s>>>(P, Fe, M, L, ctx->grid_vel, cov);
+        CK(cudaGetLastError(), "k_g2p_inplace");
+    }
+    return EMPM_OK;
+}
+
 extern "C" int empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const EmpmMaterial* mat,
                                const EmpmStep* steps, int n_tables, int n_steps, int flags, void* stream) {
     if (!ctx) return empm_set_error(nullptr, EMPM_ERR_INVALID, "ctx is NULL");
@@ -898,6 +996,15 @@ extern "C" int empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b,
     if (!sorted) flags &= EMPM_ROLLOUT_GRAPH;   // the direct path always writes the caller's buffers
     rc = upload_steps(ctx, steps, n_tables, s);
     if (rc) return rc;
+    // fused runs keep no velocity between substeps: an instance released from
+    // a hold (hold 1 in one table, 0 in a later one) needs the separate kernels
+    ctx->fuse_ok = true;
+    for (int inst = 0; inst < ctx->n_inst && ctx->fuse_ok; ++inst)
+        for (int t = 1; t < n_tables; ++t)
+            if (steps[(size_t)(t - 1) * ctx->n_inst + inst].hold && !steps[(size_t)t * ctx->n_inst + inst].hold) {
+                ctx->fuse_ok = false;
+                break;
+            }
     if (sorted) {
         rc = ensure_sorted_buffers(ctx);
         if (rc) return rc;
@@ -932,6 +1039,7 @@ extern "C" int empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b,
         key.g2p_tile = ctx->g2p_tile;
         key.tile_cap = ctx->tile_cap;
         key.seg_cap = ctx->seg_cap;
+        key.fuse = use_fused(ctx) ? 1 : 0;
         key.params_version = ctx->params_version;
         key.flags = flags & (EMPM_ROLLOUT_RESUME | EMPM_ROLLOUT_KEEP);
         if (flags & EMPM_ROLLOUT_RESUME) {
@@ -1089,6 +1197,22 @@ extern "C" int empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launch
 
 extern "C" int empm_ctx_adjoint_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3) {
     return kernel_times(ctx, 3, total_ms3, launches3);
+}
+
+extern "C" int empm_ctx_fused_kernel_times(EmpmCtx* ctx, float* total_ms, int* launches) {
+    if (!ctx || !total_ms || !launches) return empm_set_error(ctx, EMPM_ERR_INVALID, "bad arguments");
+    const int k = 6;
+    float total = 0.f;
+    for (int i = 0; i < ctx->timing_count[k]; ++i) {
+        const size_t base = ((size_t)k * ctx->timing_capacity + i) * 2;
+        CK(cudaEventSynchronize(ctx->timing_events[base + 1]), "cudaEventSynchronize");
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->timing_events[base], ctx->timing_events[base + 1]), "cudaEventElapsedTime");
+        total += ms;
+    }
+    *total_ms = total;
+    *launches = ctx->timing_count[k];
+    return EMPM_OK;
 }
 
 // ===========================================================================

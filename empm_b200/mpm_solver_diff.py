@@ -120,6 +120,7 @@ class MPMWARPDiff(object):
         self.tile_cap = 1024
         self.seg_cap = 4           # warp-aggregated P2G: longest same-cell run per reduction
         self.adj_store = True      # adjoint keeps each substep's grid and elastic F instead of recomputing
+        self.fuse = True           # rollouts fuse each G2P with the next substep's stress + P2G
 
     def initialize(self, n_particles, n_grid=100, grid_lim=1.0, device="cuda:0"):
         self.n_particles = n_particles
@@ -188,7 +189,8 @@ class MPMWARPDiff(object):
             c.set_params(params)
         c.set_options({N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_MODE: int(self.p2g_mode),
                        N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap),
-                       N.OPT_SEG_CAP: int(self.seg_cap), N.OPT_ADJ_STORE: int(bool(self.adj_store))})
+                       N.OPT_SEG_CAP: int(self.seg_cap), N.OPT_ADJ_STORE: int(bool(self.adj_store)),
+                       N.OPT_FUSE: int(bool(getattr(self, "fuse", True)))})
         return c
 
     @staticmethod
@@ -323,6 +325,24 @@ class MPMWARPDiff(object):
         self._modify(self.time, dt)
         self.time = self.time + dt
 
+    def p2g2p(self, mpm_model, mpm_state, step, dt, device="cuda:0"):
+        """One substep in place (mpm_solver_diff.py:293-429): the state's x, v,
+        C and F_trial are overwritten, unsimulated particles are left alone,
+        and with mpm_model.update_cov_with_F the covariances follow the
+        velocity gradient. `step` is unused, as in the reference."""
+        n = mpm_state.n_particles
+        ctx = self._context(mpm_model, n, mpm_state.device)
+        self._check_masks()
+        st = N.EmpmStep()
+        self._fill_step(st, self.time, dt)
+        mat = self._material(mpm_model, mpm_state)
+        cov = mpm_state.particle_cov.data_ptr() if bool(getattr(mpm_model, "update_cov_with_F", False)) else None
+        with torch.cuda.device(mpm_state.device):
+            N.check(ctx.L.empm_substep_inplace(ctx.ptr, mpm_state._particles(), mat, st, cov,
+                                               _stream_ptr(mpm_state.device)), ctx.ptr)
+        self._modify(self.time, dt)
+        self.time = self.time + dt
+
     def rollout(self, mpm_model, state_a, state_b, dt, n_steps, step_callback=None, schedule=None):
         """n_steps substeps ping-ponging between state_a and state_b on one
         launch sequence (CUDA graph when self.use_graph). Returns the state
@@ -362,11 +382,9 @@ class MPMWARPDiff(object):
         N.check(self._ctx.L.empm_ctx_timing(self._ctx.ptr, int(enable), int(max_launches)), self._ctx.ptr)
 
     def kernel_times(self):
-        """{kernel: (total_ms, launches)} for [stress_p2g, grid_update, g2p]."""
-        ms = (N.ctypes.c_float * 3)()
-        cnt = (N.ctypes.c_int * 3)()
-        N.check(self._ctx.L.empm_ctx_kernel_times(self._ctx.ptr, ms, cnt), self._ctx.ptr)
-        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("stress_p2g", "grid_update", "g2p"))}
+        """{kernel: (total_ms, launches)} for [stress_p2g, grid_update, g2p, g2p2g]
+        (g2p2g: the fused G2P + stress + P2G of fused rollouts)."""
+        return N.kernel_times(self._ctx.L, self._ctx.ptr)
 
     def adjoint_kernel_times(self):
         """{kernel: (total_ms, launches)} for the adjoint kernels [adj_g2p, adj_grid, adj_p2g]."""

@@ -26,6 +26,8 @@
  *                          add_damping_via_grid, collider closures, g2p_differentiable
  *                          in mpm_utils.py:286-665,722-734 and
  *                          mpm_solver_diff.py:473-528,612-672,756-801,835-866,878-935,1275-1286)
+ *   empm_substep_inplace <- MPMWARPDiff.p2g2p (mpm_solver_diff.py:293-429, in-place g2p and
+ *                          clip_particle_x, mpm_utils.py:441-499,582-599)
  *   empm_rollout        <- the substep loop of WarpMPMWrapper.advance_to
  *                          warp_mpm_wrapper.py:278-306 and interface.py:137-145
  *   empm_prepare        <- compute_mu_lam_from_E_nu (mpm_utils.py:277-283) and the
@@ -250,6 +252,18 @@ int  empm_unpack_particles(const EmpmParticles* src, float* x3, float* v3, float
 int  empm_substep(EmpmCtx* ctx, const EmpmParticles* in, EmpmParticles* out,
                   const EmpmMaterial* mat, const EmpmStep* step, void* stream);
 
+/* One MLS-MPM substep in place: MPMWARPDiff.p2g2p (mpm_solver_diff.py:293-429),
+ * the variant of the substep whose g2p (mpm_utils.py:441-499) writes v, C and
+ * F_trial back into the same state, moves x by atomic_add and then clamps it
+ * (clip_particle_x, :582-599). Unsimulated particles (selection != 0) are left
+ * unchanged, unlike empm_substep, where they come back cleared. The velocity
+ * modifiers write the state's v in place before P2G, as there. cov: NULL, or
+ * device float [n, 6] packed covariances updated with the velocity gradient
+ * G as cov += dt (G cov + cov G^T) (update_cov, :306-326, applied when
+ * update_cov_with_F is set). One schedule per instance, as for empm_substep. */
+int  empm_substep_inplace(EmpmCtx* ctx, EmpmParticles* state, const EmpmMaterial* mat, const EmpmStep* step,
+                          float* cov, void* stream);
+
 /* n_steps substeps, ping-ponging between a and b (the result is in a when
  * n_steps is even, else in b). steps is a host array of n_tables schedule
  * tables of n_instances entries each: n_tables == 1 reuses one table for
@@ -299,6 +313,11 @@ int  empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const Emp
                                     n_steps x (2 KiB per grid block + 36 B per particle) of device memory,
                                     recompute when that allocation fails); 0 = recompute P2G and the grid
                                     update in the reverse pass */
+#define EMPM_OPT_FUSE        7   /* sorted rollouts with warp-aggregated P2G and direct G2P: 1 = between two cell
+                                    sorts, the G2P of each substep and the stress + P2G of the next run as one
+                                    kernel that keeps only position and elastic F per particle between substeps
+                                    (default); 0 = separate kernels. Step tables that release a held instance
+                                    (hold 1 then 0) always run separately. */
 
 int  empm_ctx_set_option(EmpmCtx* ctx, int option, int value);
 
@@ -555,6 +574,10 @@ int  empm_ctx_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3);
  * G2P, adjoint grid update, adjoint P2G (the recomputed forward P2G and grid
  * update of the adjoint are counted with the forward kernels). */
 int  empm_ctx_adjoint_kernel_times(EmpmCtx* ctx, float* total_ms3, int* launches3);
+/* The same for the fused G2P + stress + P2G kernel of EMPM_OPT_FUSE rollouts
+ * (the runs' first stress + P2G and last G2P are counted with the separate
+ * kernels above). */
+int  empm_ctx_fused_kernel_times(EmpmCtx* ctx, float* total_ms, int* launches);
 
 /* Device pointers of the context's grid buffers: float4 per node in the
  * blocked layout (4x4x4-node blocks of 64 consecutive float4, block (bi,bj,bk)

@@ -360,6 +360,56 @@ def rollouts(ref, rng):
     return out
 
 
+def inplace(ref, rng):
+    """The in-place substep MPMWARPDiff.p2g2p (mpm_solver_diff.py:293-429):
+    g2p with atomic_add on x and the PhysGaussian covariance update
+    (mpm_utils.py:441-499), then clip_particle_x (:582-599). Plasticine with
+    a moving cuboid, an impulse modifier, unsimulated particles and
+    update_cov_with_F on."""
+    torch, wp = ref.torch, ref.wp
+    out = {}
+    for tag, cov_on in (("cov", True), ("nocov", False)):
+        n, G, dt, T = 220, 16, 2e-4, 6
+        x = f32(rng.uniform(0.3, 0.7, (n, 3)))
+        v = f32(rng.standard_normal((n, 3)) * 2.5)
+        vol = float(np.float32(0.4 ** 3 / n))
+        E = f32(np.exp(rng.uniform(np.log(2e3), np.log(5e4), n)))
+        nu = f32(rng.uniform(0.2, 0.45, n))
+        mpm = ref.wrapper.WarpMPMWrapper(grid_size=G, grid_lim=1.0, frame_dt=dt, sim_dt=dt, device="cpu")
+        mpm.gravity = [0.0, -9.8, 0.0]
+        mpm.material_params = dict(ref.wrapper.material_gallery["plasticine"])
+        mpm.add_particles(torch.from_numpy(x), torch.from_numpy(v), vol, torch.from_numpy(E), torch.from_numpy(nu),
+                          1e3)
+        mpm.surface_colliders.append([(0.0, 3.0 / G, 0.0), (0.0, 1.0, 0.0), "sticky", 0.0])
+        cub = dict(point=[0.5, 0.74, 0.5], size=[0.1, 0.06, 0.1], velocity=[0.0, -2.0, 0.0])
+        mpm.moving_boundaries.append([cub["point"], cub["size"], cub["velocity"], 0.0])
+        mpm.initialize()
+        mpm.mpm_solver.add_bounding_box()
+        st, model, solver = mpm.mpm_state, mpm.mpm_model, mpm.mpm_solver
+        ys = f32(rng.uniform(5e2, 5e3, n))
+        model.yield_stress.data[...] = ys
+        imp = dict(force=[0.0, 0.0, 2e-3], point=[0.45, 0.45, 0.45], size=[0.1, 0.1, 0.1], num_dt=4)
+        solver.add_impulse_on_particles(st, force=imp["force"], dt=dt, point=imp["point"], size=imp["size"],
+                                        num_dt=imp["num_dt"], device="cpu")
+        sel = (rng.uniform(size=n) < 0.1).astype(np.int32)
+        st.particle_selection.data[...] = sel
+        A = rng.standard_normal((n, 3, 3)) * 1e-2
+        S = A @ np.transpose(A, (0, 2, 1)) + 1e-4 * np.eye(3)
+        cov = f32(np.stack([S[:, 0, 0], S[:, 0, 1], S[:, 0, 2], S[:, 1, 1], S[:, 1, 2], S[:, 2, 2]], 1).reshape(-1))
+        st.particle_cov.data[...] = cov
+        model.update_cov_with_F = cov_on
+        for step in range(T):
+            solver.p2g2p(model, st, step, dt, device="cpu")
+        scen = dict(n=n, G=G, dt=dt, T=T, vol=vol, rho=1e3, gravity=[0.0, -9.8, 0.0], cuboid=cub, impulse=imp,
+                    update_cov=cov_on)
+        out[tag] = dict(scenario=json.dumps(scen), x0=x, v0=v, E=E, nu=nu, ys_in=ys, sel=sel, cov0=cov,
+                        x=st.particle_x.data.copy(), v=st.particle_v.data.copy(), C=st.particle_C.data.copy(),
+                        F_trial=st.particle_F_trial.data.copy(), F=st.particle_F.data.copy(),
+                        cov=st.particle_cov.data.copy(), ys_out=model.yield_stress.data.copy(),
+                        mu_out=model.mu.data.copy(), lam_out=model.lam.data.copy())
+    return out
+
+
 def load_dynamic_utils(ref_root: str):
     """third_party/gaussian_splatting/dynamic_utils.py, unmodified. It imports
     kornia (0.8.1, not installed here) at module level; a stub module stands in
@@ -505,7 +555,7 @@ def main():
     args = ap.parse_args()
     ref = load_reference(args.reference)
     jobs = dict(kernel_stress=kernel_stress, kernel_p2g=kernel_p2g, kernel_grid=kernel_grid,
-                kernel_g2p=kernel_g2p, rollouts=rollouts, kernel_restart=kernel_restart, lbs=lbs)
+                kernel_g2p=kernel_g2p, rollouts=rollouts, kernel_restart=kernel_restart, lbs=lbs, inplace=inplace)
     for i, (name, fn) in enumerate(jobs.items()):
         if args.only and name != args.only:
             continue

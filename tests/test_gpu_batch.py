@@ -164,3 +164,50 @@ def test_rollout_resume_needs_a_sorted_state():
                              N.ROLLOUT_RESUME, _stream_ptr(b.device))
     assert rc == N.EMPM_OK
     torch.cuda.synchronize()
+
+
+def _rollout_with_holds(specs, fuse, holds, T=70, dt=2e-4, sort_every=16):
+    """One library rollout of the batch (stream path) with per-substep hold
+    flags: holds[i] = (first, last) substeps [first, last) in which instance i
+    is held."""
+    from empm_b200 import _native as N
+    from empm_b200.mpm_data_structure import _stream_ptr
+
+    b = BatchedMPM(specs, device=DEV)
+    b.fuse, b.sort_every = fuse, sort_every
+    b._apply_options()
+    mat = N.EmpmMaterial(b.vol.data_ptr(), b.mu.data_ptr(), b.lam.data_ptr(), b.yield_stress.data_ptr(), None,
+                         b._Fe.data_ptr())
+    table = (N.EmpmStep * (T * b.n_inst))()
+    for i, sv in enumerate(b.solvers):
+        t = 0.0
+        for s in range(T):
+            sv._fill_step(table[s * b.n_inst + i], t, dt)
+            sv._modify(t, dt)
+            t += dt
+    for i, (first, last) in holds.items():
+        for s in range(first, last):
+            table[s * b.n_inst + i].hold = 1
+    N.check(b.L.empm_rollout_ex(b.ptr, b._views(0), b._views(1), mat, table, T, T, 0, _stream_ptr(DEV)), b.ptr)
+    torch.cuda.synchronize()
+    out = 1 if T % 2 else 0
+    return (b._x4[out].clone(), b._v4[out].clone(), b._C[out].clone(), b._F[out].clone(), b._Fe.clone(),
+            b.yield_stress.clone(), b.read_status())
+
+
+@pytest.mark.parametrize("holds", [{}, {1: (23, 70)}, {0: (5, 70), 3: (40, 70)}, {2: (10, 30)}],
+                         ids=["no-holds", "held-to-end", "two-held", "released"])
+def test_fused_runs_match_separate_kernels(holds):
+    """Rollouts with the fused G2P + stress + P2G runs equal the separate
+    kernels (state, elastic F, material) up to FP32 reduction order, with
+    instances held to the end of the rollout (the serving pattern) and with a
+    hold that is released again (which runs the separate kernels)."""
+    specs = _specs(dynamic=True)
+    fused = _rollout_with_holds(specs, True, holds)
+    plain = _rollout_with_holds(specs, False, holds)
+    for name, a, c in zip(("x", "v", "C", "F_trial", "F_elastic", "yield"), fused[:6], plain[:6]):
+        scale = max(1.0, float(c.abs().max()))
+        err = max_abs(a, c)
+        print(f"{holds}: {name} fused vs separate {err:.2e}")
+        assert err <= 1e-5 * scale, name
+    assert fused[6] & 1 == 0 and plain[6] & 1 == 0
