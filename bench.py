@@ -67,38 +67,57 @@ def measured_traffic(workload: str, kernel: str, particles: int):
     return NCU_DRAM_BYTES.get((workload, kernel, int(particles)))
 
 
-def rollout_launches(n_steps: int, block: int, sort_every: int, resume: bool) -> int:
+def rollout_launches(n_steps: int, block: int, sort_every: int, resume: bool, fused: bool = True) -> int:
     """This library's kernel launches in one sorted rollout of n_steps
-    substeps run as graph blocks of `block` substeps: 4 per substep (P2G,
-    block list, grid update, G2P), 4 per cell sort (keys, chunk counts, cell
-    scan, scatter; its two CUB scans are not counted) and 1 per write-back."""
+    substeps run as graph blocks of `block` substeps: per substep the touched-
+    block list and the grid update, plus per run of k substeps between two
+    cell sorts (or block ends) either k stress + P2G and k G2P launches, or,
+    fused, one stress + P2G, k - 1 fused G2P + stress + P2G and one G2P; 4 per
+    cell sort (keys, chunk counts, cell scan, scatter; its two CUB scans are
+    not counted) and 1 per write-back."""
     if sort_every <= 0:
         return 4 * n_steps   # the direct path: no sort, the caller's buffers throughout
-    sorts = unsorts = 0
+    sorts = unsorts = particle = 0
     done, since = 0, 0
     while done < n_steps:
         k = min(block, n_steps - done)
         if not (resume and done > 0):
             sorts, since = sorts + 1, 0
-        for _ in range(k):
+        left = k
+        while left > 0:
             if since >= sort_every:
                 sorts, since = sorts + 1, 0
-            since += 1
+            run = min(left, sort_every - since)
+            particle += run + 1 if (fused and run >= 2) else 2 * run
+            since += run
+            left -= run
         if not resume or done + k >= n_steps:
             unsorts += 1
         done += k
-    return 4 * n_steps + 4 * sorts + unsorts
+    return 2 * n_steps + particle + 4 * sorts + unsorts
 
 
 def bytes_per_particle(material: str):
     """Algorithmic bytes per particle-substep: x, v, C, F read + written
     (192 B) and mass, vol, mu, lam read (16 B); plasticine adds the yield read
-    and the yield/mu/lam write-back (16 B). Split: the fused stress+P2G kernel
+    and the yield/mu/lam write-back (16 B). Split: the stress+P2G kernel
     performs every read (112 / 116 B) and the material write-back (0 / 12 B);
-    G2P writes x, v, C, F (96 B)."""
+    G2P writes x, v, C, F (96 B); the fused G2P + stress + P2G kernel does one
+    whole substep of particle work (208 / 224 B)."""
     if material == "plasticine":
-        return {"substep": 224, "stress_p2g": 128, "g2p": 96}
-    return {"substep": 208, "stress_p2g": 112, "g2p": 96}
+        return {"substep": 224, "stress_p2g": 128, "g2p": 96, "g2p2g": 224}
+    return {"substep": 208, "stress_p2g": 112, "g2p": 96, "g2p2g": 208}
+
+
+# State bytes per particle the fused G2P + stress + P2G kernel moves itself:
+# position and elastic F read and written in place (32 + 72 B), vol / mu /
+# lam / yield read (16 B) and, plasticine, mu / lam / yield written (12 B).
+FUSED_STATE_BYTES = {"plasticine": 132, "jelly": 120}
+
+
+def dominant_kernel(kms):
+    """The fused kernel when a rollout used it, else the separate stress + P2G."""
+    return "g2p2g" if kms.get("g2p2g", 0.0) > 0.0 else "stress_p2g"
 
 
 class ClockSampler:
@@ -282,7 +301,7 @@ def run_ours(args):
 
     w = get_workload(args.workload, args.particles, args.grid, args.substeps)
     solver, md, st, other = W.build_product(w, device=dev)
-    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap"):
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap", "fuse"):
         val = getattr(args, opt)
         if val is not None:
             setattr(solver, opt, val)
@@ -346,7 +365,7 @@ def run_ours(args):
     bp = bytes_per_particle(w.material)
     kms = {k: v[0] / max(v[1], 1) for k, v in kt.items()}
     top = max(kms, key=kms.get)
-    dom = "stress_p2g"
+    dom = dominant_kernel(kms)
     achieved = w.n * bp[dom] / (kms[dom] / 1e3) / 1e9
     substep_ms = ms / args.steps / w.T
     traffic = measured_traffic(w.name, dom, w.n)
@@ -403,12 +422,14 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_particle": bp[dom], "launch_ms": kms[dom],
+                     "kernel_state_bytes_per_particle": FUSED_STATE_BYTES.get(w.material) if dom == "g2p2g"
+                     else bp[dom],
                      "kernel_ms": {k: round(v, 5) for k, v in kms.items()}, "top_kernel": top,
                      "timing": "CUDA events around each kernel on its launch stream, stream path of one "
                                f"rollout in this run ({stream_ms:.2f} ms vs {ms / args.steps:.2f} ms graph)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": rollout_launches(w.T, w.T, solver.sort_every, False) * args.steps,
+        "gpu_launches": rollout_launches(w.T, w.T, solver.sort_every, False, dom == "g2p2g") * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -485,6 +506,8 @@ def run_ours_c4(args):
     explicit = [o for o in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap") if getattr(args, o) is not None]
     for opt in explicit:
         setattr(batch, opt, getattr(args, opt))
+    if args.fuse is not None:
+        batch.fuse = bool(args.fuse)
     tuned = None
     if not explicit and not args.no_autotune:
         # launch options from the autotuner, on this population, outside the timed region
@@ -494,8 +517,7 @@ def run_ours_c4(args):
         res = A.tune_batch(batch, dt, substeps=50)
         tuned = {"options": res["options"], "candidates": len(res["ms"]), "seconds": time.perf_counter() - t_tune,
                  "best_ms_per_substep": min(res["ms"].values()),
-                 "default_ms_per_substep": res["ms"].get(json.dumps(dict(sort_every=32, p2g_mode=2, tile_cap=1024,
-                                                                         seg_cap=4, g2p_tile=0), sort_keys=True))}
+                 "default_ms_per_substep": res["ms"].get(json.dumps(A.DEFAULTS, sort_keys=True))}
     init = [t.clone() for t in (batch._x4[0], batch._v4[0], batch._C[0], batch._F[0], batch.mu, batch.lam,
                                 batch.yield_stress)]
 
@@ -550,7 +572,7 @@ def run_ours_c4(args):
     peak, peak_kind = load_peaks()
     bp = bytes_per_particle("plasticine")
     kms = {k: v[0] / max(v[1], 1) for k, v in kt.items()}
-    dom = "stress_p2g"
+    dom = dominant_kernel(kms)
     achieved = total * bp[dom] / (kms[dom] / 1e3) / 1e9
     substep_ms = ms / args.steps / T
 
@@ -656,7 +678,7 @@ def run_ours_c4(args):
                               if batch.resume_blocks else "; every block sorts and writes back"),
                    "options": {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode,
                                "g2p_tile": batch.g2p_tile, "tile_cap": batch.tile_cap,
-                               "seg_cap": batch.seg_cap},
+                               "seg_cap": batch.seg_cap, "fuse": bool(batch.fuse)},
                    "autotune": tuned,
                    "substep_us": substep_ms * 1e3,
                    "substep_hbm_frac": (total * bp["substep"] / (substep_ms / 1e3) / 1e9) / peak,
@@ -674,12 +696,14 @@ def run_ours_c4(args):
                      "traffic": measured_traffic("c4", dom, total),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, same workload",
                      "algorithmic_bytes_per_particle": bp[dom], "launch_ms": kms[dom],
+                     "kernel_state_bytes_per_particle": FUSED_STATE_BYTES["plasticine"] if dom == "g2p2g"
+                     else bp[dom],
                      "kernel_ms": {k: round(v, 5) for k, v in kms.items()},
                      "timing": "CUDA events around each kernel on its launch stream, stream path of one "
                                f"population rollout in this run ({stream_ms:.2f} ms vs {ms / args.steps:.2f} ms graph)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": total * 36, "d2h_bytes_per_step": total * 12},
-        "gpu_launches": rollout_launches(T, 50, batch.sort_every, batch.resume_blocks) * args.steps,
+        "gpu_launches": rollout_launches(T, 50, batch.sort_every, batch.resume_blocks, dom == "g2p2g") * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -1323,6 +1347,8 @@ def main():
     ap.add_argument("--tile-cap", dest="tile_cap", type=int, default=None)
     ap.add_argument("--seg-cap", dest="seg_cap", type=int, default=None,
                     help="warp-aggregated P2G: longest same-cell run per reduction (4, 8, 16, 32)")
+    ap.add_argument("--fuse", dest="fuse", type=int, default=None,
+                    help="1 = fused G2P + stress + P2G between cell sorts (default), 0 = separate kernels")
     ap.add_argument("--resume-blocks", dest="resume_blocks", type=int, default=None,
                     help="c4: 1 = graph blocks continue from the library's sorted state (default), 0 = each block "
                          "sorts the caller's buffers and writes them back")

@@ -9,7 +9,9 @@ substeps of the caller's own workload under each candidate:
 * ``p2g_mode`` / ``tile_cap`` / ``seg_cap``: warp-aggregated reductions into
   the grid over same-cell runs of at most 4 or 8 lanes, or accumulation in a
   per-CTA shared-memory node tile of 512 / 1024 / 2048 nodes (the tile shape);
-* ``g2p_tile``: G2P gathering directly from L2 or from a staged tile.
+* ``g2p_tile``: G2P gathering directly from L2 or from a staged tile;
+* ``fuse``: the G2P of each substep and the stress + P2G of the next as one
+  kernel between cell sorts, or separate kernels.
 
 It restores the state after every trial, keeps the fastest candidate and
 applies it. Results are cached in memory (and, when ``path`` is given, in a
@@ -25,11 +27,13 @@ import os
 from typing import Dict, List, Optional, Sequence
 
 CANDIDATES: List[Dict[str, int]] = [
-    dict(sort_every=s, p2g_mode=m, tile_cap=c, seg_cap=k, g2p_tile=g)
-    for s, (m, c, k), g in itertools.product(
-        (8, 16, 32), ((2, 1024, 4), (2, 1024, 8), (1, 512, 4), (1, 1024, 4), (1, 2048, 4)), (0, 1))
+    dict(sort_every=s, p2g_mode=m, tile_cap=c, seg_cap=k, g2p_tile=g, fuse=f)
+    for s, (m, c, k), g, f in itertools.product(
+        (8, 16, 32), ((2, 1024, 4), (2, 1024, 8), (1, 512, 4), (1, 1024, 4), (1, 2048, 4)), (0, 1), (1, 0))
+    if f == 1 or (m == 2 and g == 0)   # fusing applies to warp-aggregated P2G with direct G2P only
 ]
-OPTION_NAMES = ("sort_every", "p2g_mode", "tile_cap", "seg_cap", "g2p_tile")
+OPTION_NAMES = ("sort_every", "p2g_mode", "tile_cap", "seg_cap", "g2p_tile", "fuse")
+DEFAULTS = dict(sort_every=32, p2g_mode=2, tile_cap=1024, seg_cap=4, g2p_tile=0, fuse=1)
 
 _MEMORY: Dict[str, Dict] = {}
 
@@ -81,7 +85,8 @@ def _restore_colliders(snap) -> None:
 
 def _apply(target, opts: Dict[str, int]) -> None:
     for k in OPTION_NAMES:
-        setattr(target, k, int(opts[k]) if k != "g2p_tile" else bool(opts[k]))
+        v = opts.get(k, DEFAULTS[k])
+        setattr(target, k, bool(v) if k in ("g2p_tile", "fuse") else int(v))
 
 
 def tune_batch(batch, dt: float, substeps: int = 32, candidates: Optional[List[Dict[str, int]]] = None,

@@ -6,11 +6,24 @@ from empm_b200 import autotune as A
 
 def test_candidates_cover_every_launch_option():
     keys = {tuple(sorted(c.items())) for c in A.CANDIDATES}
-    assert len(keys) == len(A.CANDIDATES) == 30
+    assert len(keys) == len(A.CANDIDATES) == 36
     assert {c["sort_every"] for c in A.CANDIDATES} == {8, 16, 32}
     assert {(c["p2g_mode"], c["tile_cap"], c["seg_cap"]) for c in A.CANDIDATES} == {
         (2, 1024, 4), (2, 1024, 8), (1, 512, 4), (1, 1024, 4), (1, 2048, 4)}
     assert {c["g2p_tile"] for c in A.CANDIDATES} == {0, 1}
+    # the separate-kernel variant is a candidate wherever fusing applies
+    unfused = [c for c in A.CANDIDATES if c["fuse"] == 0]
+    assert len(unfused) == 6 and all(c["p2g_mode"] == 2 and c["g2p_tile"] == 0 for c in unfused)
+    assert A.DEFAULTS in A.CANDIDATES
+
+
+def test_apply_fills_options_missing_from_old_cache_entries():
+    class T:
+        pass
+
+    t = T()
+    A._apply(t, dict(sort_every=16, p2g_mode=2, tile_cap=1024, seg_cap=8, g2p_tile=0))
+    assert (t.sort_every, t.seg_cap, t.fuse, t.g2p_tile) == (16, 8, True, False)
 
 
 def test_signature_buckets_particle_counts():
