@@ -657,6 +657,33 @@ def run_ours_c4(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(c4_instance_workload(specs[0], dt, T), budget_s=12.0, max_substeps=60)
+    served = None
+    if not args.no_served and world == 1:
+        # the serving stream's figures in the same line (BASELINE metric: batched / served vs
+        # plain, p50 / p99), on one GPU: the population's buffers are released first
+        bopts = {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode, "g2p_tile": batch.g2p_tile,
+                 "tile_cap": batch.tile_cap, "seg_cap": batch.seg_cap, "fuse": bool(batch.fuse)}
+        resume = batch.resume_blocks
+        del batch
+        import gc
+
+        gc.collect()
+        torch.cuda.empty_cache()
+        c5 = measure_c5(args, dev, world, rank, local, cpu_baseline_leg=False)
+        if c5 is not None:
+            cf = c5["config"]
+            served = {"metric": c5["metric"], "value": c5["value"], "unit": c5["unit"],
+                      "workload": cf["workload"], "requests": cf["requests"], "completed": cf["completed"],
+                      "gradient_requests": cf["gradient_requests"], "latency_ms": cf["latency_ms"],
+                      "makespan_s": cf["makespan_s"], "plain_value": cf["plain_value"],
+                      "served_vs_plain": cf["served_vs_plain"], "plain_kernel_value": cf["plain_kernel_value"],
+                      "served_vs_plain_kernel": cf["served_vs_plain_kernel"], "plain": cf["plain"],
+                      "plain_kernel": cf["plain_kernel"], "timing": cf["timing"], "gpu_launches": c5["gpu_launches"],
+                      "clocks": c5["clocks"]}
+    else:
+        bopts = {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode, "g2p_tile": batch.g2p_tile,
+                 "tile_cap": batch.tile_cap, "seg_cap": batch.seg_cap, "fuse": bool(batch.fuse)}
+        resume = batch.resume_blocks
     if world > 1:
         import torch.distributed as dist
 
@@ -675,10 +702,8 @@ def run_ours_c4(args):
                    "l2": "inputs larger than L2 (working set ~1 GB > 126 MB), no flush",
                    "launch": "one CUDA graph per 50-substep block for the whole population" +
                              ("; blocks continue from the library's cell-sorted state, one write-back per rollout"
-                              if batch.resume_blocks else "; every block sorts and writes back"),
-                   "options": {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode,
-                               "g2p_tile": batch.g2p_tile, "tile_cap": batch.tile_cap,
-                               "seg_cap": batch.seg_cap, "fuse": bool(batch.fuse)},
+                              if resume else "; every block sorts and writes back"),
+                   "options": bopts,
                    "autotune": tuned,
                    "substep_us": substep_ms * 1e3,
                    "substep_hbm_frac": (total * bp["substep"] / (substep_ms / 1e3) / 1e9) / peak,
@@ -690,7 +715,8 @@ def run_ours_c4(args):
                    "batched_vs_plain_rollout": (value / world) / plain_rollout_value if plain_rollout_value else None,
                    "plain_rollout": "each instance alone through this library's rollout path (cell sort, one CUDA "
                                     "graph per 300-substep rollout)",
-                   "status_word": status},
+                   "status_word": status,
+                   "served": served},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": measured_traffic("c4", dom, total),
@@ -703,7 +729,7 @@ def run_ours_c4(args):
                                f"population rollout in this run ({stream_ms:.2f} ms vs {ms / args.steps:.2f} ms graph)"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": total * 36, "d2h_bytes_per_step": total * 12},
-        "gpu_launches": rollout_launches(T, 50, batch.sort_every, batch.resume_blocks, dom == "g2p2g") * args.steps,
+        "gpu_launches": rollout_launches(T, 50, bopts["sort_every"], resume, dom == "g2p2g") * args.steps,
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -936,6 +962,22 @@ def run_ours_c5(args):
     world, rank, local = dist_setup(args)
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
+    line = measure_c5(args, dev, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def measure_c5(args, dev, world, rank, local, cpu_baseline_leg=True):
+    """The serving stream's JSON line (rank 0; other ranks get None). With
+    world > 1 the makespan is the max and the served work the sum over ranks
+    (one collective each); the process group stays up."""
+    import torch
+
     from empm_b200 import workloads as W
     from empm_b200.adjoint import CheckpointedRollout
     from empm_b200.batch import single_instance
@@ -1058,7 +1100,7 @@ def run_ours_c5(args):
     plain_kernel_value = plain_ps / (kernel_ms / 1e3)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_baseline_leg and not args.no_cpu_baseline:
         cpu = cpu_baseline(W.c2(n=200_000, T=40), budget_s=10.0, max_substeps=40)
         cpu["sample"] += " (the serving stream's plasticine material distributions)"
     if world > 1:
@@ -1070,9 +1112,8 @@ def run_ours_c5(args):
         sv = t[1:].clone()
         dist.all_reduce(sv, op=dist.ReduceOp.SUM)
         value = float(sv.item()) / float(mk.item())
-        dist.destroy_process_group()
     if rank != 0:
-        return 0
+        return None
     n_grad_substeps = sum(r[3] for r in ok if r[1])
     line = {
         "metric": "served " + METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": 1,
@@ -1114,8 +1155,7 @@ def run_ours_c5(args):
         "gpu_launches": 4 * stats["substeps"] + 8 * n_grad_substeps,
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # ---------------------------------------------------------------------------
@@ -1337,6 +1377,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="c4: skip the one-instance-at-a-time comparison")
+    ap.add_argument("--no-served", dest="no_served", action="store_true",
+                    help="c4: skip the serving-stream leg nested in the line (config.served)")
     ap.add_argument("--ref-substeps", type=int, default=2, help="substeps per step of the reference arm")
     ap.add_argument("--particles", type=int, default=None, help="override the workload's particle count")
     ap.add_argument("--grid", type=int, default=None, help="override the workload's grid resolution")
