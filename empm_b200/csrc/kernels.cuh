@@ -31,6 +31,10 @@
 #ifndef EMPM_G2P_MIN_CTAS
 #define EMPM_G2P_MIN_CTAS 8
 #endif
+// ... and for the fused G2P + stress + P2G kernel
+#ifndef EMPM_FUSED_MIN_CTAS
+#define EMPM_FUSED_MIN_CTAS 4
+#endif
 
 namespace empm {
 
@@ -663,7 +667,7 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
 // the run: when a particle's instance becomes held at substep s, its state
 // after the G2P of s-1 is written in full, then left alone.
 template <int ROUNDS, int MAT = -1>
-__global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_g2p2g(ParticleArrays P, MaterialArrays M, F9Planes Fe,
+__global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g(ParticleArrays P, MaterialArrays M, F9Planes Fe,
                                                                   Launch L, int g2p_table, const float4* vel,
                                                                   float4* mom, unsigned char* flags) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
