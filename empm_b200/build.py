@@ -3,7 +3,8 @@
     python -m empm_b200.build [--verbose]
 
 Every ``csrc/*.cu`` is compiled to an object and linked into
-``empm_b200/_lib/libempm_b200.so`` (cudart linked statically).
+``empm_b200/_lib/libempm_b200.so`` (cudart linked statically). Objects are
+rebuilt when the hash of their sources, the headers and the flags changes.
 """
 from __future__ import annotations
 
@@ -22,6 +23,9 @@ BUILD_DIR = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                      "-Xptxas", "-warn-spills"]
+# extra nvcc arguments, e.g. launch-shape macros for a sweep:
+#   EMPM_NVCC_EXTRA="-DEMPM_FUSED_MIN_CTAS=3" python -m empm_b200.build
+NVCC_FLAGS += os.environ.get("EMPM_NVCC_EXTRA", "").split()
 
 
 def nvcc() -> str:

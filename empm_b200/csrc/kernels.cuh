@@ -35,6 +35,10 @@
 #ifndef EMPM_FUSED_MIN_CTAS
 #define EMPM_FUSED_MIN_CTAS 4
 #endif
+// 1: the fused kernel's G2P gathers with a run-time outer stencil loop
+#ifndef EMPM_FUSED_G2P_LOOP
+#define EMPM_FUSED_G2P_LOOP 0
+#endif
 
 namespace empm {
 
@@ -684,7 +688,11 @@ __global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g(ParticleArra
             const Stencil st = make_stencil(x, c.inv_dx);
             const bool in_grid = stencil_in_grid(st, c.G);
             GlobalFetch fetch{vel, &c};
+#if EMPM_FUSED_G2P_LOOP
+            const G2POut o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
+#else
             const G2POut o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
+#endif
             const float dx = 1.f / c.inv_dx;   // as g2p_particle computes it
             const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
             V3 nx = x + dt * o.v;

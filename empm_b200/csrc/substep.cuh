@@ -376,6 +376,53 @@ __device__ __forceinline__ G2POut g2p_gather(const Stencil& st, float inv_dx, Fe
     return o;
 }
 
+// g2p_gather with a run-time loop over the outer stencil axis (weights picked
+// by selects): a third of the code, fewer gathers in flight. The kernel that
+// runs G2P and P2G back to back uses it where its size is what limits it.
+template <typename Fetch>
+__device__ __forceinline__ G2POut g2p_gather_rt(const Stencil& st, float inv_dx, Fetch fetch) {
+    V3 vs = v3(0.f, 0.f, 0.f);
+    V3 m0 = vs, m1 = vs, m2 = vs;
+    V3 g0 = vs, g1 = vs, g2 = vs;
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
+        const float dwx = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        V3 si = v3(0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float wxy = wx * st.w[1][j], dxy = dwx * st.w[1][j], xdy = wx * st.dw[1][j];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const V3 g = fetch(i, j, k);
+                const float wz = st.w[2][k];
+                const V3 wg = (wxy * wz) * g;
+                si = si + wg;
+                if (j) m1 = m1 + (float)j * wg;
+                if (k) m2 = m2 + (float)k * wg;
+                g0 = g0 + (dxy * wz) * g;
+                g1 = g1 + (xdy * wz) * g;
+                g2 = g2 + (wxy * st.dw[2][k]) * g;
+            }
+        }
+        vs = vs + si;
+        m0 = m0 + (float)i * si;
+    }
+    G2POut o;
+    o.v = vs;
+    const float c4 = 4.f * inv_dx;
+    const V3 mc[3] = {m0 - st.fx[0] * vs, m1 - st.fx[1] * vs, m2 - st.fx[2] * vs};
+    const V3 gc[3] = {g0, g1, g2};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            o.C.m[3 * r + c] = c4 * comp(mc[c], r);
+            o.gradv.m[3 * r + c] = inv_dx * comp(gc[c], r);
+        }
+    return o;
+}
+
 __device__ __forceinline__ bool finite3(V3 a) {
     return isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
 }

@@ -144,7 +144,7 @@ class MPMDifferentiableSimulationTrail(autograd.Function):
             prev, _ = _run(mpm_solver, mpm_model, prev, extra_no_grad_steps, substep_size)
         prev.update_mass()
         mpm_solver.prepare_mu_lam(mpm_model, prev, device=device)
-        ctx.requires_grad = requires_grad
+        ctx.taped = requires_grad   # (ctx.requires_grad is reserved by torch.autograd)
         if not requires_grad:
             final, recorded = _run(mpm_solver, mpm_model, prev, num_substeps, substep_size, record_every=substep,
                                    step_callback=mpm_solver.step_callback)

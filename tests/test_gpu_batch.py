@@ -205,9 +205,15 @@ def test_fused_runs_match_separate_kernels(holds):
     specs = _specs(dynamic=True)
     fused = _rollout_with_holds(specs, True, holds)
     plain = _rollout_with_holds(specs, False, holds)
+    # tolerances of the other parity tests: positions 1e-5 between GPU paths,
+    # fields relative to their largest magnitude (1e-4 for C, whose run-to-run
+    # spread under a different reduction order is about 3e-5 here even with
+    # identical kernels: see the "released" case, which runs the separate
+    # kernels in both modes)
+    tol = {"x": 1e-5, "v": 1e-5, "C": 1e-4, "F_trial": 2e-5, "F_elastic": 2e-5, "yield": 1e-5}
     for name, a, c in zip(("x", "v", "C", "F_trial", "F_elastic", "yield"), fused[:6], plain[:6]):
         scale = max(1.0, float(c.abs().max()))
         err = max_abs(a, c)
-        print(f"{holds}: {name} fused vs separate {err:.2e}")
-        assert err <= 1e-5 * scale, name
+        print(f"{holds}: {name} fused vs separate {err:.2e} (scale {scale:.3g})")
+        assert err <= tol[name] * scale, name
     assert fused[6] & 1 == 0 and plain[6] & 1 == 0
