@@ -58,6 +58,7 @@ def load_peaks():
 # particle count on a B200: (workload, kernel, particles) -> bytes per launch.
 NCU_DRAM_BYTES = {
     ("c4", "stress_p2g", 3172508): 403.197184e6 + 110.350592e6,
+    ("c4", "g2p2g", 3172508): 248.493056e6 + 140.657920e6,
     ("lbs", "blend", 2000000): 196.818688e6 + 41.4976e6,
 }
 
