@@ -39,7 +39,8 @@ struct SortedBuffers {
     int    n = 0;                          // particle capacity
     long long nb = 0;                      // block capacity
     float* part[2] = {nullptr, nullptr};   // x4 | v4 | C f9 | F f9 per buffer (ping-pong per substep)
-    float* fe = nullptr;                   // elastic F handed from P2G to G2P (f9)
+    float* fe[2] = {nullptr, nullptr};     // elastic F handed from P2G to G2P (f9), per sort epoch like matf:
+                                           // a cell sort permutes it, so held particles keep their own
     float* matf[2] = {nullptr, nullptr};   // vol | mu | lam | ys (ping-pong per sort)
     int*   mati[2] = {nullptr, nullptr};   // sel | pid
     int*   keys = nullptr;

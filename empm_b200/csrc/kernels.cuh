@@ -36,8 +36,10 @@
 #define EMPM_FUSED_MIN_CTAS 4
 #endif
 // 1: the fused kernel's G2P gathers with a run-time outer stencil loop
+// (population workload: 598 us per launch against 604 us fully unrolled; at 3
+// or 2 CTAs per SM 603-608 and 722 us)
 #ifndef EMPM_FUSED_G2P_LOOP
-#define EMPM_FUSED_G2P_LOOP 0
+#define EMPM_FUSED_G2P_LOOP 1
 #endif
 
 namespace empm {
@@ -517,6 +519,7 @@ struct PermuteArgs {
     const float* ys_s;  float* ys_d;
     const int*   sel_s; int*   sel_d;
     const int*   pid_s; int*   pid_d;   // pid_s NULL: source is in caller order
+    F9Planes     fe_s, fe_d;             // elastic F (fe_s.a NULL: not moved)
     const int*   keys;
     const int*   ranks;
     const int*   offsets;    // cell offsets
@@ -538,6 +541,7 @@ __global__ void k_sort_scatter(const PermuteArgs a) {
     a.ys_d[d] = __ldg(a.ys_s + p);
     a.sel_d[d] = a.sel_s ? __ldg(a.sel_s + p) : 0;
     a.pid_d[d] = a.pid_s ? __ldg(a.pid_s + p) : p;
+    if (a.fe_s.a) f9_store(a.fe_d, d, f9_load(a.fe_s, p));
 }
 
 struct UnsortArgs {

@@ -119,8 +119,9 @@ static void free_sorted(SortedBuffers& sb) {
         if (sb.part[i]) cudaFree(sb.part[i]);
         if (sb.matf[i]) cudaFree(sb.matf[i]);
         if (sb.mati[i]) cudaFree(sb.mati[i]);
+        if (sb.fe[i]) cudaFree(sb.fe[i]);
     }
-    void* ptrs[] = {sb.fe, sb.keys, sb.ranks, sb.block_counts, sb.block_offsets, sb.chunk_counts, sb.chunk_offsets,
+    void* ptrs[] = {sb.keys, sb.ranks, sb.block_counts, sb.block_offsets, sb.chunk_counts, sb.chunk_offsets,
                     sb.cell_counts, sb.cell_offsets, sb.chunks, sb.nchunks, sb.scan_tmp};
     for (void* q : ptrs) if (q) cudaFree(q);
     sb = SortedBuffers();
@@ -650,8 +651,8 @@ static int ensure_sorted_buffers(EmpmCtx* ctx) {
         e = cudaMalloc(&sb.part[i], sizeof(float) * 26 * padded4(n) + 64);
         if (e == cudaSuccess) e = cudaMalloc(&sb.matf[i], sizeof(float) * 4 * (size_t)n + 64);
         if (e == cudaSuccess) e = cudaMalloc(&sb.mati[i], sizeof(int) * 2 * (size_t)n + 64);
+        if (e == cudaSuccess) e = cudaMalloc(&sb.fe[i], sizeof(float) * 9 * (size_t)n + 64);
     }
-    if (e == cudaSuccess) e = cudaMalloc(&sb.fe, sizeof(float) * 9 * (size_t)n + 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.keys, sizeof(int) * (size_t)n + 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.ranks, sizeof(int) * (size_t)n + 64);
     if (e == cudaSuccess) e = cudaMalloc(&sb.block_counts, sizeof(int) * nblocks);
@@ -727,6 +728,15 @@ static int launch_sort(EmpmCtx* ctx, SortedState& ss, const ParticleArrays* user
     }
     const int dp = user_src ? ss.pc : 1 - ss.pc;
     const int dm = user_src ? ss.mc : 1 - ss.mc;
+    // elastic F travels with the sort: particles of a held instance keep
+    // theirs (the others' is rewritten by their next stress + P2G)
+    a.fe_s = F9Planes{};
+    if (user_src) {
+        if (user_mat->F_elastic) a.fe_s = f9_planes(user_mat->F_elastic, n);
+    } else {
+        a.fe_s = f9_planes(sb.fe[ss.mc], n);
+    }
+    a.fe_d = f9_planes(sb.fe[dm], n);
     a.dst = particle_arrays(sb.part[dp], n);
     const MaterialArrays D = sorted_material(ctx, dm);
     a.vol_d = const_cast<float*>(D.vol); a.mu_d = D.mu; a.lam_d = D.lam; a.ys_d = D.ys;
@@ -762,7 +772,7 @@ static TiledArgs sorted_args(EmpmCtx* ctx, const SortedState& ss, int table) {
     TiledArgs t;
     t.P = particle_arrays(sb.part[ss.pc], n);
     t.M = sorted_material(ctx, ss.mc);
-    t.Fe = f9_planes(sb.fe, n);
+    t.Fe = f9_planes(sb.fe[ss.mc], n);
     t.L = make_launch(ctx, table);
     t.cl.chunks = sb.chunks;
     t.cl.nchunks = sb.nchunks;
@@ -900,7 +910,7 @@ static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, cons
     UnsortArgs u;
     u.src = particle_arrays(ctx->sb.part[ss.pc], n);
     u.dst = particle_arrays((n_steps & 1) ? b : a, n);
-    u.Fe_s = f9_planes(ctx->sb.fe, n);
+    u.Fe_s = f9_planes(ctx->sb.fe[ss.mc], n);
     u.Fe_d = f9_planes(mat->F_elastic, n);
     const MaterialArrays M = sorted_material(ctx, ss.mc);
     u.mu_s = M.mu; u.mu_d = mat->mu;
@@ -1594,6 +1604,7 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
         um.mu = const_cast<float*>(ckpt_mu);
         um.lam = const_cast<float*>(ckpt_lam);
         um.yield_stress = const_cast<float*>(ckpt_yield);
+        um.F_elastic = nullptr;   // not an input of a segment (its P2G recomputes it)
         rc = launch_sort(ctx, ss, &ua, &um, s);
         if (rc) return rc;
         CK(cudaMemcpyAsync(ab.states, ctx->sb.part[ss.pc], state_floats * sizeof(float), d2d, s), "sorted checkpoint");
@@ -1801,6 +1812,7 @@ extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmPa
         um.mu = const_cast<float*>(ckpt_mu);
         um.lam = const_cast<float*>(ckpt_lam);
         um.yield_stress = const_cast<float*>(ckpt_yield);
+        um.F_elastic = nullptr;   // not an input of a segment (its P2G recomputes it)
         rc = launch_sort(ctx, ss, &ua, &um, s);
         if (rc) return rc;
         CK(cudaMemcpyAsync(seg->states, ctx->sb.part[ss.pc], 26 * np * sizeof(float), d2d, s), "sorted checkpoint");

@@ -21,7 +21,8 @@ the GPU tests in tests/test_gpu_fullsize.py compare against:
                    material (3e4, 0.35, 2e3) and the guess (1e4, 0.25, 1e3).
                    Central finite differences (h = 1e-3 relative) of the loss
                    in E, nu, yield stress and along a seeded direction of the
-                   initial velocities.
+                   initial velocities, and the FP64 residual x_T - x_T(target)
+                   of every particle.
 
 The workloads come from empm_b200.workloads (seeded numpy generators; no
 GPU is involved). The oracle keeps the colliders as the reference does, in
@@ -33,7 +34,7 @@ disagree. With float64 tests the FP32 and FP64 oracles drift apart by
 6e-7. Runtime on 8 host cores: about 12 min (c2), 12 min (c4)
 and 10 min (c3).
 
-    python tests/golden/make_fullsize.py [c2] [c4] [c3]
+    python tests/golden/make_fullsize.py [c2] [c4] [c3] [c3_residual]
 """
 from __future__ import annotations
 
@@ -120,15 +121,26 @@ def c3_direction(n: int) -> np.ndarray:
     return (np.random.default_rng(C3_DIR_SEED).standard_normal((n, 3)) * 0.05).astype(np.float32)
 
 
-def c3_loss(w, target, E=None, nu=None, ys=None, v=None) -> float:
+def c3_final(w, E=None, nu=None, ys=None, v=None) -> np.ndarray:
     sim = O.OracleSim(w.x, w.v if v is None else v, w.vol, w.rho.astype(np.float64) * w.vol,
                       w.E if E is None else E, w.nu if nu is None else nu, n_grid=w.G,
                       material=OS.MATERIAL_IDS[w.material], gravity=w.gravity,
                       yield_stress=w.ys if ys is None else ys, precision="fp64_omp", collider_f32=True)
     sim.colliders = OS.oracle_colliders(w.colliders)
     sim.rollout(w.dt, w.T)
-    d = sim.x - target
+    return sim.x
+
+
+def c3_loss(w, target, **kw) -> float:
+    d = c3_final(w, **kw) - target
     return float((d * d).sum(1).mean())
+
+
+def c3_residual(w, target) -> np.ndarray:
+    """x_T(guess) - x_T(target) of every particle in FP64, stored as float32
+    (its values are about 2e-5, so float32 keeps 7 digits of it): the
+    residual whose 2/N multiple is dL/dx_T."""
+    return (c3_final(w) - target).astype(np.float32)
 
 
 def make_c3(path: str) -> None:
@@ -138,7 +150,8 @@ def make_c3(path: str) -> None:
     ts = OS.sim_from_workload(tw, precision="fp64_omp", collider_f32=True)
     ts.rollout(tw.dt, tw.T)
     target = ts.x.copy()
-    base = c3_loss(w, target)
+    residual = c3_residual(w, target)
+    base = float((residual.astype(np.float64) ** 2).sum(1).mean())
     print(f"c3 target + base loss {base:.9e} ({time.time() - t0:.0f} s)", flush=True)
     E0, nu0, ys0 = float(w.E[0]), float(w.nu[0]), float(w.ys[0])
     v64 = w.v.astype(np.float64)
@@ -159,15 +172,28 @@ def make_c3(path: str) -> None:
     np.savez_compressed(path, names=np.array(names), fd=np.array([fd[k] for k in names]),
                         loss_plus=np.array([lp[k] for k in names]), loss_minus=np.array([lm[k] for k in names]),
                         step=np.array([cases[k][0] for k in names]), loss=base, h=C3_H, dir_seed=C3_DIR_SEED,
-                        target_subset_idx=subset(w.n, 4096, 3003), target_subset_x=target[subset(w.n, 4096, 3003)])
+                        residual=residual)
+
+
+def add_c3_residual(path: str) -> None:
+    """Recompute only the FP64 residual of an existing c3 fixture."""
+    w = W.c3()
+    tw = W.c3(guess=False)
+    ts = OS.sim_from_workload(tw, precision="fp64_omp", collider_f32=True)
+    ts.rollout(tw.dt, tw.T)
+    old = dict(np.load(path))
+    old.pop("target_subset_idx", None)
+    old.pop("target_subset_x", None)
+    old["residual"] = c3_residual(w, ts.x.copy())
+    np.savez_compressed(path, **old)
 
 
 def main(argv) -> None:
     O.build()
     jobs = argv or ["c2", "c4", "c3"]
-    make = {"c2": make_c2, "c4": make_c4, "c3": make_c3}
+    make = {"c2": make_c2, "c4": make_c4, "c3": make_c3, "c3_residual": add_c3_residual}
     for j in jobs:
-        make[j](os.path.join(HERE, f"fullsize_{j}.npz"))
+        make[j](os.path.join(HERE, f"fullsize_{j.split('_')[0]}.npz"))
 
 
 if __name__ == "__main__":

@@ -112,7 +112,38 @@ def test_c4_population_vs_fp64_oracle():
     assert worst <= POS_BAR
 
 
+def _c3_grads(res, md, direction):
+    g_E, g_nu, _ = prepare_adjoint(md.E, md.nu, res["mu"], res["lam"])
+    return {"E": float(g_E.double().sum()), "nu": float(g_nu.double().sum()),
+            "yield_stress": float(res["yield_stress"].double().sum()),
+            "v0_dir": float((res["v"].double() * direction.double()).sum())}
+
+
+def _c3_errors(got, fd, names, theta, what):
+    """Relative errors; a derivative that vanishes (no particle reaches the
+    yield surface in this rollout, so dL/dyield is 0 up to rounding) is
+    measured against the largest parameter-scaled sensitivity instead."""
+    scale = max(abs(fd[k] * theta[k]) for k in names)
+    worst = 0.0
+    for k in names:
+        if abs(fd[k] * theta[k]) > 1e-6 * scale:
+            rel, kind = abs(got[k] - fd[k]) / abs(fd[k]), "relative error"
+        else:
+            rel, kind = abs((got[k] - fd[k]) * theta[k]) / scale, "vanishing derivative; error / largest sensitivity"
+        worst = max(worst, rel)
+        print(f"c3 {what} dL/d{k}: adjoint {got[k]:.6e} central difference {fd[k]:.6e} {kind} {rel:.2e}")
+    return worst
+
+
 def test_c3_gradients_vs_central_differences():
+    """The loss of this workload is small (4.9e-10: the guess and target
+    rollouts end about 2e-5 apart) next to the FP32 rounding of the positions
+    over 400 substeps (about 1e-7), so the FP32 residual x_T - x_T(target)
+    the GPU forms itself is off by a few 1e-3, and so is any gradient built on
+    it. The adjoint is therefore checked on the FP64 residual of the oracle
+    (dL/dx_T = 2 r / N from the fixture), which isolates its own error: bar
+    1e-3. The gradient built on the GPU's own residual is reported beside it
+    with the bar 1e-2 that this rounding leaves."""
     f = _fixture("c3")
     names = [str(s) for s in f["names"]]
     fd = dict(zip(names, f["fd"]))
@@ -133,30 +164,17 @@ def test_c3_gradients_vs_central_differences():
     tape = CheckpointedRollout(solver, md, st, w.dt, w.T, checkpoint_every=20)
     final = tape.forward()
     diff = final.particle_x - x_target
-    loss = float((diff * diff).sum(1).mean())
-    res = tape.backward(g_x=2.0 * diff / w.n)
-    g_E, g_nu, _ = prepare_adjoint(md.E, md.nu, res["mu"], res["lam"])
+    loss = float((diff.double() ** 2).sum(1).mean())
     direction = t((np.random.default_rng(int(f["dir_seed"])).standard_normal((w.n, 3)) * 0.05).astype(np.float32))
-    got = {"E": float(g_E.double().sum()), "nu": float(g_nu.double().sum()),
-           "yield_stress": float(res["yield_stress"].double().sum()),
-           "v0_dir": float((res["v"].double() * direction.double()).sum())}
-    print(f"c3 loss {loss:.6e} (FP64 oracle {float(f['loss']):.6e}); stored tape: {tape.stored}")
-    # Sensitivities scaled by the parameter (dL/dtheta * theta, and the
-    # directional derivative as it is): a derivative that vanishes (no
-    # particle reaches the yield surface in this rollout, so dL/dyield is 0 up
-    # to rounding) is checked against the largest sensitivity instead of
-    # itself.
+    r64 = t(f["residual"])
+    res_diff = float((diff.double() - r64.double()).abs().max())
     theta = {"E": float(w.E[0]), "nu": float(w.nu[0]), "yield_stress": float(w.ys[0]), "v0_dir": 1.0}
-    scale = max(abs(fd[k] * theta[k]) for k in names)
-    worst = 0.0
-    for k in names:
-        if abs(fd[k] * theta[k]) > 1e-6 * scale:
-            rel = abs(got[k] - fd[k]) / abs(fd[k])
-            kind = "relative error"
-        else:
-            rel = abs((got[k] - fd[k]) * theta[k]) / scale
-            kind = "vanishing derivative; error / largest scaled sensitivity"
-        worst = max(worst, rel)
-        print(f"c3 dL/d{k}: adjoint {got[k]:.6e} central difference {fd[k]:.6e} {kind} {rel:.2e}")
+    print(f"c3 loss {loss:.6e} (FP64 oracle {float(f['loss']):.6e}); stored tape: {tape.stored}; "
+          f"max |FP32 residual - FP64 residual| {res_diff:.2e} (residual max {float(r64.abs().max()):.2e})")
+    adj = _c3_errors(_c3_grads(tape.backward(g_x=2.0 * r64 / w.n), md, direction), fd, names, theta,
+                     "adjoint on the FP64 residual:")
+    e2e = _c3_errors(_c3_grads(tape.backward(g_x=2.0 * diff / w.n), md, direction), fd, names, theta,
+                     "on the GPU's own residual:")
     assert abs(loss - float(f["loss"])) <= 1e-2 * float(f["loss"])
-    assert worst <= GRAD_BAR
+    assert adj <= GRAD_BAR
+    assert e2e <= 1e-2
