@@ -21,8 +21,9 @@ the GPU tests in tests/test_gpu_fullsize.py compare against:
                    material (3e4, 0.35, 2e3) and the guess (1e4, 0.25, 1e3).
                    Central finite differences (h = 1e-3 relative) of the loss
                    in E, nu, yield stress and along a seeded direction of the
-                   initial velocities, and the FP64 residual x_T - x_T(target)
-                   of every particle.
+                   initial velocities, in the Lame parameters mu and lam
+                   separately (scaled by 1 +- h), and the FP64 residual
+                   x_T - x_T(target) of every particle.
 
 The workloads come from empm_b200.workloads (seeded numpy generators; no
 GPU is involved). The oracle keeps the colliders as the reference does, in
@@ -34,7 +35,7 @@ disagree. With float64 tests the FP32 and FP64 oracles drift apart by
 6e-7. Runtime on 8 host cores: about 12 min (c2), 12 min (c4)
 and 10 min (c3).
 
-    python tests/golden/make_fullsize.py [c2] [c4] [c3] [c3_residual]
+    python tests/golden/make_fullsize.py [c2] [c4] [c3] [c3_residual] [c3_lame]
 """
 from __future__ import annotations
 
@@ -121,11 +122,13 @@ def c3_direction(n: int) -> np.ndarray:
     return (np.random.default_rng(C3_DIR_SEED).standard_normal((n, 3)) * 0.05).astype(np.float32)
 
 
-def c3_final(w, E=None, nu=None, ys=None, v=None) -> np.ndarray:
+def c3_final(w, E=None, nu=None, ys=None, v=None, mu_scale=1.0, lam_scale=1.0) -> np.ndarray:
     sim = O.OracleSim(w.x, w.v if v is None else v, w.vol, w.rho.astype(np.float64) * w.vol,
                       w.E if E is None else E, w.nu if nu is None else nu, n_grid=w.G,
                       material=OS.MATERIAL_IDS[w.material], gravity=w.gravity,
                       yield_stress=w.ys if ys is None else ys, precision="fp64_omp", collider_f32=True)
+    sim.mu *= mu_scale
+    sim.lam *= lam_scale
     sim.colliders = OS.oracle_colliders(w.colliders)
     sim.rollout(w.dt, w.T)
     return sim.x
@@ -173,6 +176,26 @@ def make_c3(path: str) -> None:
                         loss_plus=np.array([lp[k] for k in names]), loss_minus=np.array([lm[k] for k in names]),
                         step=np.array([cases[k][0] for k in names]), loss=base, h=C3_H, dir_seed=C3_DIR_SEED,
                         residual=residual)
+    add_c3_lame(path)
+
+
+def add_c3_lame(path: str) -> None:
+    """Central differences of an existing c3 fixture's loss in the Lame
+    parameters separately (mu and lam scaled by 1 +- h): dL/dnu is a
+    difference of the two, which these resolve one at a time."""
+    w = W.c3()
+    tw = W.c3(guess=False)
+    ts = OS.sim_from_workload(tw, precision="fp64_omp", collider_f32=True)
+    ts.rollout(tw.dt, tw.T)
+    target = ts.x.copy()
+    old = dict(np.load(path))
+    for name in ("mu", "lam"):
+        kw = lambda sc: {f"{name}_scale": sc}  # noqa: E731
+        lp = c3_loss(w, target, **kw(1.0 + C3_H))
+        lm = c3_loss(w, target, **kw(1.0 - C3_H))
+        old[f"fd_log_{name}"] = np.float64((lp - lm) / (2.0 * C3_H))
+        print(f"c3 dL/dlog({name}) = {old[f'fd_log_{name}']:.9e}", flush=True)
+    np.savez_compressed(path, **old)
 
 
 def add_c3_residual(path: str) -> None:
@@ -191,7 +214,7 @@ def add_c3_residual(path: str) -> None:
 def main(argv) -> None:
     O.build()
     jobs = argv or ["c2", "c4", "c3"]
-    make = {"c2": make_c2, "c4": make_c4, "c3": make_c3, "c3_residual": add_c3_residual}
+    make = {"c2": make_c2, "c4": make_c4, "c3": make_c3, "c3_residual": add_c3_residual, "c3_lame": add_c3_lame}
     for j in jobs:
         make[j](os.path.join(HERE, f"fullsize_{j.split('_')[0]}.npz"))
 
