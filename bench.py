@@ -1370,7 +1370,7 @@ def main():
     ap.add_argument("--c5-rate", dest="c5_rate", type=float, default=20.0, help="c5: arrivals per second")
     ap.add_argument("--c5-seconds", dest="c5_seconds", type=float, default=60.0, help="c5: arrival window")
     ap.add_argument("--c5-budget-gb", dest="c5_budget_gb", type=float, default=60.0, help="c5: HBM budget")
-    ap.add_argument("--c5-plain", dest="c5_plain", type=int, default=12, help="c5: requests timed one at a time")
+    ap.add_argument("--c5-plain", dest="c5_plain", type=int, default=24, help="c5: requests timed one at a time")
     ap.add_argument("--c5-grad-fraction", dest="c5_grad_fraction", type=float, default=0.3,
                     help="c5: fraction of requests that also ask for a gradient")
     ap.add_argument("--checkpoint-every", dest="checkpoint_every", type=int, default=20,

@@ -35,6 +35,18 @@
 #ifndef EMPM_FUSED_MIN_CTAS
 #define EMPM_FUSED_MIN_CTAS 4
 #endif
+// 1: each warp of the fused kernel first copies the grid nodes its lanes'
+// stencils cover (their bounding box, at most EMPM_WARP_TILE_NODES nodes) into
+// shared memory and gathers from there; warps whose box is larger, leaves the
+// grid or spans two instances gather from global memory. Measured on the
+// population workload it is slower than gathering through L1 (648 us per
+// launch with 128-node boxes, 613 us with 192, against 595 us), so it is off.
+#ifndef EMPM_FUSED_WARP_TILE
+#define EMPM_FUSED_WARP_TILE 0
+#endif
+#ifndef EMPM_WARP_TILE_NODES
+#define EMPM_WARP_TILE_NODES 128
+#endif
 // 1: the fused kernel's G2P gathers with a run-time outer stencil loop
 // (population workload: 598 us per launch against 604 us fully unrolled; at 3
 // or 2 CTAs per SM 603-608 and 722 us)
@@ -435,6 +447,36 @@ struct GlobalFetch {
     }
 };
 
+// Node velocities from a warp's shared-memory copy of the nodes its lanes'
+// stencils cover: a box with origin o and extents e (tile index
+// ((i - o0) * e1 + (j - o1)) * e2 + (k - o2)). The outer axis may be a run-time
+// index (g2p_gather_rt), so its term is formed per call.
+struct WarpTileFetch {
+    const float4* tile;
+    int o0, o1, o2, e1, e2;
+    struct Bound {
+        const float4* tile;
+        int x0, e12;
+        int y[3], z[3];
+        __device__ __forceinline__ V3 operator()(int i, int j, int k) const {
+            const float4 g = tile[x0 + i * e12 + y[j] + z[k]];
+            return v3(g.x, g.y, g.z);
+        }
+    };
+    __device__ __forceinline__ Bound bind(const Stencil& st, bool) const {
+        Bound b;
+        b.tile = tile;
+        b.e12 = e1 * e2;
+        b.x0 = (st.b[0] - o0) * b.e12;
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            b.y[o] = (st.b[1] + o - o1) * e2;
+            b.z[o] = st.b[2] + o - o2;
+        }
+        return b;
+    }
+};
+
 __global__ void __launch_bounds__(128, EMPM_G2P_MIN_CTAS) k_g2p_direct(ParticleArrays P, F9Planes Fe, MaterialArrays M,
                                                     ParticleArrays out, Launch L, const float4* vel) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -683,19 +725,81 @@ __global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g(ParticleArra
     const StepConsts c = consts_of(L, inst);   // substep s: stress + P2G
     P2GParticle q;
     bool valid = false;
+    // which lanes run the G2P of substep s-1 (simulated, not held)
+    bool g_on = false;
+    float4 xm = make_float4(0.f, 0.f, 0.f, 0.f);
     if (p < L.n_total && !(M.sel && __ldg(M.sel + p) != 0)) {
-        const EmpmStep& sg = L.steps[(size_t)g2p_table * L.n_inst + inst];   // substep s-1: G2P
-        if (!sg.hold) {
+        g_on = !L.steps[(size_t)g2p_table * L.n_inst + inst].hold;
+        if (g_on) xm = __ldg(P.x + p);
+    }
+#if EMPM_FUSED_WARP_TILE
+    // the warp's stencil nodes into shared memory (all lanes take part)
+    __shared__ float4 s_tile[256 / 32][EMPM_WARP_TILE_NODES];
+    const int wlane = threadIdx.x & 31;
+    float4* wtile = s_tile[threadIdx.x >> 5];
+    int gb[3] = {0, 0, 0};
+    if (g_on) {
+        gb[0] = base_node(xm.x, c.inv_dx);
+        gb[1] = base_node(xm.y, c.inv_dx);
+        gb[2] = base_node(xm.z, c.inv_dx);
+    }
+    const unsigned g_lanes = __ballot_sync(0xffffffffu, g_on);
+    int box_o[3], box_e[3];
+    bool tiled = false;
+    if (g_lanes) {
+        int hi[3];
+#pragma unroll
+        for (int a3 = 0; a3 < 3; ++a3) {
+            box_o[a3] = __reduce_min_sync(0xffffffffu, g_on ? gb[a3] : INT_MAX);
+            hi[a3] = __reduce_max_sync(0xffffffffu, g_on ? gb[a3] : INT_MIN);
+            box_e[a3] = hi[a3] - box_o[a3] + 3;
+        }
+        const int imin = __reduce_min_sync(0xffffffffu, g_on ? inst : INT_MAX);
+        const int imax = __reduce_max_sync(0xffffffffu, g_on ? inst : INT_MIN);
+        const int leader = __ffs(g_lanes) - 1;
+        const int Gw = __shfl_sync(0xffffffffu, c.G, leader);
+        const int NBw = __shfl_sync(0xffffffffu, c.NB, leader);
+        const int boffw = __shfl_sync(0xffffffffu, c.boff, leader);
+        const int count = box_e[0] * box_e[1] * box_e[2];
+        tiled = imin == imax && count <= EMPM_WARP_TILE_NODES && box_o[0] >= 0 && box_o[1] >= 0 &&
+                box_o[2] >= 0 && hi[0] + 2 < Gw && hi[1] + 2 < Gw && hi[2] + 2 < Gw;
+        if (tiled) {
+            const int e12 = box_e[1] * box_e[2];
+            for (int t = wlane; t < count; t += 32) {
+                const int ti = t / e12, tr = t - ti * e12;
+                const int tj = tr / box_e[2], tk = tr - tj * box_e[2];
+                const int gi = box_o[0] + ti, gj = box_o[1] + tj, gk = box_o[2] + tk;
+                const long long addr = ((long long)(boffw + block_of(gi, gj, gk, NBw)) << 6) | ((gi & 3) << 4) |
+                                       ((gj & 3) << 2) | (gk & 3);
+                wtile[t] = __ldg(vel + addr);
+            }
+        }
+        __syncwarp();
+    }
+#endif
+    if (g_on) {
+        {
+            const EmpmStep& sg = L.steps[(size_t)g2p_table * L.n_inst + inst];   // substep s-1: G2P
             const float dt = sg.dt;
-            const float4 xm = __ldg(P.x + p);
             const V3 x = v3(xm.x, xm.y, xm.z);
             const Stencil st = make_stencil(x, c.inv_dx);
             const bool in_grid = stencil_in_grid(st, c.G);
+#if EMPM_FUSED_WARP_TILE
+            G2POut o;
+            if (tiled) {
+                const WarpTileFetch fetch{wtile, box_o[0], box_o[1], box_o[2], box_e[1], box_e[2]};
+                o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
+            } else {
+                const GlobalFetch fetch{vel, &c};
+                o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
+            }
+#else
             GlobalFetch fetch{vel, &c};
 #if EMPM_FUSED_G2P_LOOP
             const G2POut o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
 #else
             const G2POut o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
+#endif
 #endif
             const float dx = 1.f / c.inv_dx;   // as g2p_particle computes it
             const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
