@@ -294,6 +294,9 @@ struct AdjP2GArgs {
     float*         g_mass; // accumulated over substeps
 };
 
+// MAT: the material every instance of the launch uses (plasticine 5 and jelly
+// 0 have kernels of their own), or -1 (switch per instance).
+template <int MAT = -1>
 __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const AdjP2GArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.L.n_total) return;
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
     const M3 g_tau = (-vol * dt) * gSv;
 
     SpectralEval e;
-    spectral_eval(f9_load(a.P.F, p), __ldg(a.M.mu + p), __ldg(a.M.lam + p), __ldg(a.M.ys + p), dt, c.ms, e);
+    spectral_eval<MAT>(f9_load(a.P.F, p), __ldg(a.M.mu + p), __ldg(a.M.lam + p), __ldg(a.M.ys + p), dt, c.ms, e);
     {
         // sum_n H_n Sv^T gmv_n, component a = sum_b dot(column b of Sv, sum_n H_n[a][b] gmv_n)
         const M3 Sv = (-vol) * spectral_tau(e);

@@ -383,6 +383,63 @@ __global__ void __launch_bounds__(256) k_grid_update_list(const GridUpdateArgs a
     }
 }
 
+// Grid update over the listed blocks, one warp per block and two nodes per
+// lane (grid-stride over the list): the block id, its instance, the instance
+// constants and the step table are read once per warp, where
+// k_grid_update_list reads them once per node.
+template <bool kKeep>
+__global__ void __launch_bounds__(256) k_grid_update_warps(const GridUpdateArgs a, const int* active) {
+    const int count = __ldg(active);
+    if (a.store && blockIdx.x == 0 && threadIdx.x == 0) {
+        a.store_list[0] = count;
+        if (a.max_count) atomicMax(a.max_count, count);
+    }
+    const bool save = a.store && count <= a.store_cap;
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long slot = warp; slot < count; slot += nwarps) {
+        const int b = __ldg(active + 1 + slot);
+        const int inst = __ldg(active + 1 + a.L.nblocks + slot);
+        const InstanceConsts* I = a.L.inst + inst;
+        const EmpmStep& st = a.L.steps[(size_t)a.L.table * a.L.n_inst + inst];
+        const V3 g = v3(__ldg(&I->g[0]), __ldg(&I->g[1]), __ldg(&I->g[2]));
+        const float damping = __ldg(&I->damping);
+        const float dt = st.dt;
+        const int n_coll = st.n_colliders;
+        const int G = __ldg(&I->G), NB = __ldg(&I->NB), boff = __ldg(&I->boff);
+        const float dx = __ldg(&I->dx);
+        const long long base = (long long)b << 6;
+        const float4 m0 = a.mom[base + lane];
+        const float4 m1 = a.mom[base + lane + 32];
+        if (!kKeep) {
+            a.mom[base + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+            a.mom[base + lane + 32] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int in_block = lane + 32 * h;
+            const float4 m = h ? m1 : m0;
+            V3 v = grid_velocity(m, dt, g, damping);
+            if (n_coll > 0) {
+                int i, j, k;
+                node_coords(((long long)(b - boff) << 6) | in_block, NB, i, j, k);
+                if (i < G && j < G && k < G) {
+                    const long long dense = ((long long)i * G + j) * G + k;
+                    apply_colliders(st, i, j, k, G, dx, dense, v);
+                }
+            }
+            const float4 v4 = make_float4(v.x, v.y, v.z, m.w);
+            a.vel[base + in_block] = v4;
+            if (save) {
+                a.store[slot * 128 + in_block] = m;
+                a.store[slot * 128 + 64 + in_block] = v4;
+            }
+        }
+        if (save && lane == 0) a.store_list[1 + slot] = b;
+    }
+}
+
 // -------------------------------------------------------------------------
 // G2P (shared by both paths through the fetch functor)
 // -------------------------------------------------------------------------

@@ -129,10 +129,13 @@ EMPM_HD void spectral_viscoplastic(T s[3], const T& mu, const T& ys, float dt, c
     for (int a = 0; a < 3; ++a) s[a] = sexp(i2mu * (r * st[a]) + tr / 3.f);
 }
 
-template <class T>
+// MAT >= 0 compiles the map for that material alone (a batch whose instances
+// all use it); -1 switches on ms.material.
+template <class T, int MAT = -1>
 EMPM_HD SpectralOut<T> spectral_map(const T s_in[3], T mu, T lam, T ys, float dt, const MaterialScalars& ms) {
     T s[3] = {s_in[0], s_in[1], s_in[2]};
-    switch (ms.material) {
+    const int material = MAT >= 0 ? MAT : ms.material;
+    switch (material) {
         case 1: spectral_von_mises(s, mu, lam, ys, ms, false); break;
         case 2: spectral_sand(s, mu, lam, ms); break;
         case 3: spectral_viscoplastic(s, mu, ys, dt, ms); break;
@@ -143,7 +146,7 @@ EMPM_HD SpectralOut<T> spectral_map(const T s_in[3], T mu, T lam, T ys, float dt
 #pragma unroll
     for (int a = 0; a < 3; ++a) { o.f[a] = s[a]; o.h[a] = sconst(s[a], 0.f); }
     const T J = s[0] * s[1] * s[2];
-    switch (ms.material) {
+    switch (material) {
         case 0:
         case 5: {  // fixed-corotated: 2 mu (F - R) F^T + lam J (J - 1) I
             const T vol = lam * J * (J - 1.f);
@@ -198,13 +201,14 @@ struct SpectralEval {
     SpectralOut<D6> o;
 };
 
+template <int MAT = -1>
 EMPM_HD void spectral_eval(const M3& Ft, float mu, float lam, float ys, float dt, const MaterialScalars& ms,
                            SpectralEval& e) {
     V3 sv;
     svd3(Ft, e.U, sv, e.V);
     e.s[0] = sv.x; e.s[1] = sv.y; e.s[2] = sv.z;
     const D6 s[3] = {dseed<6>(sv.x, 0), dseed<6>(sv.y, 1), dseed<6>(sv.z, 2)};
-    e.o = spectral_map<D6>(s, dseed<6>(mu, 3), dseed<6>(lam, 4), dseed<6>(ys, 5), dt, ms);
+    e.o = spectral_map<D6, MAT>(s, dseed<6>(mu, 3), dseed<6>(lam, 4), dseed<6>(ys, 5), dt, ms);
 }
 
 // tau = U diag(h) U^T

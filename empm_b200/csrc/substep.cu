@@ -553,6 +553,12 @@ static ParticleArrays particle_arrays(float* base, int n) {
 // otherwise run on a fraction of the SMs; measured 16.7 -> 15.0 us for 20k
 // particles; G2P measured no better). The kernels use no block-wide
 // synchronisation, so any multiple of the warp size works.
+// 1: the grid update runs one warp per touched block (k_grid_update_warps),
+// 0: one thread per node (k_grid_update_list)
+#ifndef EMPM_GRID_UPDATE_WARPS
+#define EMPM_GRID_UPDATE_WARPS 1
+#endif
+
 static int particle_threads(const EmpmCtx* ctx, long long n, int usual) {
     return blocks_for(n, usual) >= 2LL * ctx->sm_count ? usual : 64;
 }
@@ -592,7 +598,11 @@ static int launch_grid_update_list(EmpmCtx* ctx, const Launch& L, cudaStream_t s
     k_collect_blocks<kKeep><<<blocks_for(ctx->nblocks, 256), 256, 0, stream>>>(ctx->flags, (int)ctx->nblocks,
                                                                                ctx->active, L);
     CK(cudaGetLastError(), "k_collect_blocks");
+#if EMPM_GRID_UPDATE_WARPS
+    k_grid_update_warps<kKeep><<<ctx->sm_count * 8, 256, 0, stream>>>(g, ctx->active);
+#else
     k_grid_update_list<kKeep><<<ctx->sm_count * 8, 256, 0, stream>>>(g, ctx->active);
+#endif
     CK(cudaGetLastError(), "k_grid_update_list");
     return EMPM_OK;
 }
@@ -1520,7 +1530,11 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         ap.g_ys = gm_ys;
         ap.g_mass = gm_mass;
         timing_mark(ctx, 5, 0, s);
-        k_adj_p2g<<<blocks_for(n, 128), 128, 0, s>>>(ap);
+        switch (uniform_material(ctx)) {
+            case 5: k_adj_p2g<5><<<blocks_for(n, 128), 128, 0, s>>>(ap); break;
+            case 0: k_adj_p2g<0><<<blocks_for(n, 128), 128, 0, s>>>(ap); break;
+            default: k_adj_p2g<-1><<<blocks_for(n, 128), 128, 0, s>>>(ap); break;
+        }
         timing_mark(ctx, 5, 1, s);
         CK(cudaGetLastError(), "k_adj_p2g");
     }
