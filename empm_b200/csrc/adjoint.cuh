@@ -27,9 +27,12 @@
 #include "spectral.cuh"
 
 // Minimum resident CTAs (of 128 threads) per SM asked of the compiler for the
-// two particle kernels of the adjoint.
+// two particle kernels of the adjoint. The one-pass G2P adjoint keeps 33
+// accumulators live across its stencil loop: at 4 CTAs (128 registers) it
+// spills 12 B and took 45.2 us per 200k-particle substep, at 5 CTAs (96
+// registers, 140 B spilled) 53.5 us, at 6 (80 registers, 244 B) 48.8 us.
 #ifndef EMPM_ADJ_G2P_MIN_CTAS
-#define EMPM_ADJ_G2P_MIN_CTAS 6
+#define EMPM_ADJ_G2P_MIN_CTAS 4
 #endif
 // 1: the G2P adjoint's scatter loops over the outer stencil axis at run time
 #ifndef EMPM_ADJ_G2P_ROLL
@@ -64,6 +67,7 @@ EMPM_HD V3 weight_hessian_times(const Stencil& st, int i, int j, int k, V3 b) {
 // ---------------------------------------------------------------------------
 struct AdjG2PArgs {
     ParticleArrays P;      // state of substep k (x)
+    const float4*  x_next; // x after substep k (written by its G2P)
     F9Planes       Fe;     // elastic F of substep k
     MaterialArrays M;      // selection
     ParticleArrays Gn;     // adjoint of the state after substep k
@@ -75,6 +79,16 @@ struct AdjG2PArgs {
     int            seg_cap;  // longest same-cell run summed with shuffles (a power of two)
 };
 
+// One pass over the stencil. Per node n (weight w, weight gradient dw, node
+// velocity vg) with q_n = gv' + dt gx'_clamped + 4 inv_dx gC' (o_n - fx):
+//   scatter   w q_n + gGv dw                       (gGv = dt gF' F_e^T)
+//   x adjoint dot(vg, q_n) dw + inv_dx^2 H_n gGv^T vg
+// and the forward's v' = sum w vg and grad v' = sum vg (x) dw, needed for the
+// x and F_elastic adjoints, are summed in the same pass. Every sum factorises
+// over the inner stencil axis (per row (i, j) the three nodes are combined
+// with wz_k, dwz_k, (1, -2, 1) and k wz_k); the Hessian term is kept as its
+// six moments sum_n H_n[pair] vg_n and contracted with gGv after the loop.
+//
 // Lanes whose particles share an instance and base cell (contiguous in cell
 // order) sum their node-velocity adjoints with shuffles; the segment head
 // issues one reduction per node, as k_p2g_warpagg does for the momentum.
@@ -91,14 +105,6 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     const V3 x = v3(xm.x, xm.y, xm.z);
     const Stencil st = make_stencil(x, valid ? c.inv_dx : 1.f);
     const bool in_grid = valid && stencil_in_grid(st, c.G);
-    G2POut o;
-    o.v = v3(0.f, 0.f, 0.f);
-    o.C = m3_zero();
-    o.gradv = m3_zero();
-    if (valid) {
-        const GlobalFetch fetch{a.vel, &c};
-        o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
-    }
     // segments of lanes with the same validity, instance and base cell
     const int b0 = valid ? st.b[0] : lane, b1 = valid ? st.b[1] : -1, b2 = valid ? st.b[2] : -1;
     const int u0 = __shfl_up_sync(0xffffffffu, b0, 1), u1 = __shfl_up_sync(0xffffffffu, b1, 1),
@@ -119,30 +125,42 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     const unsigned take = (lane + 1 <= end ? 1u : 0u) | (lane + 2 <= end ? 2u : 0u) | (lane + 4 <= end ? 4u : 0u) |
                           (lane + 8 <= end ? 8u : 0u) | (lane + 16 <= end ? 16u : 0u);
 
-    // x' = clamp(x + dt v'): the clamp passes the adjoint only strictly inside the band
+    // x' = clamp(x + dt v'): the clamp passes the adjoint only strictly inside
+    // the band. x + dt v' lies strictly inside it exactly when the clamped x'
+    // that the forward G2P wrote does (a value clamped to a bound is not).
     const float dx = 1.f / c.inv_dx;
     const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
-    const V3 y = x + dt * o.v;
+    const float4 xn = valid ? __ldg(a.x_next + p) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 gx4 = valid ? __ldg(a.Gn.x + p) : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 gv4 = valid ? __ldg(a.Gn.v + p) : make_float4(0.f, 0.f, 0.f, 0.f);
-    const V3 gxu = v3(y.x > lo && y.x < hi ? gx4.x : 0.f, y.y > lo && y.y < hi ? gx4.y : 0.f,
-                      y.z > lo && y.z < hi ? gx4.z : 0.f);
-    const V3 gvt = v3(gv4.x, gv4.y, gv4.z) + dt * gxu;
-    const M3 gC = valid ? f9_load(a.Gn.C, p) : m3_zero();
-    const M3 gF = valid ? f9_load(a.Gn.F, p) : m3_zero();
-    // F' = (I + dt grad v) F_e
-    const M3 Fe = valid ? f9_load(a.Fe, p) : m3_zero();
-    const M3 gGv = dt * (gF * transpose(Fe));
-    const M3 gFe = transpose(m3_identity() + dt * o.gradv) * gF;
-
-    // per node: q = gvt + 4 inv_dx gC (o - fx); node velocity adjoint w q + gGv dweight
-    const float c4 = 4.f * c.inv_dx;
-    const float idx2 = c.inv_dx * c.inv_dx;
-    const V3 fx = v3(st.fx[0], st.fx[1], st.fx[2]);
-    const V3 q0 = gvt - c4 * (gC * fx);
-    const V3 Q0 = c4 * col(gC, 0), Q1 = c4 * col(gC, 1), Q2 = c4 * col(gC, 2);
-    V3 gxa = gxu - (c4 * c.inv_dx) * (transpose(gC) * o.v);
-    const M3 gGvT = transpose(gGv);
+    const V3 gxu = v3(xn.x > lo && xn.x < hi ? gx4.x : 0.f, xn.y > lo && xn.y < hi ? gx4.y : 0.f,
+                      xn.z > lo && xn.z < hi ? gx4.z : 0.f);
+    // q_n = q0 + i Q0 + j Q1 + k Q2 with Q_c = 4 inv_dx gC'[:, c]; G_c = inv_dx gGv[:, c]
+    V3 q0, Q0, Q1, Q2, G0, G1, G2;
+    {
+        const V3 gvt = v3(gv4.x, gv4.y, gv4.z) + dt * gxu;
+        const M3 gC = valid ? f9_load(a.Gn.C, p) : m3_zero();
+        const float c4 = 4.f * c.inv_dx;
+        q0 = gvt - c4 * (gC * v3(st.fx[0], st.fx[1], st.fx[2]));
+        Q0 = c4 * col(gC, 0);
+        Q1 = c4 * col(gC, 1);
+        Q2 = c4 * col(gC, 2);
+        // F' = (I + dt grad v) F_e: gGv = dt gF' F_e^T
+        const M3 gF = valid ? f9_load(a.Gn.F, p) : m3_zero();
+        const M3 gGv = (dt * c.inv_dx) * (gF * transpose(valid ? f9_load(a.Fe, p) : m3_zero()));
+        G0 = col(gGv, 0);
+        G1 = col(gGv, 1);
+        G2 = col(gGv, 2);
+    }
+    const float wz0 = st.w[2][0], wz1 = st.w[2][1], wz2 = st.w[2][2], kz2 = 2.f * wz2;
+    const float uz0 = st.dw[2][0], uz1 = st.dw[2][1], uz2 = st.dw[2][2];
+    const V3 zero = v3(0.f, 0.f, 0.f);
+    V3 Vs = zero;                      // sum w vg (the forward's v')
+    V3 D0 = zero, D1 = zero, D2 = zero;   // columns of sum vg (x) dweight / inv_dx
+    V3 X3 = zero;                      // sum dot(vg, q) dweight / inv_dx
+    V3 Hv[6];                          // sum H[pair] vg, pairs xx, yy, zz, xy, xz, yz (grid units)
+#pragma unroll
+    for (int r = 0; r < 6; ++r) Hv[r] = zero;
 #if EMPM_ADJ_G2P_ROLL
 #pragma unroll 1
 #else
@@ -151,27 +169,39 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     for (int i = 0; i < 3; ++i) {
         const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
         const float ux = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        const float hx = bspline_d2(i);
         const V3 qi = q0 + (float)i * Q0;
+        V3 Vi = zero;
 #pragma unroll
-        for (int j = 0; j < 3; ++j)
+        for (int j = 0; j < 3; ++j) {
+            const float wy = st.w[1][j], uy = st.dw[1][j];
+            const float wxy = wx * wy, dxy = ux * wy, xdy = wx * uy;
+            const V3 qij = j == 0 ? qi : qi + (float)j * Q1;
+            // scatter value of node k: wz_k P + k wz_k Qr + dwz_k R
+            const V3 P = wxy * qij + dxy * G0 + xdy * G1;
+            const V3 Qr = wxy * Q2;
+            const V3 R = wxy * G2;
+            V3 vg[3];
+            float sk[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
                 const bool node_ok = valid && (in_grid || (ix >= 0 && iy >= 0 && iz >= 0 && ix < c.G && iy < c.G &&
                                                            iz < c.G));
                 const long long addr = node_ok ? gaddr(c, ix, iy, iz) : 0;
-                V3 gvg = v3(0.f, 0.f, 0.f);
+                vg[k] = zero;
                 if (node_ok) {
                     const float4 g4 = __ldg(a.vel + addr);
-                    const V3 vg = v3(g4.x, g4.y, g4.z);
-                    const float wy = st.w[1][j], wz = st.w[2][k];
-                    const float uy = st.dw[1][j], uz = st.dw[2][k];
-                    const float w = wx * wy * wz;
-                    const V3 dw = c.inv_dx * v3(ux * wy * wz, wx * uy * wz, wx * wy * uz);
-                    const V3 q = qi + (float)j * Q1 + (float)k * Q2;
-                    gvg = w * q + gGv * dw;
-                    gxa = gxa + dot(vg, q) * dw + idx2 * weight_hessian_times(st, i, j, k, gGvT * vg);
+                    vg[k] = v3(g4.x, g4.y, g4.z);
                 }
+                const float wz = k == 0 ? wz0 : (k == 1 ? wz1 : wz2);
+                const float uz = k == 0 ? uz0 : (k == 1 ? uz1 : uz2);
+                V3 gvg = wz * P + uz * R;
+                if (k == 1) gvg = gvg + wz1 * Qr;
+                if (k == 2) gvg = gvg + kz2 * Qr;
+                if (!node_ok) gvg = zero;
+                sk[k] = dot(vg[k], qij);
+                if (k) sk[k] += (float)k * dot(vg[k], Q2);
                 // reduction rounds unrolled, each skipped by a warp-uniform branch
 #pragma unroll
                 for (int r = 0; r < 5; ++r) {
@@ -185,11 +215,46 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
                 }
                 if (head && node_ok) red_add_v4(a.gacc + addr, make_float4(gvg.x, gvg.y, gvg.z, 0.f));
             }
+            const V3 T0 = wz0 * vg[0] + wz1 * vg[1] + wz2 * vg[2];
+            const V3 T1 = uz0 * vg[0] + uz1 * vg[1] + uz2 * vg[2];
+            const V3 T2 = vg[0] - 2.f * vg[1] + vg[2];
+            const float sg0 = wz0 * sk[0] + wz1 * sk[1] + wz2 * sk[2];
+            const float sg1 = uz0 * sk[0] + uz1 * sk[1] + uz2 * sk[2];
+            Vi = Vi + wxy * T0;
+            D0 = D0 + dxy * T0;
+            D1 = D1 + xdy * T0;
+            D2 = D2 + wxy * T1;
+            X3 = X3 + v3(dxy * sg0, xdy * sg0, wxy * sg1);
+            Hv[0] = Hv[0] + (hx * wy) * T0;
+            Hv[1] = Hv[1] + (wx * bspline_d2(j)) * T0;
+            Hv[2] = Hv[2] + wxy * T2;
+            Hv[3] = Hv[3] + (ux * uy) * T0;
+            Hv[4] = Hv[4] + dxy * T1;
+            Hv[5] = Hv[5] + xdy * T1;
+        }
+        Vs = Vs + Vi;
     }
-    if (live) {
-        a.gx[p] = make_float4(gxa.x, gxa.y, gxa.z, 0.f);
-        f9_store(a.gFe, p, gFe);
+    if (!live) return;
+    // F' = (I + dt grad v) F_e  ->  gF_e = (I + dt grad v)^T gF' (gF' read again rather than kept live)
+    M3 A;   // I + dt grad v, grad v = inv_dx [D0 | D1 | D2] (columns)
+    {
+        const V3 dc[3] = {D0, D1, D2};
+        const float s = dt * c.inv_dx;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int cl = 0; cl < 3; ++cl) A.m[3 * r + cl] = (r == cl ? 1.f : 0.f) + s * comp(dc[cl], r);
     }
+    f9_store(a.gFe, p, transpose(A) * (valid ? f9_load(a.Gn.F, p) : m3_zero()));
+    // sum_n H_n gGv^T vg_n, component a = sum_b dot(column b of gGv, sum_n H_n[a][b] vg_n); with G = inv_dx gGv
+    // the term inv_dx^2 (...) is inv_dx (...) in G. The forward's C' = 4 inv_dx (...) enters the x
+    // adjoint as -4 inv_dx^2 gC'^T v' = -inv_dx (dot(Q_c, v'))_c.
+    const V3 hS = v3(dot(G0, Hv[0]) + dot(G1, Hv[3]) + dot(G2, Hv[4]),
+                     dot(G0, Hv[3]) + dot(G1, Hv[1]) + dot(G2, Hv[5]),
+                     dot(G0, Hv[4]) + dot(G1, Hv[5]) + dot(G2, Hv[2]));
+    const V3 QV = v3(dot(Q0, Vs), dot(Q1, Vs), dot(Q2, Vs));
+    const V3 gxa = gxu + c.inv_dx * (X3 + hS - QV);
+    a.gx[p] = make_float4(gxa.x, gxa.y, gxa.z, 0.f);
 }
 
 // ---------------------------------------------------------------------------
@@ -327,15 +392,24 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
     const bool in_grid = stencil_in_grid(st, c.G);
     const float dx = c.dx;
     const float idx2 = c.inv_dx * c.inv_dx;
-    V3 Wg = v3(0.f, 0.f, 0.f);      // sum w gmv
-    M3 gCd = m3_zero();             // sum w gmv (x) dpos
-    M3 gSv = m3_zero();             // sum gmv (x) dweight
+    // Every sum of the gather factorises over the inner stencil axis: per row
+    // (i, j) the three nodes are combined with the weights wz_k, dwz_k, the
+    // second derivatives (1, -2, 1) and k wz_k, then the rows are summed with
+    // weights in x and y. v + Cd dpos at node (i, j, k) is e_ij + k c2 with
+    // c2 = dx Cd[:, 2], so s_k = gm_k + dot(gmv_k, e_ij) + k dot(gmv_k, c2).
+    const V3 zero = v3(0.f, 0.f, 0.f);
+    V3 Wg = zero, Im = zero, Jm = zero, Km = zero;   // sum w gmv, and its moments in i, j, k
+    V3 S0 = zero, S1 = zero, S2 = zero;              // columns of sum gmv (x) dweight / inv_dx
+    V3 X3 = zero;                                    // sum s dweight / inv_dx
     float gmass = 0.f;
-    V3 gxa = v3(0.f, 0.f, 0.f);
     V3 Hg[6];                       // sum H[pair] gmv, pairs xx, yy, zz, xy, xz, yz (grid units)
 #pragma unroll
-    for (int r = 0; r < 6; ++r) Hg[r] = v3(0.f, 0.f, 0.f);
+    for (int r = 0; r < 6; ++r) Hg[r] = zero;
     const StencilAddr sa = stencil_addr(c.boff, c.NB, st.b);
+    const V3 Cd0 = col(Cd, 0), Cd1 = col(Cd, 1), c2 = dx * col(Cd, 2);
+    const V3 e0 = v - st.fx[2] * c2;
+    const float wz0 = st.w[2][0], wz1 = st.w[2][1], wz2 = st.w[2][2], kz2 = 2.f * wz2;
+    const float uz0 = st.dw[2][0], uz1 = st.dw[2][1], uz2 = st.dw[2][2];
 #if EMPM_ADJ_P2G_ROLL
 #pragma unroll 1
 #else
@@ -345,34 +419,62 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
         const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
         const float ux = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
         const float hx = bspline_d2(i);
-        const float px = ((float)i - st.fx[0]) * dx;
+        const V3 ei = e0 + (((float)i - st.fx[0]) * dx) * Cd0;
+        V3 Wi = zero;
 #pragma unroll
-        for (int j = 0; j < 3; ++j)
+        for (int j = 0; j < 3; ++j) {
+            float4 g[3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                if (!in_grid && !node_in_grid(st.b, i, j, k, c.G)) continue;
-                const float4 g4 = __ldg(a.gmom + sa.at(i, j, k));
-                const V3 gmv = v3(g4.x, g4.y, g4.z);
-                const float wy = st.w[1][j], wz = st.w[2][k];
-                const float uy = st.dw[1][j], uz = st.dw[2][k];
-                const float w = wx * wy * wz;
-                const V3 dw = c.inv_dx * v3(ux * wy * wz, wx * uy * wz, wx * wy * uz);
-                const V3 dpos = v3(px, ((float)j - st.fx[1]) * dx, ((float)k - st.fx[2]) * dx);
-                const float s = g4.w + dot(gmv, v + Cd * dpos);
-                gmass += w * s;
-                Wg = Wg + w * gmv;
-                gCd = gCd + outer(w * gmv, dpos);
-                gSv = gSv + outer(gmv, dw);
-                gxa = gxa + (mass * s) * dw;
-                Hg[0] = Hg[0] + (hx * wy * wz) * gmv;
-                Hg[1] = Hg[1] + (wx * bspline_d2(j) * wz) * gmv;
-                Hg[2] = Hg[2] + (wx * wy * bspline_d2(k)) * gmv;
-                Hg[3] = Hg[3] + (ux * uy * wz) * gmv;
-                Hg[4] = Hg[4] + (ux * wy * uz) * gmv;
-                Hg[5] = Hg[5] + (wx * uy * uz) * gmv;
+            for (int k = 0; k < 3; ++k)
+                g[k] = (in_grid || node_in_grid(st.b, i, j, k, c.G)) ? __ldg(a.gmom + sa.at(i, j, k))
+                                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+            const V3 g0 = v3(g[0].x, g[0].y, g[0].z), g1 = v3(g[1].x, g[1].y, g[1].z),
+                     g2 = v3(g[2].x, g[2].y, g[2].z);
+            const V3 eij = ei + (((float)j - st.fx[1]) * dx) * Cd1;
+            const float s0 = g[0].w + dot(g0, eij);
+            const float s1 = g[1].w + dot(g1, eij) + dot(g1, c2);
+            const float s2 = g[2].w + dot(g2, eij) + 2.f * dot(g2, c2);
+            const V3 T0 = wz0 * g0 + wz1 * g1 + wz2 * g2;
+            const V3 T1 = uz0 * g0 + uz1 * g1 + uz2 * g2;
+            const V3 T2 = g0 - 2.f * g1 + g2;
+            const V3 Tk = wz1 * g1 + kz2 * g2;
+            const float sg0 = wz0 * s0 + wz1 * s1 + wz2 * s2;
+            const float sg1 = uz0 * s0 + uz1 * s1 + uz2 * s2;
+            const float wy = st.w[1][j], uy = st.dw[1][j];
+            const float wxy = wx * wy, dxy = ux * wy, xdy = wx * uy;
+            gmass += wxy * sg0;
+            const V3 Wr = wxy * T0;
+            Wi = Wi + Wr;
+            if (j) Jm = Jm + (float)j * Wr;
+            Km = Km + wxy * Tk;
+            S0 = S0 + dxy * T0;
+            S1 = S1 + xdy * T0;
+            S2 = S2 + wxy * T1;
+            X3 = X3 + v3(dxy * sg0, xdy * sg0, wxy * sg1);
+            Hg[0] = Hg[0] + (hx * wy) * T0;
+            Hg[1] = Hg[1] + (wx * bspline_d2(j)) * T0;
+            Hg[2] = Hg[2] + wxy * T2;
+            Hg[3] = Hg[3] + (ux * uy) * T0;
+            Hg[4] = Hg[4] + dxy * T1;
+            Hg[5] = Hg[5] + xdy * T1;
+        }
+        Wg = Wg + Wi;
+        Im = Im + (float)i * Wi;
+    }
+    // sum (w gmv) (x) dpos, columns dx (moment - fx Wg); sum gmv (x) dweight, columns inv_dx S
+    M3 gCd, gSv;
+    {
+        const V3 cc[3] = {dx * (Im - st.fx[0] * Wg), dx * (Jm - st.fx[1] * Wg), dx * (Km - st.fx[2] * Wg)};
+        const V3 sc[3] = {c.inv_dx * S0, c.inv_dx * S1, c.inv_dx * S2};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int cl = 0; cl < 3; ++cl) {
+                gCd.m[3 * r + cl] = comp(cc[cl], r);
+                gSv.m[3 * r + cl] = comp(sc[cl], r);
             }
     }
-    gxa = gxa - mass * (transpose(Cd) * Wg);
+    V3 gxa = (mass * c.inv_dx) * X3 - mass * (transpose(Cd) * Wg);
 
     V3 gv = mass * Wg;
     {

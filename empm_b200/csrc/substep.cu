@@ -1490,6 +1490,7 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         }
         AdjG2PArgs ag;
         ag.P = Pk;
+        ag.x_next = particle_arrays(d.states + (size_t)(k + 1) * state_floats, n).x;
         ag.Fe = Fk;
         ag.M = Mw;
         ag.Gn = Gp;

@@ -285,11 +285,20 @@ EMPM_HD P2GPre p2g_pre(const P2GParticle& q, float dx, float inv_dx, float dt) {
 }
 
 // Calls emit(i, j, k, contribution) for the 27 stencil nodes in (i, j, k) order.
+//
+// The contribution of node (i, j, k) factorises over the inner axis:
+//   wz_k P_ij + (k wz_k) Q_ij + dwz_k R_ij,   mass wz_k (m wx wy),
+// with P_ij = m wx wy (a + i B0 + j B1) + dwx wy S0 + wx dwy S1,
+// Q_ij = m wx wy B2 and R_ij = wx wy S2, formed once per stencil row: about
+// 10 flops per node instead of 20.
 template <typename Emit>
 __device__ __forceinline__ void p2g_emit(const P2GPre& p, Emit emit) {
     const Stencil& st = p.st;
     const V3 B0 = col(p.B, 0), B1 = col(p.B, 1), B2 = col(p.B, 2);
     const V3 S0 = col(p.S, 0), S1 = col(p.S, 1), S2 = col(p.S, 2);
+    const float wz0 = st.w[2][0], wz1 = st.w[2][1], wz2 = st.w[2][2];
+    const float kz2 = 2.f * wz2;
+    const float uz0 = st.dw[2][0], uz1 = st.dw[2][1], uz2 = st.dw[2][2];
     // the outer axis is a loop (weights picked by selects): a third of the
     // code of the fully unrolled 27 nodes, for the instruction cache (a loop
     // over the middle axis as well measured slower)
@@ -300,17 +309,18 @@ __device__ __forceinline__ void p2g_emit(const P2GPre& p, Emit emit) {
         const float dwx = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const V3 aij = ai + (float)j * B1;
+            const V3 aij = j == 0 ? ai : ai + (float)j * B1;
             const float wxy = wx * st.w[1][j], dxy = dwx * st.w[1][j], xdy = wx * st.dw[1][j];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const V3 aijk = aij + (float)k * B2;
-                const float wz = st.w[2][k];
-                const float wm = (wxy * wz) * p.m;
-                const float f0 = dxy * wz, f1 = xdy * wz, f2 = wxy * st.dw[2][k];
-                const V3 c = wm * aijk + f0 * S0 + f1 * S1 + f2 * S2;
-                emit(i, j, k, make_float4(c.x, c.y, c.z, wm));
-            }
+            const float mw = wxy * p.m;
+            const V3 P = mw * aij + dxy * S0 + xdy * S1;
+            const V3 Q = mw * B2;
+            const V3 R = wxy * S2;
+            const V3 c0 = wz0 * P + uz0 * R;
+            emit(i, j, 0, make_float4(c0.x, c0.y, c0.z, wz0 * mw));
+            const V3 c1 = wz1 * (P + Q) + uz1 * R;
+            emit(i, j, 1, make_float4(c1.x, c1.y, c1.z, wz1 * mw));
+            const V3 c2 = wz2 * P + kz2 * Q + uz2 * R;
+            emit(i, j, 2, make_float4(c2.x, c2.y, c2.z, wz2 * mw));
         }
     }
 }
