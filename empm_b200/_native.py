@@ -23,6 +23,7 @@ SHAPE_CUBE, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_HALFSPACE = 1, 2, 3, 4
 GATE_OFF, GATE_APPLY, GATE_ZERO_ALL = 0, 1, 2
 OPT_SORT_EVERY, OPT_P2G_MODE, OPT_G2P_TILE, OPT_TILE_CAP, OPT_SEG_CAP, OPT_ADJ_STORE = 1, 2, 3, 4, 5, 6
 OPT_FUSE = 7
+OPT_SEGMENT_GRAPH = 8
 MOD_IMPULSE, MOD_IMPULSE_MASK, MOD_SET_VELOCITY, MOD_ROTATION, MOD_MOVER = 1, 2, 3, 4, 5
 MOD_SET_VELOCITY_LAYERED = 6
 

@@ -24,6 +24,16 @@ struct GraphKey {
     int           start_pc, start_mc, start_since;   // sorted state a resumed sequence starts in
 };
 
+// What a segment's captured substep loop depends on besides the segment's
+// own buffers: the context epoch and options, and the caller's buffers where
+// the loop works on them directly (unsorted segments).
+struct SegGraphKey {
+    unsigned long long epoch;
+    unsigned long long params_version;
+    int                seg_cap, p2g_mode, sort_every, n;
+    const void*        buf[8];
+};
+
 // One captured rollout launch sequence and the sorted state it ends in.
 struct GraphEntry {
     GraphKey        key{};
@@ -116,6 +126,10 @@ struct EmpmCtx {
     static constexpr int kGraphs = 16;     // cached rollout graphs (LRU)
     GraphEntry   graphs[kGraphs];
     unsigned long long graph_clock = 0;
+    // bumped whenever captured launch sequences stop matching the context
+    // (options, instance tables, reallocated buffers): segment graphs compare it
+    unsigned long long epoch = 1;
+    int          segment_graph = 1;        // stored segments replay their substeps from a CUDA graph
     // the sorted state the last rollout ended in, which EMPM_ROLLOUT_RESUME
     // continues from: particle / material buffer and substeps since its sort
     bool         resident = false;
@@ -165,6 +179,12 @@ struct EmpmSegment {
     int*     pid = nullptr;       // [np] caller index of each position (cell order)
     int*     max_count = nullptr; // device: largest touched-block count of the forward pass
     std::vector<EmpmStep> tables;
+    EmpmStep* d_tables = nullptr; // device copy of tables, read by the segment's kernels
+    bool     tables_on_device = false;
+    // the substep loops of the forward and reverse passes, captured once and
+    // replayed while the key (context epoch, options, buffers) still matches
+    SegGraphKey     fwd_key{}, rev_key{};
+    cudaGraphExec_t fwd_exec = nullptr, rev_exec = nullptr;
 };
 
 int empm_set_error(EmpmCtx* ctx, int code, const char* fmt, ...);

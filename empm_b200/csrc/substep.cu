@@ -171,6 +171,7 @@ static InstanceConsts instance_consts(const EmpmModelParams& P, int n, int poff,
 // tables, step-table storage): recapture on next use.
 static void invalidate_graphs(EmpmCtx* ctx) {
     for (GraphEntry& g : ctx->graphs) g.valid = false;
+    ctx->epoch++;
 }
 
 static void destroy_graphs(EmpmCtx* ctx) {
@@ -179,6 +180,7 @@ static void destroy_graphs(EmpmCtx* ctx) {
         g.exec = nullptr;
         g.valid = false;
     }
+    ctx->epoch++;
 }
 
 static int upload_instances(EmpmCtx* ctx) {
@@ -307,6 +309,7 @@ extern "C" int empm_ctx_set_option(EmpmCtx* ctx, int option, int value) {
             break;
         case EMPM_OPT_ADJ_STORE: ctx->adj_store = value != 0; break;
         case EMPM_OPT_FUSE: ctx->fuse = value != 0; break;
+        case EMPM_OPT_SEGMENT_GRAPH: ctx->segment_graph = value != 0; break;
         case EMPM_OPT_SEG_CAP:
             if (value < 1 || value > 32 || (value & (value - 1)) != 0)
                 return empm_set_error(ctx, EMPM_ERR_INVALID, "seg_cap %d not a power of two in 1..32", value);
@@ -522,6 +525,13 @@ static Launch make_launch(EmpmCtx* ctx, int table) {
     return L;
 }
 
+// the same on another step-table array (a stored segment's own)
+static Launch make_launch_on(EmpmCtx* ctx, const EmpmStep* steps, int table) {
+    Launch L = make_launch(ctx, table);
+    L.steps = steps;
+    return L;
+}
+
 static ParticleArrays particle_arrays(const EmpmParticles* p, int n) {
     ParticleArrays a;
     a.x = reinterpret_cast<float4*>(p->x);
@@ -652,6 +662,7 @@ static int ensure_sorted_buffers(EmpmCtx* ctx) {
     if (sb.allocated && sb.n >= ctx->n_particles && sb.nb >= ctx->nblocks) return EMPM_OK;
     free_sorted(sb);
     ctx->resident = false;
+    ctx->epoch++;
     // sized for the context's capacity, so that re-laid batches reuse them
     const int n = ctx->cap_particles;
     const size_t nblocks = (size_t)ctx->cap_blocks;
@@ -933,7 +944,7 @@ static int launch_rollout(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, cons
     return EMPM_OK;
 }
 
-static int upload_steps(EmpmCtx* ctx, const EmpmStep* steps, int n_tables, cudaStream_t stream) {
+static int check_steps(EmpmCtx* ctx, const EmpmStep* steps, int n_tables) {
     if (!steps) return empm_set_error(ctx, EMPM_ERR_INVALID, "steps is NULL");
     if (n_tables < 1 || n_tables > 100000) return empm_set_error(ctx, EMPM_ERR_INVALID, "n_tables %d out of [1, 100000]", n_tables);
     const size_t total = (size_t)n_tables * ctx->n_inst;
@@ -942,7 +953,14 @@ static int upload_steps(EmpmCtx* ctx, const EmpmStep* steps, int n_tables, cudaS
             steps[s].n_modifiers < 0 || steps[s].n_modifiers > EMPM_MAX_MODIFIERS)
             return empm_set_error(ctx, EMPM_ERR_INVALID, "step entry %zu: collider/modifier count out of range", s);
     }
-    int rc = ensure_step_capacity(ctx, n_tables);
+    return EMPM_OK;
+}
+
+static int upload_steps(EmpmCtx* ctx, const EmpmStep* steps, int n_tables, cudaStream_t stream) {
+    int rc = check_steps(ctx, steps, n_tables);
+    if (rc) return rc;
+    const size_t total = (size_t)n_tables * ctx->n_inst;
+    rc = ensure_step_capacity(ctx, n_tables);
     if (rc) return rc;
     // pageable source: the runtime stages it before returning, so the caller may reuse it
     CK(cudaMemcpyAsync(ctx->d_steps, steps, sizeof(EmpmStep) * total, cudaMemcpyHostToDevice, stream),
@@ -1304,6 +1322,7 @@ static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
     }
     const size_t np = padded4(ctx->cap_particles);
     if (!ab.gacc) {
+        ctx->epoch++;
         const size_t grid_bytes = (size_t)ctx->cap_blocks * 64 * sizeof(float4);
         ab.cap_n = ctx->cap_particles;
         ab.cap_blocks = ctx->cap_blocks;
@@ -1318,6 +1337,7 @@ static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
         CK(cudaMalloc(&ab.gmats, 4 * np * sizeof(float)), "adjoint material");
     }
     if (n_steps > ab.capacity) {
+        ctx->epoch++;
         if (ab.states) CK(cudaDeviceSynchronize(), "sync before adjoint buffer growth");
         if (ab.states) cudaFree(ab.states);
         if (ab.mats) cudaFree(ab.mats);
@@ -1333,6 +1353,7 @@ static int ensure_adjoint_buffers(EmpmCtx* ctx, int n_steps) {
         // pass recomputes instead (free_store leaves store_cap at 0)
         if (ab.store_cap) CK(cudaDeviceSynchronize(), "sync before adjoint store growth");
         free_store(ab);
+        ctx->epoch++;
         const size_t nb = (size_t)ab.cap_blocks;
         cudaError_t e = cudaMalloc(&ab.gsave, (size_t)n_steps * nb * 128 * sizeof(float4));
         if (e == cudaSuccess) e = cudaMalloc(&ab.gsave_list, (size_t)n_steps * (nb + 1) * sizeof(int));
@@ -1384,6 +1405,7 @@ struct SegmentData {
     float* fe = nullptr;       // n_steps x f9 planes
     size_t cap_blocks = 0;     // grid blocks per substep slot
     int* max_count = nullptr;  // running maximum of the touched-block counts, or NULL
+    const EmpmStep* steps = nullptr;   // device step tables: [n_steps) as run, [n_steps, 2 n_steps) for recomputing
     MaterialArrays base;
 };
 
@@ -1415,7 +1437,7 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
             continue;
         }
         const F9Planes Fk = f9_planes(d.fe + (size_t)k * 9 * np, n);
-        const Launch Lk = make_launch(ctx, k);
+        const Launch Lk = make_launch_on(ctx, d.steps, k);
         timing_mark(ctx, 0, 0, s);
         if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
                                          ctx->seg_cap, uniform_material(ctx));
@@ -1444,11 +1466,11 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
 // The reverse pass: for each substep from the last, its grid (restored from
 // the store, or recomputed from the stored state with the step tables
 // [n_steps, 2 n_steps) that omit the velocity modifiers), then the three
-// adjoint kernels; finally the adjoint back into the caller's order.
-// Gp / gm_*: the incoming adjoint in the segment's order (updated in place).
+// adjoint kernels (segment_reverse_unpermute then takes the adjoint back into
+// the caller's order). Gp / gm_*: the incoming adjoint in the segment's order
+// (updated in place).
 static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp, float* gm_mu, float* gm_lam,
-                           float* gm_ys, float* gm_mass, EmpmParticles* grad, EmpmMaterialGrad* gmat,
-                           cudaStream_t s) {
+                           float* gm_ys, float* gm_mass, cudaStream_t s) {
     AdjointBuffers& ab = ctx->adj;
     const int n = d.n, n_steps = d.n_steps;
     const size_t np = d.np;
@@ -1465,7 +1487,7 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
     for (int k = n_steps - 1; k >= 0; --k) {
         float* snap = d.mats + (size_t)k * 3 * np;
         const ParticleArrays Pk = particle_arrays(d.states + (size_t)k * state_floats, n);
-        const Launch Lk = make_launch(ctx, k);
+        const Launch Lk = make_launch_on(ctx, d.steps, k);
         F9Planes Fk = Fe;
         const float4* slot = d.store ? d.gsave + (size_t)k * d.cap_blocks * 128 : nullptr;
         const int* slot_list = d.store ? d.glist + (size_t)k * (d.cap_blocks + 1) : nullptr;
@@ -1476,7 +1498,7 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         } else {
             CK(cudaMemcpyAsync(ab.work, snap, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, s),
                "restore snapshot");
-            const Launch Lrec = make_launch(ctx, n_steps + k);
+            const Launch Lrec = make_launch_on(ctx, d.steps, n_steps + k);
             timing_mark(ctx, 0, 0, s);
             if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pk, Mw, Fe, Lrec, ctx->grid_mom,
                                              ctx->flags, ctx->seg_cap, uniform_material(ctx));
@@ -1539,6 +1561,14 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         timing_mark(ctx, 5, 1, s);
         CK(cudaGetLastError(), "k_adj_p2g");
     }
+    return EMPM_OK;
+}
+
+// The adjoint of a sorted segment back into the caller's order.
+static int segment_reverse_unpermute(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp, float* gm_mu,
+                                     float* gm_lam, float* gm_ys, float* gm_mass, EmpmParticles* grad,
+                                     EmpmMaterialGrad* gmat, cudaStream_t s) {
+    const int n = d.n;
     if (d.sorted) {
         GradPermuteArgs back;
         back.src = Gp;
@@ -1668,25 +1698,86 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
     d.glist = ab.gsave_list;
     d.fe = ab.fe_store;
     d.cap_blocks = (size_t)ab.cap_blocks;
+    d.steps = ctx->d_steps;
     d.base = base;
     rc = segment_forward(ctx, d, s);
+    if (!rc) rc = segment_reverse(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, s);
     if (rc) return rc;
-    return segment_reverse(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, grad, gmat, s);
+    return segment_reverse_unpermute(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, grad, gmat, s);
 }
 
 // ---------------------------------------------------------------------------
 // stored segments: the forward keeps what the reverse pass needs
 // ---------------------------------------------------------------------------
+// Runs body(stream) for stream s: replayed from a segment's cached graph when
+// its key still matches, captured first otherwise (on the context's own
+// stream, joined to s by events, as the rollout graphs are). Kernel timing
+// and EMPM_OPT_SEGMENT_GRAPH 0 run the body directly. A substep loop of a
+// stored segment touches only the segment's and the context's buffers
+// (unsorted reverse passes also the caller's, which are in the key), so one
+// capture serves every later pass of a pooled segment.
+template <typename Body>
+static int run_segment_body(EmpmCtx* ctx, cudaGraphExec_t& exec, SegGraphKey& have, const SegGraphKey& want,
+                            cudaStream_t s, Body body) {
+    if (ctx->timing || !ctx->segment_graph) return body(s);
+    if (!exec || memcmp(&have, &want, sizeof(want)) != 0) {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        CK(cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal), "begin segment capture");
+        const int rc = body(ctx->own_stream);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        CK(e, "end segment capture");
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            exec = nullptr;
+            return empm_check_cuda(ctx, e, "segment graph instantiate");
+        }
+        have = want;
+    }
+    CK(cudaEventRecord(ctx->ev_a, s), "record");
+    CK(cudaStreamWaitEvent(ctx->own_stream, ctx->ev_a, 0), "wait");
+    CK(cudaGraphLaunch(exec, ctx->own_stream), "segment graph launch");
+    CK(cudaEventRecord(ctx->ev_b, ctx->own_stream), "record");
+    CK(cudaStreamWaitEvent(s, ctx->ev_b, 0), "wait");
+    return EMPM_OK;
+}
+
+static SegGraphKey segment_key(const EmpmCtx* ctx) {
+    SegGraphKey k;
+    memset(&k, 0, sizeof(k));
+    k.epoch = ctx->epoch;
+    k.params_version = ctx->params_version;
+    k.seg_cap = ctx->seg_cap;
+    k.p2g_mode = ctx->p2g_mode;
+    k.sort_every = ctx->sort_every;
+    k.n = ctx->n_particles;
+    return k;
+}
 static size_t segment_bytes(size_t np, size_t cap_blocks, int n_steps) {
     const size_t k = (size_t)n_steps;
     return ((k + 1) * 26 * np + k * 3 * np + k * 9 * np + np) * sizeof(float) + 2 * np * sizeof(int) +
            k * cap_blocks * 128 * sizeof(float4) + k * (cap_blocks + 1) * sizeof(int);
 }
 
+static size_t segment_bytes(const EmpmCtx* ctx, size_t np, size_t cap_blocks, int n_steps) {
+    return segment_bytes(np, cap_blocks, n_steps) + (size_t)n_steps * ctx->n_inst * sizeof(EmpmStep) + sizeof(int);
+}
+
 static void segment_free(EmpmSegment* seg) {
     void* ptrs[] = {seg->states, seg->mats, seg->gsave, seg->glist, seg->fe, seg->vol, seg->sel, seg->pid,
-                    seg->max_count};
+                    seg->max_count, seg->d_tables};
     for (void* q : ptrs) if (q) cudaFree(q);
+    if (seg->fwd_exec) cudaGraphExecDestroy(seg->fwd_exec);
+    if (seg->rev_exec) cudaGraphExecDestroy(seg->rev_exec);
+    seg->fwd_exec = seg->rev_exec = nullptr;
+    seg->d_tables = nullptr;
+    seg->tables_on_device = false;
     seg->states = seg->mats = seg->fe = seg->vol = nullptr;
     seg->gsave = nullptr;
     seg->glist = seg->sel = seg->pid = seg->max_count = nullptr;
@@ -1701,7 +1792,7 @@ extern "C" int empm_segment_bytes(EmpmCtx* ctx, int n_steps, int block_cap, size
     if (!ctx || !out) return empm_set_error(ctx, EMPM_ERR_INVALID, "ctx or out is NULL");
     if (n_steps < 1 || n_steps > 100000)
         return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d out of [1, 100000]", n_steps);
-    *out = segment_bytes(padded4(ctx->n_particles), segment_block_cap(ctx, block_cap), n_steps);
+    *out = segment_bytes(ctx, padded4(ctx->n_particles), segment_block_cap(ctx, block_cap), n_steps);
     return EMPM_OK;
 }
 
@@ -1728,13 +1819,14 @@ extern "C" int empm_segment_create(EmpmCtx* ctx, int n_steps, int block_cap, Emp
     if (e == cudaSuccess) e = cudaMalloc(&seg->sel, np * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&seg->pid, np * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&seg->max_count, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&seg->d_tables, k * (size_t)ctx->n_inst * sizeof(EmpmStep));
     if (e != cudaSuccess) {
         segment_free(seg);
         delete seg;
         if (e == cudaErrorMemoryAllocation) {
             cudaGetLastError();   // an allocation failure is not sticky; clear it
             return empm_set_error(ctx, EMPM_ERR_OOM, "segment store of %d substeps (%zu bytes) does not fit", n_steps,
-                                  segment_bytes(np, nb, n_steps));
+                                  segment_bytes(ctx, np, nb, n_steps));
         }
         return empm_check_cuda(ctx, e, "segment store");
     }
@@ -1774,6 +1866,7 @@ static SegmentData segment_data(const EmpmSegment* seg) {
     d.fe = seg->fe;
     d.cap_blocks = seg->block_cap;
     d.max_count = seg->max_count;
+    d.steps = seg->d_tables;
     d.base.vol = seg->vol;
     d.base.mu = d.base.lam = d.base.ys = nullptr;
     d.base.sel = seg->has_sel ? seg->sel : nullptr;
@@ -1795,15 +1888,24 @@ extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmPa
         return empm_set_error(ctx, EMPM_ERR_INVALID, "n_steps %d, the segment holds %d", n_steps, seg->n_steps);
     if (!steps) return empm_set_error(ctx, EMPM_ERR_INVALID, "steps is NULL");
     const size_t per = (size_t)n_steps * ctx->n_inst;
+    rc = check_steps(ctx, steps, n_steps);
+    if (rc) return rc;
     for (size_t e = 0; e < per; ++e)
         if (steps[e].hold) return empm_set_error(ctx, EMPM_ERR_UNSUPPORTED, "held substeps cannot be differentiated");
     cudaStream_t s = (cudaStream_t)stream;
     seg->ready = false;
     seg->checked = false;
     seg->max_touched = 0;
-    seg->tables.assign(steps, steps + per);
-    rc = upload_steps(ctx, seg->tables.data(), n_steps, s);
-    if (rc) return rc;
+    // the segment keeps its own device copy of its step tables (uploaded only
+    // when they change), so its captured substep loop can be replayed as is
+    if (!seg->tables_on_device || seg->tables.size() != per ||
+        memcmp(seg->tables.data(), steps, per * sizeof(EmpmStep)) != 0) {
+        seg->tables.assign(steps, steps + per);
+        seg->tables_on_device = false;
+        CK(cudaMemcpyAsync(seg->d_tables, seg->tables.data(), per * sizeof(EmpmStep), cudaMemcpyHostToDevice, s),
+           "segment step tables");
+        seg->tables_on_device = true;
+    }
     const int n = seg->n;
     if (n == 0) {
         seg->ready = true;
@@ -1851,7 +1953,8 @@ extern "C" int empm_segment_forward(EmpmCtx* ctx, EmpmSegment* seg, const EmpmPa
         if (seg->has_sel) CK(cudaMemcpyAsync(seg->sel, mat->selection, sizeof(int) * n, d2d, s), "copy material");
     }
     const SegmentData d = segment_data(seg);
-    rc = segment_forward(ctx, d, s);
+    rc = run_segment_body(ctx, seg->fwd_exec, seg->fwd_key, segment_key(ctx), s,
+                          [&](cudaStream_t bs) { return segment_forward(ctx, d, bs); });
     if (rc) return rc;
     // the state after the last substep, its elastic F and the updated
     // material scalars, in the caller's order
@@ -1919,8 +2022,6 @@ extern "C" int empm_segment_reverse(EmpmCtx* ctx, EmpmSegment* seg, EmpmParticle
                               "of %zu: make it with block_cap >= %d and run the forward pass again",
                               seg->max_touched, seg->block_cap, seg->max_touched);
     cudaStream_t s = (cudaStream_t)stream;
-    rc = upload_steps(ctx, seg->tables.data(), seg->n_steps, s);
-    if (rc) return rc;
     const int n = seg->n;
     if (n == 0) return EMPM_OK;
     rc = ensure_adjoint_buffers(ctx, 0);
@@ -1951,7 +2052,17 @@ extern "C" int empm_segment_reverse(EmpmCtx* ctx, EmpmSegment* seg, EmpmParticle
         CK(cudaGetLastError(), "k_permute_grad");
         Gp = perm.dst;
     }
-    return segment_reverse(ctx, segment_data(seg), Gp, gm_mu, gm_lam, gm_ys, gm_mass, grad, gmat, s);
+    const SegmentData d = segment_data(seg);
+    SegGraphKey key = segment_key(ctx);
+    if (!seg->sorted) {   // the loop then works on the caller's adjoint arrays
+        const void* b[8] = {grad->x, grad->v, grad->C, grad->F, gmat->mu, gmat->lam, gmat->yield_stress, gmat->mass};
+        memcpy(key.buf, b, sizeof(b));
+    }
+    rc = run_segment_body(ctx, seg->rev_exec, seg->rev_key, key, s, [&](cudaStream_t bs) {
+        return segment_reverse(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, bs);
+    });
+    if (rc) return rc;
+    return segment_reverse_unpermute(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, grad, gmat, s);
 }
 
 extern "C" int empm_restart_F(EmpmCtx* ctx, EmpmParticles* p, const float* target, const int* selection,

@@ -121,6 +121,7 @@ class MPMWARPDiff(object):
         self.seg_cap = 4           # warp-aggregated P2G: longest same-cell run per reduction
         self.adj_store = True      # adjoint keeps each substep's grid and elastic F instead of recomputing
         self.fuse = True           # rollouts fuse each G2P with the next substep's stress + P2G
+        self.segment_graph = True  # stored tape segments replay their substep loops from CUDA graphs
 
     def initialize(self, n_particles, n_grid=100, grid_lim=1.0, device="cuda:0"):
         self.n_particles = n_particles
@@ -190,7 +191,8 @@ class MPMWARPDiff(object):
         c.set_options({N.OPT_SORT_EVERY: int(self.sort_every), N.OPT_P2G_MODE: int(self.p2g_mode),
                        N.OPT_G2P_TILE: int(bool(self.g2p_tile)), N.OPT_TILE_CAP: int(self.tile_cap),
                        N.OPT_SEG_CAP: int(self.seg_cap), N.OPT_ADJ_STORE: int(bool(self.adj_store)),
-                       N.OPT_FUSE: int(bool(getattr(self, "fuse", True)))})
+                       N.OPT_FUSE: int(bool(getattr(self, "fuse", True))),
+                       N.OPT_SEGMENT_GRAPH: int(bool(getattr(self, "segment_graph", True)))})
         return c
 
     @staticmethod

@@ -318,6 +318,10 @@ int  empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const Emp
                                     kernel that keeps only position and elastic F per particle between substeps
                                     (default); 0 = separate kernels. Step tables that release a held instance
                                     (hold 1 then 0) always run separately. */
+#define EMPM_OPT_SEGMENT_GRAPH 8 /* stored segments (empm_segment_forward / _reverse): 1 = each segment captures
+                                    its substep loop as a CUDA graph on first use and replays it while the
+                                    context's options and buffers are unchanged (default); 0 = launch the
+                                    kernels one by one */
 
 int  empm_ctx_set_option(EmpmCtx* ctx, int option, int value);
 
@@ -428,6 +432,10 @@ int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* 
  *                       be reversed more than once. It checks the touched
  *                       block count (empm_segment_blocks, once per forward
  *                       pass) and returns EMPM_ERR_INVALID after an overflow.
+ * A segment keeps a device copy of its step tables (uploaded again only when
+ * they change) and, with EMPM_OPT_SEGMENT_GRAPH, its captured substep loops:
+ * the first forward and reverse pass of a segment capture them, so make those
+ * calls outside stream capture.
  * Gradients equal those of empm_adjoint_segment (which stores and reverses one
  * segment inside one call) up to the order of floating-point reductions. */
 typedef struct EmpmSegment EmpmSegment;

@@ -310,6 +310,56 @@ def test_segment_adjoint_store_matches_recompute(sort_every):
 
 
 @pytest.mark.parametrize("sort_every", [16, 0])
+def test_segment_graphs_match_direct_launches(sort_every):
+    """Stored segments capture their substep loops as CUDA graphs on first use
+    and replay them on later passes of the pooled segments. Replayed passes,
+    including one whose step tables changed (a later start time moves the
+    impulse's gate), give the gradients of the same passes launched kernel by
+    kernel, up to the order of the atomics."""
+    dt, T, every = 2e-4, 10, 4
+    p = _problem(5, n=1500, G=24, seed=21, floor=True, deform=0.25, speed=0.5)
+    p["v"][:, 1] = np.float32(-1.0)
+    p["sort_every"] = sort_every
+    p["modifiers"] = [dict(kind="impulse", force=[0.0, 0.0, 2e-3], point=[0.3, 0.2, 0.3], size=[0.15, 0.15, 0.15],
+                           num_dt=3)]
+    n = p["n"]
+    rng = np.random.default_rng(23)
+    g_x = _t(rng.standard_normal((n, 3)))
+    g_v = _t(rng.standard_normal((n, 3)))
+
+    def run(graphs, t0, passes):
+        st, md, sv = _setup(p, dt)
+        sv.segment_graph = graphs
+        x0, v0 = st.particle_x.clone(), st.particle_v.clone()
+        mat0 = (md.mu.clone(), md.lam.clone(), md.yield_stress.clone())
+        out = []
+        for _ in range(passes):
+            st.particle_x = x0
+            st.particle_v = v0
+            for dst, src in zip((md.mu, md.lam, md.yield_stress), mat0):
+                dst.copy_(src)
+            sv.time = t0
+            tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=every, store=True)
+            final = tape.forward()
+            res = tape.backward(g_x=g_x, g_v=g_v)
+            torch.cuda.synchronize()
+            out.append((final.particle_x.double().cpu().numpy(),
+                        {k: v.double().cpu().numpy() for k, v in res.items()}))
+            tape.release()
+        return out
+
+    for t0 in (0.0, 1.5 * dt):
+        replayed = run(True, t0, 3)      # pass 1 may size the segments; later passes replay
+        direct = run(False, t0, 1)[0]
+        for xf, res in replayed[1:]:
+            assert float(np.abs(xf - direct[0]).max()) <= 1e-5
+            for k in res:
+                a, b = res[k], direct[1][k]
+                rel = float(np.linalg.norm(a - b)) / max(float(np.linalg.norm(b)), 1e-30)
+                assert rel <= 2e-3, (t0, k, rel)
+
+
+@pytest.mark.parametrize("sort_every", [16, 0])
 def test_checkpointed_segments_fd(sort_every):
     """Finite differences through checkpointed segments (re-run in the reverse
     pass), the path taken when the stored rollout does not fit."""
