@@ -761,7 +761,7 @@ def run_ours_c3(args):
     target = W.c3(guess=False, **kw)
     every = args.checkpoint_every
     solver, md, st, other = W.build_product(target, device=dev)
-    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap", "adj_store"):
+    for opt in ("sort_every", "p2g_mode", "g2p_tile", "tile_cap", "seg_cap", "adj_store", "fuse"):
         val = getattr(args, opt)
         if val is not None:
             setattr(solver, opt, val)

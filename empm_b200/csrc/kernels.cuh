@@ -897,6 +897,99 @@ __global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g(ParticleArra
     warpagg_scatter<ROUNDS>(valid, inst, q, c, mom, flags);
 }
 
+// Stored segments of a differentiable rollout (cell-sorted): the G2P of
+// substep k-1 and the stress + P2G of substep k in one pass, writing what the
+// reverse pass reads instead of handing state from kernel to kernel: the full
+// state before substep k (its velocity after the modifiers, as the P2G of the
+// separate kernels leaves it), the mu / lam / yield snapshot before substep k
+// and the elastic F of substep k. Segments hold no instances (step-table hold)
+// and their particles stay in one order, so every thread writes only its own
+// particle of the substep-k arrays.
+struct SegmentStoreArgs {
+    ParticleArrays prev;     // state before substep k-1 (x read)
+    F9Planes       fe_prev;  // elastic F of substep k-1
+    ParticleArrays cur;      // out: state before substep k
+    F9Planes       fe_cur;   // out: elastic F of substep k
+    float*         snap;     // out: mu | lam | yield before substep k, stride np
+    long long      np;
+};
+
+template <int ROUNDS, int MAT = -1>
+__global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g_store(MaterialArrays M, Launch L, int g2p_table,
+                                                                        const float4* vel, float4* mom,
+                                                                        unsigned char* flags, SegmentStoreArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int inst = p < L.n_total ? find_instance_particle(L, p) : 0;
+    const StepConsts c = consts_of(L, inst);   // substep k: stress + P2G
+    P2GParticle q;
+    bool valid = false;
+    if (p < L.n_total) {
+        const float mu0 = __ldg(M.mu + p), lam0 = __ldg(M.lam + p), ys0 = __ldg(M.ys + p);
+        a.snap[p] = mu0;
+        a.snap[a.np + p] = lam0;
+        a.snap[2 * a.np + p] = ys0;
+        const float4 xm = __ldg(a.prev.x + p);
+        if (M.sel && __ldg(M.sel + p) != 0) {
+            // unsimulated: the G2P writes the reference's constant state, no P2G
+            a.cur.x[p] = make_float4(0.f, 0.f, 0.f, xm.w);
+            a.cur.v[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+            f9_store(a.cur.C, p, m3_zero());
+            f9_store(a.cur.F, p, m3_identity());
+        } else {
+            const float dt = L.steps[(size_t)g2p_table * L.n_inst + inst].dt;   // substep k-1
+            const V3 x = v3(xm.x, xm.y, xm.z);
+            const Stencil st = make_stencil(x, c.inv_dx);
+            const bool in_grid = stencil_in_grid(st, c.G);
+            const GlobalFetch fetch{vel, &c};
+            const G2POut o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
+            const float dx = 1.f / c.inv_dx;   // as g2p_particle computes it
+            const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
+            V3 nx = x + dt * o.v;
+            nx = v3(fminf(fmaxf(nx.x, lo), hi), fminf(fmaxf(nx.y, lo), hi), fminf(fmaxf(nx.z, lo), hi));
+            const M3 Fn = (m3_identity() + dt * o.gradv) * f9_load(a.fe_prev, p);
+            unsigned bad = 0;
+            if (!finite3(o.v) || !finite3(nx) || !isfinite(Fn.m[0] + Fn.m[4] + Fn.m[8])) bad |= EMPM_STATUS_NAN;
+            if (fmaxf(fmaxf(fabsf(o.v.x), fabsf(o.v.y)), fabsf(o.v.z)) * dt > dx) bad |= EMPM_STATUS_CFL;
+            if (!in_grid) bad |= EMPM_STATUS_OUT_OF_BAND;
+            if (bad) atomicOr(c.status, bad);
+            const EmpmStep& sp = *c.step;
+            V3 v = o.v;
+            if (sp.n_modifiers > 0) {
+                const int mi = M.pid ? __ldg(M.pid + p) : p;
+                apply_modifiers(sp, mi, nx, xm.w, v);
+            }
+            a.cur.x[p] = make_float4(nx.x, nx.y, nx.z, xm.w);
+            a.cur.v[p] = make_float4(v.x, v.y, v.z, 0.f);
+            f9_store(a.cur.C, p, o.C);
+            f9_store(a.cur.F, p, Fn);
+            float mu = mu0, lam = lam0, ys = ys0;
+            const ConstitutiveOut co = constitutive<MAT>(Fn, mu, lam, ys, sp.dt, c.ms);
+            f9_store(a.fe_cur, p, co.F);
+            if (co.mat_changed) { M.mu[p] = mu; M.lam[p] = lam; M.ys[p] = ys; }
+            q.st = make_stencil(nx, c.inv_dx);
+            q.wm_scale = xm.w;
+            q.v = v;
+            q.Cd = damp_affine(o.C, c.rpic);
+            q.Sv = (-__ldg(M.vol + p)) * co.tau;
+            valid = true;
+        }
+    }
+    warpagg_scatter<ROUNDS>(valid, inst, q, c, mom, flags);
+}
+
+// k_g2p2g_store at the default run cap (4) for a launch whose instances all
+// use material (plasticine 5 and jelly 0 have kernels of their own, -1 any).
+// Returns false for other run caps (the caller runs the separate kernels).
+static inline bool launch_g2p2g_store(int grid_ctas, int threads, cudaStream_t s, const MaterialArrays& M,
+                                      const Launch& L, int g2p_table, const float4* vel, float4* mom,
+                                      unsigned char* flags, const SegmentStoreArgs& a, int seg_cap, int material) {
+    if (seg_cap != 4) return false;
+    if (material == 5) k_g2p2g_store<2, 5><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
+    else if (material == 0) k_g2p2g_store<2, 0><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
+    else k_g2p2g_store<2, -1><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
+    return true;
+}
+
 static inline void launch_g2p2g(int grid_ctas, int threads, cudaStream_t s, const ParticleArrays& P,
                                 const MaterialArrays& M, const F9Planes& Fe, const Launch& L, int g2p_table,
                                 const float4* vel, float4* mom, unsigned char* flags, int seg_cap,

@@ -1415,7 +1415,10 @@ struct SegmentData {
 // the state after it is only needed by the caller: its P2G writes the
 // velocity modifiers into that substep's stored velocities, which the reverse
 // pass reads. With the store, P2G writes each substep's elastic F straight
-// into its store slot and the grid update saves the touched grid blocks.
+// into its store slot and the grid update saves the touched grid blocks; on
+// the sorted path (run cap 4, EMPM_OPT_FUSE) every substep after the first
+// runs its stress + P2G in one kernel with the previous substep's G2P
+// (k_g2p2g_store), which writes the stored state and snapshot itself.
 static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
     AdjointBuffers& ab = ctx->adj;
     const int n = d.n;
@@ -1426,24 +1429,45 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
     Mw.lam = ab.work + np;
     Mw.ys = ab.work + 2 * np;
     const F9Planes Fe = f9_planes(ab.fe, n);
+    // sorted stored segments: from the second substep on, the G2P of the
+    // previous substep and the stress + P2G of this one run as one kernel
+    // that writes the stored state, snapshot and elastic F itself
+    const bool fused = d.store && d.sorted && ctx->fuse && ctx->seg_cap == 4 && d.n_steps > 1;
     for (int k = 0; k < d.n_steps; ++k) {
-        CK(cudaMemcpyAsync(d.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, s),
-           "snapshot");
         const ParticleArrays Pin = particle_arrays(d.states + (size_t)k * state_floats, n);
         const ParticleArrays Pout = particle_arrays(d.states + (size_t)(k + 1) * state_floats, n);
         if (!d.store) {
+            CK(cudaMemcpyAsync(d.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice,
+                               s), "snapshot");
             const int rc = launch_substep_arrays(ctx, Pin, Pout, Mw, Fe, k, d.sorted, s);
             if (rc) return rc;
             continue;
         }
         const F9Planes Fk = f9_planes(d.fe + (size_t)k * 9 * np, n);
         const Launch Lk = make_launch_on(ctx, d.steps, k);
-        timing_mark(ctx, 0, 0, s);
-        if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
-                                         ctx->seg_cap, uniform_material(ctx));
-        else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
-        timing_mark(ctx, 0, 1, s);
-        CK(cudaGetLastError(), "adjoint segment P2G");
+        if (fused && k > 0) {
+            SegmentStoreArgs sa;
+            sa.prev = particle_arrays(d.states + (size_t)(k - 1) * state_floats, n);
+            sa.fe_prev = f9_planes(d.fe + (size_t)(k - 1) * 9 * np, n);
+            sa.cur = Pin;
+            sa.fe_cur = Fk;
+            sa.snap = d.mats + (size_t)k * 3 * np;
+            sa.np = (long long)np;
+            timing_mark(ctx, 6, 0, s);
+            launch_g2p2g_store(blocks_for(n, 256), 256, s, Mw, Lk, k - 1, ctx->grid_vel, ctx->grid_mom, ctx->flags, sa,
+                               ctx->seg_cap, uniform_material(ctx));
+            timing_mark(ctx, 6, 1, s);
+            CK(cudaGetLastError(), "k_g2p2g_store");
+        } else {
+            CK(cudaMemcpyAsync(d.mats + (size_t)k * 3 * np, ab.work, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice,
+                               s), "snapshot");
+            timing_mark(ctx, 0, 0, s);
+            if (d.sorted) launch_p2g_warpagg(blocks_for(n, 256), 256, s, Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags,
+                                             ctx->seg_cap, uniform_material(ctx));
+            else k_p2g_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Mw, Fk, Lk, ctx->grid_mom, ctx->flags);
+            timing_mark(ctx, 0, 1, s);
+            CK(cudaGetLastError(), "adjoint segment P2G");
+        }
         // the grid update stores the touched blocks as it goes, and clears the
         // accumulator and the touched flags as for a plain substep
         timing_mark(ctx, 1, 0, s);
@@ -1455,6 +1479,7 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
         const int rc = launch_grid_update_list<false>(ctx, Lk, s, &slot);
         if (rc) return rc;
         timing_mark(ctx, 1, 1, s);
+        if (fused && k + 1 < d.n_steps) continue;   // the next fused kernel runs this G2P
         timing_mark(ctx, 2, 0, s);
         k_g2p_direct<<<blocks_for(n, 128), 128, 0, s>>>(Pin, Fk, Mw, Pout, Lk, ctx->grid_vel);
         timing_mark(ctx, 2, 1, s);
