@@ -27,10 +27,10 @@
 #include "spectral.cuh"
 
 // Minimum resident CTAs (of 128 threads) per SM asked of the compiler for the
-// two particle kernels of the adjoint. The one-pass G2P adjoint keeps 33
+// two particle kernels of the adjoint. The one-pass G2P adjoint keeps 18
 // accumulators live across its stencil loop: at 4 CTAs (128 registers) it
-// spills 12 B and took 45.2 us per 200k-particle substep, at 5 CTAs (96
-// registers, 140 B spilled) 53.5 us, at 6 (80 registers, 244 B) 48.8 us.
+// does not spill and took 43.5 us per 200k-particle substep, at 5 CTAs (96
+// registers, 60 B spilled) 48.0 us, at 6 (80 registers, 132 B) 45.5 us.
 #ifndef EMPM_ADJ_G2P_MIN_CTAS
 #define EMPM_ADJ_G2P_MIN_CTAS 4
 #endif
@@ -86,8 +86,8 @@ struct AdjG2PArgs {
 // and the forward's v' = sum w vg and grad v' = sum vg (x) dw, needed for the
 // x and F_elastic adjoints, are summed in the same pass. Every sum factorises
 // over the inner stencil axis (per row (i, j) the three nodes are combined
-// with wz_k, dwz_k, (1, -2, 1) and k wz_k); the Hessian term is kept as its
-// six moments sum_n H_n[pair] vg_n and contracted with gGv after the loop.
+// with wz_k, dwz_k, (1, -2, 1) and k wz_k); the Hessian term is contracted
+// with gGv row by row.
 //
 // Lanes whose particles share an instance and base cell (contiguous in cell
 // order) sum their node-velocity adjoints with shuffles; the segment head
@@ -157,10 +157,10 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     const V3 zero = v3(0.f, 0.f, 0.f);
     V3 Vs = zero;                      // sum w vg (the forward's v')
     V3 D0 = zero, D1 = zero, D2 = zero;   // columns of sum vg (x) dweight / inv_dx
-    V3 X3 = zero;                      // sum dot(vg, q) dweight / inv_dx
-    V3 Hv[6];                          // sum H[pair] vg, pairs xx, yy, zz, xy, xz, yz (grid units)
-#pragma unroll
-    for (int r = 0; r < 6; ++r) Hv[r] = zero;
+    // sum dot(vg, q) dweight + inv_dx sum H gGv^T vg, both over inv_dx (the
+    // Hessian term contracted row by row: three accumulators instead of the
+    // 18 of its moments, which let the kernel fit fewer registers)
+    V3 X3 = zero;
 #if EMPM_ADJ_G2P_ROLL
 #pragma unroll 1
 #else
@@ -224,13 +224,14 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
             D0 = D0 + dxy * T0;
             D1 = D1 + xdy * T0;
             D2 = D2 + wxy * T1;
-            X3 = X3 + v3(dxy * sg0, xdy * sg0, wxy * sg1);
-            Hv[0] = Hv[0] + (hx * wy) * T0;
-            Hv[1] = Hv[1] + (wx * bspline_d2(j)) * T0;
-            Hv[2] = Hv[2] + wxy * T2;
-            Hv[3] = Hv[3] + (ux * uy) * T0;
-            Hv[4] = Hv[4] + dxy * T1;
-            Hv[5] = Hv[5] + xdy * T1;
+            // sum_n H_n gGv^T vg_n over the row, component a = sum_b dot(G_b, H[a][b] row sum), with
+            // the pair row sums (hx wy) T0, (wx hy) T0, wxy T2, (ux uy) T0, dxy T1, xdy T1
+            const float d00 = dot(G0, T0), d10 = dot(G1, T0), d01 = dot(G0, T1), d11 = dot(G1, T1);
+            const float d21 = dot(G2, T1), d22 = dot(G2, T2);
+            const float uxy = ux * uy;
+            X3 = X3 + v3(dxy * (sg0 + d21) + (hx * wy) * d00 + uxy * d10,
+                         xdy * (sg0 + d21) + uxy * d00 + (wx * bspline_d2(j)) * d10,
+                         wxy * (sg1 + d22) + dxy * d01 + xdy * d11);
         }
         Vs = Vs + Vi;
     }
@@ -246,14 +247,10 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
             for (int cl = 0; cl < 3; ++cl) A.m[3 * r + cl] = (r == cl ? 1.f : 0.f) + s * comp(dc[cl], r);
     }
     f9_store(a.gFe, p, transpose(A) * (valid ? f9_load(a.Gn.F, p) : m3_zero()));
-    // sum_n H_n gGv^T vg_n, component a = sum_b dot(column b of gGv, sum_n H_n[a][b] vg_n); with G = inv_dx gGv
-    // the term inv_dx^2 (...) is inv_dx (...) in G. The forward's C' = 4 inv_dx (...) enters the x
-    // adjoint as -4 inv_dx^2 gC'^T v' = -inv_dx (dot(Q_c, v'))_c.
-    const V3 hS = v3(dot(G0, Hv[0]) + dot(G1, Hv[3]) + dot(G2, Hv[4]),
-                     dot(G0, Hv[3]) + dot(G1, Hv[1]) + dot(G2, Hv[5]),
-                     dot(G0, Hv[4]) + dot(G1, Hv[5]) + dot(G2, Hv[2]));
+    // With G = inv_dx gGv the Hessian term inv_dx^2 sum H gGv^T vg is inv_dx sum H G^T vg (in X3).
+    // The forward's C' = 4 inv_dx (...) enters the x adjoint as -4 inv_dx^2 gC'^T v' = -inv_dx (dot(Q_c, v'))_c.
     const V3 QV = v3(dot(Q0, Vs), dot(Q1, Vs), dot(Q2, Vs));
-    const V3 gxa = gxu + c.inv_dx * (X3 + hS - QV);
+    const V3 gxa = gxu + c.inv_dx * (X3 - QV);
     a.gx[p] = make_float4(gxa.x, gxa.y, gxa.z, 0.f);
 }
 
