@@ -201,12 +201,57 @@ struct SpectralEval {
     SpectralOut<D6> o;
 };
 
+// Fixed-corotated stress with no return map (jelly, and plasticine inside its
+// yield surface), with its Jacobian written out: f = s, the scalars pass
+// through, h_a = 2 mu (s_a - 1) s_a + lam J (J - 1) with J = s0 s1 s2, so
+//   dh_a/ds_b = 2 mu (2 s_a - 1) [a = b] + lam (2 J - 1) J_b,  J_b = dJ/ds_b,
+//   dh_a/dmu = 2 (s_a - 1) s_a,  dh_a/dlam = J (J - 1).
+// The same values and derivatives as spectral_map on Dual<6> numbers on that
+// branch, for a fraction of its arithmetic.
+EMPM_HD void spectral_fcr_elastic(const float s[3], float mu, float lam, float ys, SpectralOut<D6>& o) {
+    const float J = s[0] * s[1] * s[2];
+    const float Jb[3] = {s[1] * s[2], s[0] * s[2], s[0] * s[1]};
+    const float vol = lam * J * (J - 1.f);
+    const float cv = lam * (2.f * J - 1.f);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        o.f[a] = dseed<6>(s[a], a);
+        o.h[a].v = (2.f * mu) * (s[a] - 1.f) * s[a] + vol;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) o.h[a].d[b] = cv * Jb[b] + (a == b ? (2.f * mu) * (2.f * s[a] - 1.f) : 0.f);
+        o.h[a].d[3] = 2.f * (s[a] - 1.f) * s[a];
+        o.h[a].d[4] = J * (J - 1.f);
+        o.h[a].d[5] = 0.f;
+    }
+    o.mu = dseed<6>(mu, 3);
+    o.lam = dseed<6>(lam, 4);
+    o.ys = dseed<6>(ys, 5);
+}
+
+// The von Mises yield test of constitutive() (constitutive.cuh) on the
+// singular values: true when the return map changes nothing.
+EMPM_HD bool von_mises_inside(const float s[3], float mu, float lam, float ys, bool damage) {
+    const V3 sig = v3(fmaxf(s[0], 0.01f), fmaxf(s[1], 0.01f), fmaxf(s[2], 0.01f));
+    const V3 eps = v3(logf(sig.x), logf(sig.y), logf(sig.z));
+    const float tr = eps.x + eps.y + eps.z;
+    const V3 tau = 2.f * mu * eps + v3(lam * tr, lam * tr, lam * tr);
+    const float sum_tau = tau.x + tau.y + tau.z;
+    const V3 cond = tau - v3(sum_tau / 3.f, sum_tau / 3.f, sum_tau / 3.f);
+    if (!(length(cond) > ys)) return true;
+    return damage && ys <= 0.f;
+}
+
 template <int MAT = -1>
 EMPM_HD void spectral_eval(const M3& Ft, float mu, float lam, float ys, float dt, const MaterialScalars& ms,
                            SpectralEval& e) {
     V3 sv;
     svd3(Ft, e.U, sv, e.V);
     e.s[0] = sv.x; e.s[1] = sv.y; e.s[2] = sv.z;
+    const int material = MAT >= 0 ? MAT : ms.material;
+    if (material == 0 || (material == 5 && von_mises_inside(e.s, mu, lam, ys, true))) {
+        spectral_fcr_elastic(e.s, mu, lam, ys, e.o);
+        return;
+    }
     const D6 s[3] = {dseed<6>(sv.x, 0), dseed<6>(sv.y, 1), dseed<6>(sv.z, 2)};
     e.o = spectral_map<D6, MAT>(s, dseed<6>(mu, 3), dseed<6>(lam, 4), dseed<6>(ys, 5), dt, ms);
 }
