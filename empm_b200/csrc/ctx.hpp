@@ -31,7 +31,16 @@ struct SegGraphKey {
     unsigned long long epoch;
     unsigned long long params_version;
     int                seg_cap, p2g_mode, sort_every, n;
-    const void*        buf[8];
+    int                n_steps, store;
+    const void*        buf[10];
+};
+
+// A captured re-run + reverse pass of a checkpointed segment
+// (empm_adjoint_segment), cached per context by its key.
+struct AdjSegGraph {
+    SegGraphKey        key{};
+    cudaGraphExec_t    exec = nullptr;
+    unsigned long long used = 0;
 };
 
 // One captured rollout launch sequence and the sorted state it ends in.
@@ -130,6 +139,8 @@ struct EmpmCtx {
     // (options, instance tables, reallocated buffers): segment graphs compare it
     unsigned long long epoch = 1;
     int          segment_graph = 1;        // stored segments replay their substeps from a CUDA graph
+    static constexpr int kAdjGraphs = 4;   // cached checkpointed-segment graphs (LRU)
+    AdjSegGraph  adj_graphs[kAdjGraphs];
     // the sorted state the last rollout ended in, which EMPM_ROLLOUT_RESUME
     // continues from: particle / material buffer and substeps since its sort
     bool         resident = false;

@@ -279,6 +279,8 @@ extern "C" int empm_ctx_create(const EmpmModelParams* params, int n_particles, i
 extern "C" int empm_ctx_destroy(EmpmCtx* ctx) {
     if (!ctx) return EMPM_OK;
     destroy_graphs(ctx);
+    for (AdjSegGraph& g : ctx->adj_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t ev : ctx->timing_events) cudaEventDestroy(ev);
     free_sorted(ctx->sb);
     free_adjoint(ctx->adj);
@@ -1609,6 +1611,58 @@ static int segment_reverse_unpermute(EmpmCtx* ctx, const SegmentData& d, Particl
     return EMPM_OK;
 }
 
+// Runs body(stream) for stream s: replayed from a cached graph (a stored
+// segment's, or one of the context's for checkpointed segments) when its key
+// still matches, captured first otherwise (on the context's own
+// stream, joined to s by events, as the rollout graphs are). Kernel timing
+// and EMPM_OPT_SEGMENT_GRAPH 0 run the body directly. A substep loop of a
+// stored segment touches only the segment's and the context's buffers
+// (unsorted reverse passes also the caller's, which are in the key), so one
+// capture serves every later pass of a pooled segment.
+template <typename Body>
+static int run_segment_body(EmpmCtx* ctx, cudaGraphExec_t& exec, SegGraphKey& have, const SegGraphKey& want,
+                            cudaStream_t s, Body body) {
+    if (ctx->timing || !ctx->segment_graph) return body(s);
+    if (!exec || memcmp(&have, &want, sizeof(want)) != 0) {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        CK(cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal), "begin segment capture");
+        const int rc = body(ctx->own_stream);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        CK(e, "end segment capture");
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            exec = nullptr;
+            return empm_check_cuda(ctx, e, "segment graph instantiate");
+        }
+        have = want;
+    }
+    CK(cudaEventRecord(ctx->ev_a, s), "record");
+    CK(cudaStreamWaitEvent(ctx->own_stream, ctx->ev_a, 0), "wait");
+    CK(cudaGraphLaunch(exec, ctx->own_stream), "segment graph launch");
+    CK(cudaEventRecord(ctx->ev_b, ctx->own_stream), "record");
+    CK(cudaStreamWaitEvent(s, ctx->ev_b, 0), "wait");
+    return EMPM_OK;
+}
+
+static SegGraphKey segment_key(const EmpmCtx* ctx) {
+    SegGraphKey k;
+    memset(&k, 0, sizeof(k));
+    k.epoch = ctx->epoch;
+    k.params_version = ctx->params_version;
+    k.seg_cap = ctx->seg_cap;
+    k.p2g_mode = ctx->p2g_mode;
+    k.sort_every = ctx->sort_every;
+    k.n = ctx->n_particles;
+    return k;
+}
+
 extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* ckpt_mu,
                                     const float* ckpt_lam, const float* ckpt_yield, const EmpmMaterial* mat,
                                     const EmpmStep* steps, int n_steps, EmpmParticles* grad,
@@ -1725,8 +1779,29 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
     d.cap_blocks = (size_t)ab.cap_blocks;
     d.steps = ctx->d_steps;
     d.base = base;
-    rc = segment_forward(ctx, d, s);
-    if (!rc) rc = segment_reverse(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, s);
+    // the re-run and the reverse pass replay a graph captured by an earlier
+    // call with the same key: on the sorted path they touch only the
+    // context's buffers; on the caller-order path the caller's material and
+    // adjoint arrays are part of the key
+    SegGraphKey key = segment_key(ctx);
+    key.n_steps = n_steps;
+    key.store = d.store ? 1 : 0;
+    if (!sorted) {
+        const void* b[10] = {mat->vol, mat->selection, grad->x, grad->v, grad->C, grad->F,
+                             gmat->mu, gmat->lam, gmat->yield_stress, gmat->mass};
+        memcpy(key.buf, b, sizeof(b));
+    }
+    AdjSegGraph* g = &ctx->adj_graphs[0];
+    for (AdjSegGraph& e : ctx->adj_graphs) {
+        if (e.exec && memcmp(&e.key, &key, sizeof(key)) == 0) { g = &e; break; }
+        if (e.used < g->used) g = &e;
+    }
+    g->used = ++ctx->graph_clock;
+    rc = run_segment_body(ctx, g->exec, g->key, key, s, [&](cudaStream_t bs) {
+        int r = segment_forward(ctx, d, bs);
+        if (!r) r = segment_reverse(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, bs);
+        return r;
+    });
     if (rc) return rc;
     return segment_reverse_unpermute(ctx, d, Gp, gm_mu, gm_lam, gm_ys, gm_mass, grad, gmat, s);
 }
@@ -1734,56 +1809,6 @@ extern "C" int empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, con
 // ---------------------------------------------------------------------------
 // stored segments: the forward keeps what the reverse pass needs
 // ---------------------------------------------------------------------------
-// Runs body(stream) for stream s: replayed from a segment's cached graph when
-// its key still matches, captured first otherwise (on the context's own
-// stream, joined to s by events, as the rollout graphs are). Kernel timing
-// and EMPM_OPT_SEGMENT_GRAPH 0 run the body directly. A substep loop of a
-// stored segment touches only the segment's and the context's buffers
-// (unsorted reverse passes also the caller's, which are in the key), so one
-// capture serves every later pass of a pooled segment.
-template <typename Body>
-static int run_segment_body(EmpmCtx* ctx, cudaGraphExec_t& exec, SegGraphKey& have, const SegGraphKey& want,
-                            cudaStream_t s, Body body) {
-    if (ctx->timing || !ctx->segment_graph) return body(s);
-    if (!exec || memcmp(&have, &want, sizeof(want)) != 0) {
-        if (exec) cudaGraphExecDestroy(exec);
-        exec = nullptr;
-        CK(cudaStreamBeginCapture(ctx->own_stream, cudaStreamCaptureModeThreadLocal), "begin segment capture");
-        const int rc = body(ctx->own_stream);
-        cudaGraph_t graph = nullptr;
-        cudaError_t e = cudaStreamEndCapture(ctx->own_stream, &graph);
-        if (rc) {
-            if (graph) cudaGraphDestroy(graph);
-            return rc;
-        }
-        CK(e, "end segment capture");
-        e = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) {
-            exec = nullptr;
-            return empm_check_cuda(ctx, e, "segment graph instantiate");
-        }
-        have = want;
-    }
-    CK(cudaEventRecord(ctx->ev_a, s), "record");
-    CK(cudaStreamWaitEvent(ctx->own_stream, ctx->ev_a, 0), "wait");
-    CK(cudaGraphLaunch(exec, ctx->own_stream), "segment graph launch");
-    CK(cudaEventRecord(ctx->ev_b, ctx->own_stream), "record");
-    CK(cudaStreamWaitEvent(s, ctx->ev_b, 0), "wait");
-    return EMPM_OK;
-}
-
-static SegGraphKey segment_key(const EmpmCtx* ctx) {
-    SegGraphKey k;
-    memset(&k, 0, sizeof(k));
-    k.epoch = ctx->epoch;
-    k.params_version = ctx->params_version;
-    k.seg_cap = ctx->seg_cap;
-    k.p2g_mode = ctx->p2g_mode;
-    k.sort_every = ctx->sort_every;
-    k.n = ctx->n_particles;
-    return k;
-}
 static size_t segment_bytes(size_t np, size_t cap_blocks, int n_steps) {
     const size_t k = (size_t)n_steps;
     return ((k + 1) * 26 * np + k * 3 * np + k * 9 * np + np) * sizeof(float) + 2 * np * sizeof(int) +

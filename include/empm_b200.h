@@ -318,10 +318,10 @@ int  empm_rollout_ex(EmpmCtx* ctx, EmpmParticles* a, EmpmParticles* b, const Emp
                                     kernel that keeps only position and elastic F per particle between substeps
                                     (default); 0 = separate kernels. Step tables that release a held instance
                                     (hold 1 then 0) always run separately. */
-#define EMPM_OPT_SEGMENT_GRAPH 8 /* stored segments (empm_segment_forward / _reverse): 1 = each segment captures
-                                    its substep loop as a CUDA graph on first use and replays it while the
-                                    context's options and buffers are unchanged (default); 0 = launch the
-                                    kernels one by one */
+#define EMPM_OPT_SEGMENT_GRAPH 8 /* stored segments (empm_segment_forward / _reverse) and checkpointed
+                                    segments (empm_adjoint_segment): 1 = their substep loops are captured as
+                                    CUDA graphs on first use and replayed while the context's options and
+                                    buffers are unchanged (default); 0 = launch the kernels one by one */
 
 int  empm_ctx_set_option(EmpmCtx* ctx, int option, int value);
 
@@ -393,7 +393,10 @@ typedef struct {
  * reads them; otherwise it recomputes each substep's grid first. Then the
  * three adjoint kernels run. The result is the gradient of the FP32 forward
  * map, up to FP32 rounding. The velocity written by a rotation modifier is
- * treated as independent of x. */
+ * treated as independent of x. With EMPM_OPT_SEGMENT_GRAPH the re-run and the
+ * reverse pass are captured as a CUDA graph, cached in the context (a few
+ * entries, by segment length and options), and replayed by later calls with
+ * the same key. */
 int  empm_adjoint_segment(EmpmCtx* ctx, const EmpmParticles* ckpt, const float* ckpt_mu, const float* ckpt_lam,
                           const float* ckpt_yield, const EmpmMaterial* mat, const EmpmStep* steps, int n_steps,
                           EmpmParticles* grad, EmpmMaterialGrad* gmat, void* stream);

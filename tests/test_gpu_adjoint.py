@@ -309,13 +309,15 @@ def test_segment_adjoint_store_matches_recompute(sort_every):
             assert rel <= 2e-3, (name, k, rel)
 
 
+@pytest.mark.parametrize("store", [True, False])
 @pytest.mark.parametrize("sort_every", [16, 0])
-def test_segment_graphs_match_direct_launches(sort_every):
+def test_segment_graphs_match_direct_launches(sort_every, store):
     """Stored segments capture their substep loops as CUDA graphs on first use
-    and replay them on later passes of the pooled segments. Replayed passes,
-    including one whose step tables changed (a later start time moves the
-    impulse's gate), give the gradients of the same passes launched kernel by
-    kernel, up to the order of the atomics."""
+    and replay them on later passes of the pooled segments; checkpointed
+    segments (re-run in the reverse pass) replay graphs cached in the context.
+    Replayed passes, including one whose step tables changed (a later start
+    time moves the impulse's gate), give the gradients of the same passes
+    launched kernel by kernel, up to the order of the atomics."""
     dt, T, every = 2e-4, 10, 4
     p = _problem(5, n=1500, G=24, seed=21, floor=True, deform=0.25, speed=0.5)
     p["v"][:, 1] = np.float32(-1.0)
@@ -339,8 +341,9 @@ def test_segment_graphs_match_direct_launches(sort_every):
             for dst, src in zip((md.mu, md.lam, md.yield_stress), mat0):
                 dst.copy_(src)
             sv.time = t0
-            tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=every, store=True)
+            tape = CheckpointedRollout(sv, md, st, dt, T, checkpoint_every=every, store=store)
             final = tape.forward()
+            assert tape.stored == store
             res = tape.backward(g_x=g_x, g_v=g_v)
             torch.cuda.synchronize()
             out.append((final.particle_x.double().cpu().numpy(),
