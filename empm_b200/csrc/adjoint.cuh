@@ -326,16 +326,29 @@ __global__ void __launch_bounds__(256) k_adj_grid(const AdjGridArgs a) {
 
 // Over the blocks of a store slot (a stored substep): the momentum is read
 // from the slot, so the grid's accumulator and flags are not used. One thread
-// per node, grid-stride.
+// per node, grid-stride. With rslot, the same launch then writes the node
+// velocities of the previous substep's slot back into the grid (vel) for the
+// next G2P adjoint: this pass reads no velocities from the grid, and the G2P
+// adjoint of this substep has already read them.
 __global__ void __launch_bounds__(256) k_adj_grid_stored(const AdjGridArgs a, const float4* __restrict__ slot,
-                                                         const int* __restrict__ slot_list) {
+                                                         const int* __restrict__ slot_list, float4* __restrict__ vel,
+                                                         const float4* __restrict__ rslot,
+                                                         const int* __restrict__ rlist) {
     const long long total = (long long)__ldg(slot_list) * 64;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
         const long long k = idx >> 6;
         const int lane = (int)(idx & 63);
         const int b = __ldg(slot_list + 1 + k);
         adj_grid_node(a, b, find_instance_block(a.L, b), lane, __ldg(slot + k * 128 + lane));
+    }
+    if (!rslot) return;
+    const long long rtotal = (long long)__ldg(rlist) * 64;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < rtotal; idx += stride) {
+        const long long k = idx >> 6;
+        const int in_block = (int)(idx & 63);
+        const int b = __ldg(rlist + 1 + k);
+        vel[((long long)b << 6) | in_block] = __ldg(rslot + k * 128 + 64 + in_block);
     }
 }
 

@@ -1520,8 +1520,11 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         const int* slot_list = d.store ? d.glist + (size_t)k * (d.cap_blocks + 1) : nullptr;
         if (d.store) {
             Fk = f9_planes(d.fe + (size_t)k * 9 * np, n);
-            k_restore_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_vel, slot, slot_list);
-            CK(cudaGetLastError(), "k_restore_grid");
+            // the grid adjoint of substep k + 1 restored this substep's velocities
+            if (k == n_steps - 1) {
+                k_restore_grid<<<grid_ctas, 256, 0, s>>>(ctx->grid_vel, slot, slot_list);
+                CK(cudaGetLastError(), "k_restore_grid");
+            }
         } else {
             CK(cudaMemcpyAsync(ab.work, snap, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, s),
                "restore snapshot");
@@ -1560,7 +1563,11 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         gg.flags = ctx->flags;
         gg.L = Lk;
         timing_mark(ctx, 4, 0, s);
-        if (d.store) k_adj_grid_stored<<<grid_ctas, 256, 0, s>>>(gg, slot, slot_list);
+        if (d.store) {
+            const float4* rslot = k > 0 ? d.gsave + (size_t)(k - 1) * d.cap_blocks * 128 : nullptr;
+            const int* rlist = k > 0 ? d.glist + (size_t)(k - 1) * (d.cap_blocks + 1) : nullptr;
+            k_adj_grid_stored<<<grid_ctas, 256, 0, s>>>(gg, slot, slot_list, ctx->grid_vel, rslot, rlist);
+        }
         else k_adj_grid<<<(int)nb, 256, 0, s>>>(gg);
         timing_mark(ctx, 4, 1, s);
         CK(cudaGetLastError(), "k_adj_grid");
