@@ -167,8 +167,8 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
 #pragma unroll
 #endif
     for (int i = 0; i < 3; ++i) {
-        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
-        const float ux = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        float wx, ux;
+        bspline_at(st.fx[0], i, wx, ux);
         const float hx = bspline_d2(i);
         const V3 qi = q0 + (float)i * Q0;
         V3 Vi = zero;
@@ -426,8 +426,8 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
 #pragma unroll
 #endif
     for (int i = 0; i < 3; ++i) {
-        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
-        const float ux = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        float wx, ux;
+        bspline_at(st.fx[0], i, wx, ux);
         const float hx = bspline_d2(i);
         const V3 ei = e0 + (((float)i - st.fx[0]) * dx) * Cd0;
         V3 Wi = zero;

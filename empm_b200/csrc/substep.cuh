@@ -51,6 +51,21 @@ EMPM_HD Stencil make_stencil(V3 x, float inv_dx) {
     return st;
 }
 
+// Quadratic B-spline weight and its derivative in fx at stencil offset i,
+// formed from fx (the same expressions as make_stencil): loops over a
+// run-time offset then need no table of the three weights.
+EMPM_HD void bspline_at(float f, int i, float& w, float& dw) {
+    if (i == 1) {
+        const float x = f - 1.f;
+        w = (0.f - x * x) + 0.75f;
+        dw = -2.f * x;
+        return;
+    }
+    const float t = i == 0 ? 1.5f - f : f - 0.5f;
+    w = (t * t) * 0.5f;
+    dw = i == 0 ? -t : t;
+}
+
 EMPM_HD bool stencil_in_grid(const Stencil& st, int G) {
     return st.b[0] >= 0 && st.b[1] >= 0 && st.b[2] >= 0 &&
            st.b[0] + 2 < G && st.b[1] + 2 < G && st.b[2] + 2 < G;
@@ -305,8 +320,8 @@ __device__ __forceinline__ void p2g_emit(const P2GPre& p, Emit emit) {
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
         const V3 ai = p.a + (float)i * B0;
-        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
-        const float dwx = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        float wx, dwx;
+        bspline_at(st.fx[0], i, wx, dwx);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const V3 aij = j == 0 ? ai : ai + (float)j * B1;
@@ -396,8 +411,8 @@ __device__ __forceinline__ G2POut g2p_gather_rt(const Stencil& st, float inv_dx,
     V3 g0 = vs, g1 = vs, g2 = vs;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        const float wx = i == 0 ? st.w[0][0] : (i == 1 ? st.w[0][1] : st.w[0][2]);
-        const float dwx = i == 0 ? st.dw[0][0] : (i == 1 ? st.dw[0][1] : st.dw[0][2]);
+        float wx, dwx;
+        bspline_at(st.fx[0], i, wx, dwx);
         V3 si = v3(0.f, 0.f, 0.f);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
