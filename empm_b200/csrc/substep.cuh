@@ -311,12 +311,12 @@ __device__ __forceinline__ void p2g_emit(const P2GPre& p, Emit emit) {
     const Stencil& st = p.st;
     const V3 B0 = col(p.B, 0), B1 = col(p.B, 1), B2 = col(p.B, 2);
     const V3 S0 = col(p.S, 0), S1 = col(p.S, 1), S2 = col(p.S, 2);
-    const float wz0 = st.w[2][0], wz1 = st.w[2][1], wz2 = st.w[2][2];
-    const float kz2 = 2.f * wz2;
-    const float uz0 = st.dw[2][0], uz1 = st.dw[2][1], uz2 = st.dw[2][2];
-    // the outer axis is a loop (weights picked by selects): a third of the
-    // code of the fully unrolled 27 nodes, for the instruction cache (a loop
-    // over the middle axis as well measured slower)
+    // the outer axis is a loop: a third of the code of the fully unrolled 27
+    // nodes, for the instruction cache (a loop over the middle axis as well
+    // measured slower). The weights are formed from fx where they are used
+    // rather than kept in a table: fewer live registers, fewer spills at the
+    // 64-register cap of the particle kernels (population fused kernel 586 ->
+    // 563 us for all three axes)
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
         const V3 ai = p.a + (float)i * B0;
@@ -325,11 +325,18 @@ __device__ __forceinline__ void p2g_emit(const P2GPre& p, Emit emit) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             const V3 aij = j == 0 ? ai : ai + (float)j * B1;
-            const float wxy = wx * st.w[1][j], dxy = dwx * st.w[1][j], xdy = wx * st.dw[1][j];
+            float wy_, dwy_;
+            bspline_at(st.fx[1], j, wy_, dwy_);
+            const float wxy = wx * wy_, dxy = dwx * wy_, xdy = wx * dwy_;
             const float mw = wxy * p.m;
             const V3 P = mw * aij + dxy * S0 + xdy * S1;
             const V3 Q = mw * B2;
             const V3 R = wxy * S2;
+            float wz0, uz0, wz1, uz1, wz2, uz2;
+            bspline_at(st.fx[2], 0, wz0, uz0);
+            bspline_at(st.fx[2], 1, wz1, uz1);
+            bspline_at(st.fx[2], 2, wz2, uz2);
+            const float kz2 = 2.f * wz2;
             const V3 c0 = wz0 * P + uz0 * R;
             emit(i, j, 0, make_float4(c0.x, c0.y, c0.z, wz0 * mw));
             const V3 c1 = wz1 * (P + Q) + uz1 * R;
@@ -401,8 +408,8 @@ __device__ __forceinline__ G2POut g2p_gather(const Stencil& st, float inv_dx, Fe
     return o;
 }
 
-// g2p_gather with a run-time loop over the outer stencil axis (weights picked
-// by selects): a third of the code, fewer gathers in flight. The kernel that
+// g2p_gather with a run-time loop over the outer stencil axis (weights formed
+// from fx where they are used): a third of the code, fewer gathers in flight. The kernel that
 // runs G2P and P2G back to back uses it where its size is what limits it.
 template <typename Fetch>
 __device__ __forceinline__ G2POut g2p_gather_rt(const Stencil& st, float inv_dx, Fetch fetch) {
@@ -416,18 +423,21 @@ __device__ __forceinline__ G2POut g2p_gather_rt(const Stencil& st, float inv_dx,
         V3 si = v3(0.f, 0.f, 0.f);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const float wxy = wx * st.w[1][j], dxy = dwx * st.w[1][j], xdy = wx * st.dw[1][j];
+            float wy_, dwy_;
+            bspline_at(st.fx[1], j, wy_, dwy_);
+            const float wxy = wx * wy_, dxy = dwx * wy_, xdy = wx * dwy_;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const V3 g = fetch(i, j, k);
-                const float wz = st.w[2][k];
+                float wz, dwz;
+                bspline_at(st.fx[2], k, wz, dwz);
                 const V3 wg = (wxy * wz) * g;
                 si = si + wg;
                 if (j) m1 = m1 + (float)j * wg;
                 if (k) m2 = m2 + (float)k * wg;
                 g0 = g0 + (dxy * wz) * g;
                 g1 = g1 + (xdy * wz) * g;
-                g2 = g2 + (wxy * st.dw[2][k]) * g;
+                g2 = g2 + (wxy * dwz) * g;
             }
         }
         vs = vs + si;
