@@ -527,7 +527,7 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_P2G_MIN_CTAS) k_adj_p2g(const Ad
     const M3 g_tau = (-vol * dt) * gSv;
 
     SpectralEval e;
-    spectral_eval<MAT>(f9_load(a.P.F, p), __ldg(a.M.mu + p), __ldg(a.M.lam + p), __ldg(a.M.ys + p), dt, c.ms, e);
+    spectral_eval<MAT>(f9_load(a.P.F, p), __ldg(a.M.mu + p), __ldg(a.M.lam + p), __ldg(a.M.ys + p), dt, *c.ms, e);
     {
         // sum_n H_n Sv^T gmv_n, component a = sum_b dot(column b of Sv, sum_n H_n[a][b] gmv_n)
         const M3 Sv = (-vol) * spectral_tau(e);
