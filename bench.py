@@ -58,7 +58,8 @@ def load_peaks():
 # particle count on a B200: (workload, kernel, particles) -> bytes per launch.
 NCU_DRAM_BYTES = {
     ("c4", "stress_p2g", 3172508): 403.197184e6 + 110.350592e6,
-    ("c4", "g2p2g", 3172508): 248.493056e6 + 140.657920e6,
+    ("c4", "g2p2g", 3172508): 248.482048e6 + 127.045632e6,
+    ("c3", "adj_p2g", 200000): 38.966272e6 + 0.203008e6,
     ("lbs", "blend", 2000000): 196.818688e6 + 41.4976e6,
 }
 
@@ -933,7 +934,8 @@ def run_ours_c3(args):
                    "adjoint_bytes_per_particle_substep": 3 * bp["substep"],
                    "loss_at_first_timed_step": loss0, "gradients": grads},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": measured_traffic("c3", dom, n),
                      "algorithmic_bytes_per_particle": ADJ_P2G_BYTES, "launch_ms": kms[dom],
                      "kernel_ms": {k: round(v, 5) for k, v in kms.items()},
                      "timing": "CUDA events around each kernel on its launch stream, stream path of one "
