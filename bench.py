@@ -1404,6 +1404,8 @@ def main():
     ap.add_argument("--no-autotune", dest="no_autotune", action="store_true",
                     help="c4: keep the default launch options instead of tuning them on the population")
     args = ap.parse_args()
+    if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
+        return 0   # the reference arm runs on the host cores of rank 0 alone; the other ranks do no work
     if args.workload == "lbs":
         return run_reference_lbs(args) if args.impl == "reference" else run_ours_lbs(args)
     if args.impl == "reference":

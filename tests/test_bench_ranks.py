@@ -56,3 +56,16 @@ def test_one_rank_needs_no_process_group(monkeypatch):
     assert bench.dist_setup(None) == (1, 0, 0)
     bench.rank_barrier(1)
     assert bench.rank_max(2.5, 1, "cpu") == 2.5
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    """Under a multi-rank launch the reference arm (the host-core CPU
+    implementation) runs on rank 0 alone: another rank exits 0 without work
+    or output."""
+    import subprocess
+
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1"], env=env, capture_output=True, text=True, timeout=120, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == ""
