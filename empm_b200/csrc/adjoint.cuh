@@ -52,16 +52,6 @@ namespace empm {
 // second derivative of the quadratic B-spline weight at stencil offset o
 EMPM_HD float bspline_d2(int o) { return o == 1 ? -2.f : 1.f; }
 
-// Hessian (grid units) of w = wx wy wz at node (i, j, k) of the stencil, times b
-EMPM_HD V3 weight_hessian_times(const Stencil& st, int i, int j, int k, V3 b) {
-    const float wx = st.w[0][i], wy = st.w[1][j], wz = st.w[2][k];
-    const float dx = st.dw[0][i], dy = st.dw[1][j], dz = st.dw[2][k];
-    const float hxx = bspline_d2(i) * wy * wz, hyy = wx * bspline_d2(j) * wz, hzz = wx * wy * bspline_d2(k);
-    const float hxy = dx * dy * wz, hxz = dx * wy * dz, hyz = wx * dy * dz;
-    return v3(hxx * b.x + hxy * b.y + hxz * b.z, hxy * b.x + hyy * b.y + hyz * b.z, hxz * b.x + hyz * b.y + hzz * b.z);
-}
-
-
 // ---------------------------------------------------------------------------
 // G2P adjoint
 // ---------------------------------------------------------------------------
