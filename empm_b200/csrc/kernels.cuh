@@ -771,8 +771,13 @@ __global__ void __launch_bounds__(256, EMPM_P2G_MIN_CTAS) k_p2g_warpagg(Particle
 // full state. Held instances (step-table hold) must stay held once held within
 // the run: when a particle's instance becomes held at substep s, its state
 // after the G2P of s-1 is written in full, then left alone.
-template <int ROUNDS, int MAT = -1>
-__global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g(ParticleArrays P, MaterialArrays M, F9Planes Fe,
+// MINB: resident CTAs per SM asked of the compiler. Launches over few
+// particles (CTAs of 64 threads, a few warps per SM) use MINB = 1: registers
+// are then not what limits them, so the kernel keeps all its state in
+// registers and gathers with the unrolled loop (C1, 20k particles: 25.3 ->
+// 23.7 us per substep).
+template <int ROUNDS, int MAT = -1, int MINB = EMPM_FUSED_MIN_CTAS>
+__global__ void __launch_bounds__(256, MINB) k_g2p2g(ParticleArrays P, MaterialArrays M, F9Planes Fe,
                                                                   Launch L, int g2p_table, const float4* vel,
                                                                   float4* mom, unsigned char* flags) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -850,11 +855,9 @@ __global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g(ParticleArra
             }
 #else
             GlobalFetch fetch{vel, &c};
-#if EMPM_FUSED_G2P_LOOP
-            const G2POut o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
-#else
-            const G2POut o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
-#endif
+            G2POut o;
+            if (EMPM_FUSED_G2P_LOOP && MINB > 1) o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
+            else o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
 #endif
             const float dx = 1.f / c.inv_dx;   // as g2p_particle computes it
             const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
@@ -912,8 +915,8 @@ struct SegmentStoreArgs {
     long long      np;
 };
 
-template <int ROUNDS, int MAT = -1>
-__global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g_store(MaterialArrays M, Launch L, int g2p_table,
+template <int ROUNDS, int MAT = -1, int MINB = EMPM_FUSED_MIN_CTAS>
+__global__ void __launch_bounds__(256, MINB) k_g2p2g_store(MaterialArrays M, Launch L, int g2p_table,
                                                                         const float4* vel, float4* mom,
                                                                         unsigned char* flags, SegmentStoreArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -939,7 +942,9 @@ __global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g_store(Materi
             const Stencil st = make_stencil(x, c.inv_dx);
             const bool in_grid = stencil_in_grid(st, c.G);
             const GlobalFetch fetch{vel, &c};
-            const G2POut o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
+            G2POut o;
+            if (MINB > 1) o = g2p_gather_rt(st, c.inv_dx, fetch.bind(st, in_grid));
+            else o = g2p_gather(st, c.inv_dx, fetch.bind(st, in_grid));
             const float dx = 1.f / c.inv_dx;   // as g2p_particle computes it
             const float lo = dx * 2.f, hi = c.grid_lim - dx * 2.f;
             V3 nx = x + dt * o.v;
@@ -976,13 +981,17 @@ __global__ void __launch_bounds__(256, EMPM_FUSED_MIN_CTAS) k_g2p2g_store(Materi
 }
 
 // k_g2p2g_store at the default run cap (4) for a launch whose instances all
-// use material (plasticine 5 and jelly 0 have kernels of their own, -1 any).
+// use material (plasticine 5 and jelly 0 have kernels of their own, -1 any);
+// few: a launch over few particles (the MINB = 1 variant, as for k_g2p2g).
 // Returns false for other run caps (the caller runs the separate kernels).
 static inline bool launch_g2p2g_store(int grid_ctas, int threads, cudaStream_t s, const MaterialArrays& M,
                                       const Launch& L, int g2p_table, const float4* vel, float4* mom,
-                                      unsigned char* flags, const SegmentStoreArgs& a, int seg_cap, int material) {
+                                      unsigned char* flags, const SegmentStoreArgs& a, int seg_cap, int material,
+                                      bool few = false) {
     if (seg_cap != 4) return false;
-    if (material == 5) k_g2p2g_store<2, 5><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
+    if (few && material == 5) k_g2p2g_store<2, 5, 1><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
+    else if (few && material == 0) k_g2p2g_store<2, 0, 1><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
+    else if (material == 5) k_g2p2g_store<2, 5><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
     else if (material == 0) k_g2p2g_store<2, 0><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
     else k_g2p2g_store<2, -1><<<grid_ctas, threads, 0, s>>>(M, L, g2p_table, vel, mom, flags, a);
     return true;
@@ -991,8 +1000,18 @@ static inline bool launch_g2p2g_store(int grid_ctas, int threads, cudaStream_t s
 static inline void launch_g2p2g(int grid_ctas, int threads, cudaStream_t s, const ParticleArrays& P,
                                 const MaterialArrays& M, const F9Planes& Fe, const Launch& L, int g2p_table,
                                 const float4* vel, float4* mom, unsigned char* flags, int seg_cap,
-                                int material = -1) {
+                                int material = -1, bool few = false) {
+    // few: a launch over few particles (CTAs of 64 threads) takes the MINB = 1
+    // variant where one is compiled (plasticine and jelly at run cap 4)
 #define EMPM_G2P2G(R, MAT) k_g2p2g<R, MAT><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, g2p_table, vel, mom, flags)
+    if (few && material == 5 && seg_cap == 4) {
+        k_g2p2g<2, 5, 1><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, g2p_table, vel, mom, flags);
+        return;
+    }
+    if (few && material == 0 && seg_cap == 4) {
+        k_g2p2g<2, 0, 1><<<grid_ctas, threads, 0, s>>>(P, M, Fe, L, g2p_table, vel, mom, flags);
+        return;
+    }
     if (material == 5 && seg_cap == 4) { EMPM_G2P2G(2, 5); return; }
     if (material == 5 && seg_cap == 8) { EMPM_G2P2G(3, 5); return; }
     if (material == 0 && seg_cap == 4) { EMPM_G2P2G(2, 0); return; }

@@ -859,7 +859,7 @@ static int launch_g2p2g_sorted(EmpmCtx* ctx, const SortedState& ss, int g2p_tabl
     const int tp = particle_threads(ctx, n, 256);
     timing_mark(ctx, 6, 0, stream);
     launch_g2p2g(blocks_for(n, tp), tp, stream, t.P, t.M, t.Fe, t.L, g2p_table, ctx->grid_vel, ctx->grid_mom,
-                 ctx->flags, ctx->seg_cap, uniform_material(ctx));
+                 ctx->flags, ctx->seg_cap, uniform_material(ctx), tp < 256);
     timing_mark(ctx, 6, 1, stream);
     CK(cudaGetLastError(), "k_g2p2g");
     return EMPM_OK;
@@ -1456,8 +1456,9 @@ static int segment_forward(EmpmCtx* ctx, const SegmentData& d, cudaStream_t s) {
             sa.snap = d.mats + (size_t)k * 3 * np;
             sa.np = (long long)np;
             timing_mark(ctx, 6, 0, s);
-            launch_g2p2g_store(blocks_for(n, 256), 256, s, Mw, Lk, k - 1, ctx->grid_vel, ctx->grid_mom, ctx->flags, sa,
-                               ctx->seg_cap, uniform_material(ctx));
+            const int tp = particle_threads(ctx, n, 256);
+            launch_g2p2g_store(blocks_for(n, tp), tp, s, Mw, Lk, k - 1, ctx->grid_vel, ctx->grid_mom, ctx->flags, sa,
+                               ctx->seg_cap, uniform_material(ctx), tp < 256);
             timing_mark(ctx, 6, 1, s);
             CK(cudaGetLastError(), "k_g2p2g_store");
         } else {
