@@ -86,3 +86,17 @@ def test_adjoint_entry_points_reject_bad_arguments_without_gpu():
     p.n_grid, p.grid_lim = 16, 1.0
     assert L.empm_debug_stress_adjoint(p, None, None, None, None, 0.0, None, None, None, None, None, None, 3,
                                        None) == -1
+
+
+def test_option_ids_match_header():
+    """Every launch option the header defines (EMPM_OPT_*) has the same id in
+    the Python binding."""
+    import os
+    import re
+
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "empm_b200.h")).read()
+    opts = dict(re.findall(r"#define\s+EMPM_OPT_(\w+)\s+(\d+)", hdr))
+    assert "SEGMENT_GRAPH" in opts and "FUSE" in opts
+    for name, value in opts.items():
+        assert getattr(N, "OPT_" + name) == int(value), name
