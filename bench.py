@@ -679,7 +679,10 @@ def run_ours_c4(args):
                       "gradient_requests": cf["gradient_requests"], "latency_ms": cf["latency_ms"],
                       "makespan_s": cf["makespan_s"], "plain_value": cf["plain_value"],
                       "served_vs_plain": cf["served_vs_plain"], "plain_kernel_value": cf["plain_kernel_value"],
-                      "served_vs_plain_kernel": cf["served_vs_plain_kernel"], "plain": cf["plain"],
+                      "served_vs_plain_kernel": cf["served_vs_plain_kernel"],
+                      "offered_forward_particle_substeps_per_s": cf["offered_forward_particle_substeps_per_s"],
+                      "plain_sample_value": cf["plain_sample_value"], "plain_rates": cf["plain_rates"],
+                      "plain": cf["plain"],
                       "plain_kernel": cf["plain_kernel"], "timing": cf["timing"], "gpu_launches": c5["gpu_launches"],
                       "clocks": c5["clocks"]}
     else:
@@ -1047,6 +1050,7 @@ def measure_c5(args, dev, world, rank, local, cpu_baseline_leg=True):
     sample = [arrivals[i] for i in prng.choice(len(arrivals), size=min(args.c5_plain, len(arrivals)), replace=False)]
     plain_ps, plain_ms, kernel_ms = 0, 0.0, 0.0
     plain_rows = []
+    by_kind = {k: {"ps": 0, "ms": 0.0, "kms": 0.0} for k in (False, True)}   # per kind: work, plain, kernel path
     for (_, grad, n, G, T, sd) in sample:
         req = W.c5_request(grad, n, G, T, sd)
         solver, md, st = single_instance(req.spec, device=dev)
@@ -1081,8 +1085,11 @@ def measure_c5(args, dev, world, rank, local, cpu_baseline_leg=True):
                            "ms": round(t_rollout, 2), "stored_tape": stored})
         plain_ms += t_rollout
         plain_ps += n * T
+        by_kind[bool(grad)]["ps"] += n * T
+        by_kind[bool(grad)]["ms"] += t_rollout
         if grad:
             kernel_ms += t_rollout   # the checkpointed adjoint is the only single-instance gradient path
+            by_kind[True]["kms"] += t_rollout
         else:
             # the plain kernel path: one p2g2p_differentiable call per substep
             restore()
@@ -1096,11 +1103,25 @@ def measure_c5(args, dev, world, rank, local, cpu_baseline_leg=True):
             e1.record()
             torch.cuda.synchronize()
             kernel_ms += e0.elapsed_time(e1)
+            by_kind[False]["kms"] += e0.elapsed_time(e1)
         solver.release_tape_memory()
         del solver, md, st, other, init
         gc.collect()
-    plain_value = plain_ps / (plain_ms / 1e3)
-    plain_kernel_value = plain_ps / (kernel_ms / 1e3)
+    plain_sample_value = plain_ps / (plain_ms / 1e3)
+    plain_sample_kernel_value = plain_ps / (kernel_ms / 1e3)
+    # The sample's rates per kind of request, weighted by the completed stream's
+    # own work in each kind: the time one-at-a-time service would take for
+    # this stream's mix (a sample of 24 draws its gradient share, which holds
+    # most of the plain time, with much variance). Falls back to the raw
+    # sample when it lacks a kind.
+    work = {k: sum(r[2] * r[3] for r in ok if bool(r[1]) == k) for k in (False, True)}
+    if all(by_kind[k]["ps"] > 0 for k in (False, True)):
+        t_mix = sum(work[k] * by_kind[k]["ms"] / by_kind[k]["ps"] for k in (False, True))
+        tk_mix = sum(work[k] * by_kind[k]["kms"] / by_kind[k]["ps"] for k in (False, True))
+        plain_value = (work[False] + work[True]) / (t_mix / 1e3)
+        plain_kernel_value = (work[False] + work[True]) / (tk_mix / 1e3)
+    else:
+        plain_value, plain_kernel_value = plain_sample_value, plain_sample_kernel_value
 
     cpu = None
     if rank == 0 and world == 1 and cpu_baseline_leg and not args.no_cpu_baseline:
@@ -1136,6 +1157,11 @@ def measure_c5(args, dev, world, rank, local, cpu_baseline_leg=True):
                    "makespan_s": makespan, "hbm_budget_gb": args.c5_budget_gb,
                    "engine": {k: stats[k] for k in ("blocks", "substeps", "relayouts")},
                    "plain_value": plain_value, "served_vs_plain": value / plain_value,
+                   "plain_sample_value": plain_sample_value, "plain_sample_kernel_value": plain_sample_kernel_value,
+                   "plain_rates": {("gradient" if k else "rollout"): {
+                       "api": by_kind[k]["ps"] / (by_kind[k]["ms"] / 1e3) if by_kind[k]["ms"] else None,
+                       "kernel_path": by_kind[k]["ps"] / (by_kind[k]["kms"] / 1e3) if by_kind[k]["kms"] else None,
+                       "stream_work_share": work[k] / max(1, work[False] + work[True])} for k in (False, True)},
                    "plain_kernel_value": plain_kernel_value, "served_vs_plain_kernel": value / plain_kernel_value,
                    "plain_requests": plain_rows,
                    "plain_kernel": "the same sampled requests with the rollouts driven one p2g2p_differentiable call "
@@ -1144,7 +1170,9 @@ def measure_c5(args, dev, world, rank, local, cpu_baseline_leg=True):
                    "plain": f"{len(sample)} requests sampled from the stream, one at a time through the "
                             "single-instance API (rollout with a CUDA graph; gradient: checkpointed rollout + "
                             "adjoint with 50-substep segments), each timed on its second run (context, graphs "
-                            "and buffers already built), CUDA events, no queueing",
+                            "and buffers already built), CUDA events, no queueing; plain_value combines the "
+                            "sample's rollout and gradient rates with the completed stream's work in each kind "
+                            "(plain_sample_value: the raw sample)",
                    "timing": "host monotonic clock from the first arrival to the last result",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": None,
