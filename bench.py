@@ -64,6 +64,24 @@ NCU_DRAM_BYTES = {
 }
 
 
+def mix_weighted_rate(by_kind: dict, work: dict, key: str):
+    """Rate (work per second) of serving a stream one request at a time,
+    from a sample's per-kind rates: by_kind[kind] = {"ps": sampled work, key:
+    its milliseconds}, work[kind] = the stream's work of that kind. The time
+    is the sum over kinds of work / sampled rate. None when the sample lacks a
+    kind the stream has."""
+    t_ms = 0.0
+    for k, w in work.items():
+        if w == 0:
+            continue
+        b = by_kind.get(k)
+        if not b or b["ps"] <= 0 or b[key] <= 0:
+            return None
+        t_ms += w * b[key] / b["ps"]
+    total = sum(work.values())
+    return total / (t_ms / 1e3) if t_ms > 0 else None
+
+
 def measured_traffic(workload: str, kernel: str, particles: int):
     """DRAM bytes per launch measured by ncu for this exact workload, else None."""
     return NCU_DRAM_BYTES.get((workload, kernel, int(particles)))
@@ -1115,13 +1133,8 @@ def measure_c5(args, dev, world, rank, local, cpu_baseline_leg=True):
     # most of the plain time, with much variance). Falls back to the raw
     # sample when it lacks a kind.
     work = {k: sum(r[2] * r[3] for r in ok if bool(r[1]) == k) for k in (False, True)}
-    if all(by_kind[k]["ps"] > 0 for k in (False, True)):
-        t_mix = sum(work[k] * by_kind[k]["ms"] / by_kind[k]["ps"] for k in (False, True))
-        tk_mix = sum(work[k] * by_kind[k]["kms"] / by_kind[k]["ps"] for k in (False, True))
-        plain_value = (work[False] + work[True]) / (t_mix / 1e3)
-        plain_kernel_value = (work[False] + work[True]) / (tk_mix / 1e3)
-    else:
-        plain_value, plain_kernel_value = plain_sample_value, plain_sample_kernel_value
+    plain_value = mix_weighted_rate(by_kind, work, "ms") or plain_sample_value
+    plain_kernel_value = mix_weighted_rate(by_kind, work, "kms") or plain_sample_kernel_value
 
     cpu = None
     if rank == 0 and world == 1 and cpu_baseline_leg and not args.no_cpu_baseline:

@@ -69,3 +69,19 @@ def test_reference_arm_runs_on_rank_zero_only():
                         "--warmup", "1"], env=env, capture_output=True, text=True, timeout=120, cwd=ROOT)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_mix_weighted_plain_rate():
+    """The serving leg's plain rate weights the sample's per-kind rates by the
+    stream's own work in each kind."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    by_kind = {False: {"ps": 100, "ms": 10.0}, True: {"ps": 100, "ms": 100.0}}
+    # 900 units of rollouts at 10 per ms, 100 of gradients at 1 per ms: 90 + 100 ms for 1000 units
+    rate = bench.mix_weighted_rate(by_kind, {False: 900, True: 100}, "ms")
+    assert abs(rate - 1000 / 0.190) < 1e-6
+    # a kind the stream has but the sample lacks: no estimate
+    assert bench.mix_weighted_rate({False: {"ps": 100, "ms": 10.0}}, {False: 900, True: 100}, "ms") is None
+    # a kind the sample has but the stream lacks is ignored
+    assert abs(bench.mix_weighted_rate(by_kind, {False: 900, True: 0}, "ms") - 900 / 0.090) < 1e-6
