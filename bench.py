@@ -679,8 +679,8 @@ def run_ours_c4(args):
         cpu = cpu_baseline(c4_instance_workload(specs[0], dt, T), budget_s=12.0, max_substeps=60)
     served = None
     if not args.no_served and world == 1:
-        # the serving stream's figures in the same line (BASELINE metric: batched / served vs
-        # plain, p50 / p99), on one GPU: the population's buffers are released first
+        # the serving stream's figures in the same line (the headline metric: batched / served
+        # vs plain, p50 / p99), on one GPU: the population's buffers are released first
         bopts = {"sort_every": batch.sort_every, "p2g_mode": batch.p2g_mode, "g2p_tile": batch.g2p_tile,
                  "tile_cap": batch.tile_cap, "seg_cap": batch.seg_cap, "fuse": bool(batch.fuse)}
         resume = batch.resume_blocks
