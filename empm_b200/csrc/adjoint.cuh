@@ -83,7 +83,12 @@ struct AdjG2PArgs {
 // order) sum their node-velocity adjoints with shuffles; the segment head
 // issues one reduction per node, as k_p2g_warpagg does for the momentum.
 // Every lane of the warp runs the node loop, invalid lanes with zeros.
+// ROUNDS < 5: runs are capped at 2^ROUNDS lanes (a.seg_cap equals it), so the
+// shuffle rounds the cap never needs are not compiled in; ROUNDS 5 takes any
+// a.seg_cap.
+template <int ROUNDS>
 __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const AdjG2PArgs a) {
+    const int seg_cap = ROUNDS < 5 ? (1 << ROUNDS) : a.seg_cap;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const bool live = p < a.L.n_total;
@@ -106,7 +111,7 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     // lanes, as in k_p2g_warpagg
     const unsigned run_heads = __ballot_sync(0xffffffffu, run_head);
     const int run_start = 31 - __clz(run_heads & (0xffffffffu >> (31 - lane)));
-    const bool head = run_head || ((lane - run_start) & (a.seg_cap - 1)) == 0;
+    const bool head = run_head || ((lane - run_start) & (seg_cap - 1)) == 0;
     const unsigned heads = __ballot_sync(0xffffffffu, head);
     const unsigned above = lane == 31 ? 0u : (heads & (0xffffffffu << (lane + 1)));
     const int end = above ? (__ffs(above) - 2) : 31;
@@ -194,7 +199,7 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
                 if (k) sk[k] += (float)k * dot(vg[k], Q2);
                 // reduction rounds unrolled, each skipped by a warp-uniform branch
 #pragma unroll
-                for (int r = 0; r < 5; ++r) {
+                for (int r = 0; r < ROUNDS; ++r) {
                     const int d = 1 << r;
                     if (d < maxlen) {
                         const float tx = __shfl_down_sync(0xffffffffu, gvg.x, d);

@@ -1554,7 +1554,10 @@ static int segment_reverse(EmpmCtx* ctx, const SegmentData& d, ParticleArrays Gp
         ag.gFe = gFe;
         ag.seg_cap = ctx->seg_cap;
         timing_mark(ctx, 3, 0, s);
-        k_adj_g2p<<<blocks_for(n, 128), 128, 0, s>>>(ag);
+        if (ag.seg_cap == 4)
+            k_adj_g2p<2><<<blocks_for(n, 128), 128, 0, s>>>(ag);
+        else
+            k_adj_g2p<5><<<blocks_for(n, 128), 128, 0, s>>>(ag);
         timing_mark(ctx, 3, 1, s);
         CK(cudaGetLastError(), "k_adj_g2p");
         AdjGridArgs gg;

@@ -139,6 +139,7 @@ def _setup(p, dt):
     sv.initialize(n, n_grid=G, device=DEV)
     sv.sort_every = p.get("sort_every", 16)
     sv.adj_store = p.get("adj_store", True)
+    sv.seg_cap = p.get("seg_cap", sv.seg_cap)
     for m in p.get("modifiers", []):
         if m["kind"] == "impulse":
             sv.add_impulse_on_particles(st, force=m["force"], dt=dt, point=m["point"], size=m["size"],
@@ -246,6 +247,16 @@ def test_segment_adjoint_plasticine_yielding(sort_every):
     p["sort_every"] = sort_every
     tape = _check_directional(p, 2e-4, 6, 4, seed=12)
     assert tape.bounds == [0, 4, 6]
+
+
+@pytest.mark.parametrize("seg_cap", [1, 32])
+def test_segment_adjoint_run_caps(seg_cap):
+    """Same-cell runs capped at 1 or 32 lanes: the G2P adjoint's shuffle
+    reduction takes its general form (the default cap of 4 has one with the
+    rounds fixed at compile time), checked against finite differences."""
+    p = _problem(5, n=800, G=16, seed=2, deform=0.25, speed=0.5)
+    p["seg_cap"] = seg_cap
+    _check_directional(p, 2e-4, 6, 4, seed=12)
 
 
 def test_segment_adjoint_with_floor_contact():
