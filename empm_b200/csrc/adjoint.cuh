@@ -156,6 +156,15 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
     // Hessian term contracted row by row: three accumulators instead of the
     // 18 of its moments, which let the kernel fit fewer registers)
     V3 X3 = zero;
+    // node addresses: the block index sits above the 6 bits of the local
+    // index, so the address of node (i, j, k) is a part of its row (i, j) plus
+    // a part of k (formed once here)
+    int zpart[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int iz = st.b[2] + k;
+        zpart[k] = (iz >> 2) * 64 + (iz & 3);
+    }
 #if EMPM_ADJ_G2P_ROLL
 #pragma unroll 1
 #else
@@ -178,12 +187,15 @@ __global__ void __launch_bounds__(128, EMPM_ADJ_G2P_MIN_CTAS) k_adj_g2p(const Ad
             const V3 R = wxy * G2;
             V3 vg[3];
             float sk[3];
+            const int ix = st.b[0] + i, iy = st.b[1] + j;
+            const long long row = (long long)(c.boff + ((ix >> 2) * c.NB + (iy >> 2)) * c.NB) * 64 +
+                                  (ix & 3) * 16 + (iy & 3) * 4;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const int ix = st.b[0] + i, iy = st.b[1] + j, iz = st.b[2] + k;
+                const int iz = st.b[2] + k;
                 const bool node_ok = valid && (in_grid || (ix >= 0 && iy >= 0 && iz >= 0 && ix < c.G && iy < c.G &&
                                                            iz < c.G));
-                const long long addr = node_ok ? gaddr(c, ix, iy, iz) : 0;
+                const long long addr = node_ok ? row + zpart[k] : 0;
                 vg[k] = zero;
                 if (node_ok) {
                     const float4 g4 = __ldg(a.vel + addr);
